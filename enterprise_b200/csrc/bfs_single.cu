@@ -1,0 +1,1014 @@
+// Direction-optimising single-source BFS for sm_100a.
+//
+// What it replaces (reference bfs_gpu_opt.cuh:40-288 and the kernels it
+// drives): a host-driven level loop that per level launches 13-14 kernels
+// (inspector over all V, three two-kernel scans, three reapers, three
+// expanders) and synchronises the host >= 5 times.
+//
+// Design here:
+//  * Status lives in bitmaps: `vis` (visited, 1 bit/vertex) and two frontier
+//    bitmaps fb[level & 1]. At s24 each is 2 MB and stays in L2.
+//  * Top-down (TD) levels expand classified frontier queues (small: < small_max,
+//    warp-cooperative gather; mid: warp per vertex; large: CTA per chunk of
+//    chunk_edges edges), claim vertices with atomicOr on `vis`, and append
+//    discoveries to a raw queue with warp-aggregated atomics
+//    (reference expanders K2-K4, expander.cuh:74-423).
+//  * The inspector (reference K8/K9/K11, inspector.cuh:36-432) classifies the
+//    raw queue (TD) or the unvisited set (BU) into small/mid/large queues with
+//    one single-pass decoupled look-back scan, order-preserving.
+//  * Bottom-up (BU) levels scan unvisited vertices (thread / warp / CTA tiers
+//    with early exit) against the frontier bitmap and a shared-memory hub
+//    cache of the frontier's highest-degree vertices
+//    (reference K5-K7, expander.cuh:431-819; hub cache comm.h:172-177).
+//  * The direction policy runs on the device in the inspector's last CTA
+//    (reference rule inspector.cuh:486-521 is one option; Beamer alpha/beta
+//    with switch-back is the default).
+//  * The whole traversal is one CUDA graph: a reset kernel, then a while node
+//    whose body is [expand, inspect]; the inspector sets the loop condition.
+#include <algorithm>
+#include <cooperative_groups.h>
+#include <string.h>
+
+#include "dev_common.cuh"
+#include "dev_graph.h"
+
+namespace ent {
+
+constexpr int BT = 256;          // threads per CTA of the level kernels
+constexpr int IPT = 4;           // items per thread in an inspector tile
+constexpr int TILE = BT * IPT;   // items per inspector tile
+constexpr int KS = 4;            // look-back status words per tile
+constexpr int TD = 0, BU = 1;
+
+// Device-resident loop state. Written only by the reset kernel's and the
+// inspector's last CTA; read by every kernel at start.
+struct BfsCtl {
+  int32_t src;
+  int32_t pad0;
+  int32_t* depth;
+  int32_t* parent;
+  int32_t level;      // the frontier holds the vertices at depth `level`
+  int32_t dir;        // direction used to expand `level`
+  int32_t bu_sweep;   // BU expand scans all vertices (first BU level)
+  int32_t qcur;       // ping-pong index of TD queues
+  int32_t ucur;       // ping-pong index of BU unvisited queues
+  int32_t n_q[3];     // TD frontier queue sizes (small, mid, large)
+  int32_t n_chunks;   // chunks of the large TD queue
+  int32_t n_u[3];     // BU unvisited queue sizes
+  int32_t n_raw;      // TD raw next-frontier count (atomic append)
+  int32_t done;
+  int32_t err;        // bit 1: look-back wait timed out, bit 2: level overflow
+  int32_t td_levels;
+  int32_t bu_levels;
+  int32_t pad1;
+  int64_t n_f, m_f;   // frontier size and degree sum
+  int64_t n_vis, m_vis;
+  unsigned long long acc_n, acc_m, acc_nu, acc_mu;
+  uint32_t tot[3 * KS];   // chain totals per segment, written by each segment's last tile
+  uint32_t tile_ticket;
+  uint32_t finished;
+  uint32_t epoch;
+  uint32_t pad2;
+};
+
+struct LevelArgs {
+  BfsCtl* ctl;
+  const int64_t* off;
+  const int32_t* adj;
+  const int32_t* deg;
+  int64_t V, E;
+  uint32_t* vis;
+  uint32_t* fb[2];
+  int32_t* q[2][3];
+  int32_t* qc[2];
+  int32_t* uq[2][3];
+  int32_t* raw;
+  unsigned long long* hub[2];
+  unsigned long long* tiles;  // [3 segments][seg_tiles][KS]
+  int64_t seg_tiles;
+  int32_t small_max, large_min, chunk, hub_slots, hub_shift, hub_min_deg;
+  int32_t policy;
+  double alpha, beta, ref_ratio;
+  cudaGraphConditionalHandle cond;
+  int32_t use_cond;
+  int32_t max_levels;
+};
+
+__device__ __forceinline__ int cls_of(int d, const LevelArgs& a) {
+  return d < a.small_max ? 0 : (d > a.large_min ? 2 : 1);
+}
+__device__ __forceinline__ uint32_t hub_slot(uint32_t v, int shift) { return (v * 0x9E3779B1u) >> shift; }
+
+__device__ __forceinline__ void hub_insert(const LevelArgs& a, unsigned long long* ht, int v, int d) {
+  if (a.hub_slots && d >= a.hub_min_deg)
+    atomicMax(ht + hub_slot((uint32_t)v, a.hub_shift), ((unsigned long long)(uint32_t)d << 32) | (uint32_t)v);
+}
+
+// --------------------------------------------------------------- reset ----
+__device__ void fill_neg1(int32_t* p, int64_t n, int64_t tid, int64_t nth) {
+  uintptr_t addr = (uintptr_t)p;
+  int64_t head = (int64_t)(((16 - (addr & 15)) & 15) >> 2);
+  if ((addr & 3) != 0) head = n;  // not even 4-byte aligned: scalar path
+  if (head > n) head = n;
+  for (int64_t i = tid; i < head; i += nth) p[i] = -1;
+  int64_t nvec = (n - head) >> 2;
+  int4* pv = reinterpret_cast<int4*>(p + head);
+  for (int64_t i = tid; i < nvec; i += nth) pv[i] = make_int4(-1, -1, -1, -1);
+  for (int64_t i = head + nvec * 4 + tid; i < n; i += nth) p[i] = -1;
+}
+
+__global__ void __launch_bounds__(BT) k_reset(LevelArgs a, int32_t src, int32_t* depth, int32_t* parent) {
+  BfsCtl* c = a.ctl;
+  const int64_t tid = blockIdx.x * (int64_t)BT + threadIdx.x, nth = (int64_t)gridDim.x * BT;
+  fill_neg1(depth, a.V, tid, nth);
+  if (parent) fill_neg1(parent, a.V, tid, nth);
+  const int64_t W = (a.V + 31) >> 5;
+  for (int64_t i = tid; i < W; i += nth) {
+    a.vis[i] = 0;
+    a.fb[0][i] = 0;
+    a.fb[1][i] = 0;
+  }
+  for (int64_t i = tid; i < a.hub_slots; i += nth) {
+    a.hub[0][i] = 0;
+    a.hub[1][i] = 0;
+  }
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&c->finished, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  const int d = a.deg[src];
+  const int cl = cls_of(d, a);
+  depth[src] = 0;
+  if (parent) parent[src] = src;
+  a.vis[src >> 5] = 1u << (src & 31);
+  a.fb[0][src >> 5] = 1u << (src & 31);
+  a.q[0][cl][0] = src;
+  c->src = src;
+  c->depth = depth;
+  c->parent = parent;
+  c->level = 0;
+  c->dir = a.policy == ENT_POLICY_BU_ONLY ? BU : TD;
+  c->bu_sweep = c->dir == BU;
+  c->qcur = 0;
+  c->ucur = 0;
+  for (int k = 0; k < 3; ++k) { c->n_q[k] = 0; c->n_u[k] = 0; }
+  c->n_q[cl] = 1;
+  if (cl == 2) {
+    a.qc[0][0] = 0;
+    c->n_chunks = (d + a.chunk - 1) / a.chunk;
+  } else {
+    c->n_chunks = 0;
+  }
+  c->n_raw = 0;
+  c->done = 0;
+  c->err = 0;
+  c->td_levels = 0;
+  c->bu_levels = 0;
+  c->n_f = 1;
+  c->m_f = d;
+  c->n_vis = 1;
+  c->m_vis = d;
+  c->acc_n = c->acc_m = c->acc_nu = c->acc_mu = 0;
+  for (int k = 0; k < 3 * KS; ++k) c->tot[k] = 0;
+  c->tile_ticket = 0;
+  c->finished = 0;
+  __threadfence();
+}
+
+// ------------------------------------------------------------ top-down ----
+__device__ __forceinline__ void td_visit(const LevelArgs& a, BfsCtl* c, int v, int u, bool valid, int ln,
+                                         int32_t* depth, int32_t* parent, uint32_t* fbn) {
+  bool mine = false;
+  if (valid) {
+    const uint32_t w = (uint32_t)v >> 5, b = 1u << (v & 31);
+    if (!(ld_cg(a.vis + w) & b)) {
+      const uint32_t old = atomicOr(a.vis + w, b);
+      if (!(old & b)) {
+        mine = true;
+        depth[v] = ln;
+        if (parent) parent[v] = u;
+        red_or(fbn + w, b);
+      }
+    }
+  }
+  const unsigned m = __ballot_sync(FULL, mine);
+  if (m) {
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&c->n_raw, __popc(m));
+    base = __shfl_sync(FULL, base, leader);
+    if (mine) a.raw[base + __popc(m & lanemask_lt())] = v;
+  }
+}
+
+__device__ void td_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, int32_t* parent) {
+  const int qc = c->qcur;
+  const int ns = c->n_q[0], nm = c->n_q[1], nl = c->n_q[2], nch = c->n_chunks;
+  const int32_t* __restrict__ qs = a.q[qc][0];
+  const int32_t* __restrict__ qm = a.q[qc][1];
+  const int32_t* __restrict__ ql = a.q[qc][2];
+  const int32_t* __restrict__ qch = a.qc[qc];
+  uint32_t* fbn = a.fb[(L + 1) & 1];
+  const int lane = threadIdx.x & 31;
+  const int gw = (int)((blockIdx.x * (int64_t)BT + threadIdx.x) >> 5);
+  const int nw = (int)(((int64_t)gridDim.x * BT) >> 5);
+  const int ln = L + 1;
+
+  // Large tier: one CTA per chunk of a high-degree vertex.
+  __shared__ int s_vi;
+  for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+    if (threadIdx.x == 0) {
+      int lo = 0, hi = nl - 1;
+      while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (qch[mid] <= ch) lo = mid; else hi = mid - 1;
+      }
+      s_vi = lo;
+    }
+    __syncthreads();
+    const int i = s_vi;
+    __syncthreads();
+    const int u = ql[i];
+    const int64_t beg = a.off[u] + (int64_t)(ch - qch[i]) * a.chunk;
+    const int64_t end = min(a.off[u + 1], beg + (int64_t)a.chunk);
+    for (int64_t e0 = beg; e0 < end; e0 += BT) {
+      const int64_t e = e0 + threadIdx.x;
+      const bool valid = e < end;
+      const int v = valid ? __ldg(a.adj + e) : 0;
+      td_visit(a, c, v, u, valid, ln, depth, parent, fbn);
+    }
+  }
+  // Mid tier: one warp per vertex.
+  for (int i = gw; i < nm; i += nw) {
+    const int u = qm[i];
+    const int64_t beg = a.off[u], end = a.off[u + 1];
+    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+      const int64_t e = e0 + lane;
+      const bool valid = e < end;
+      const int v = valid ? __ldg(a.adj + e) : 0;
+      td_visit(a, c, v, u, valid, ln, depth, parent, fbn);
+    }
+  }
+  // Small tier: a warp gathers the adjacency lists of 32 vertices and
+  // processes the concatenation 32 edges at a time.
+  for (int base = gw * 32; base < ns; base += nw * 32) {
+    const int i = base + lane;
+    int u = -1, d = 0;
+    int64_t st = 0;
+    if (i < ns) {
+      u = qs[i];
+      st = a.off[u];
+      d = (int)(a.off[u + 1] - st);
+    }
+    int incl = d;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
+    const int excl = incl - d;
+    for (int r = 0; r < total; r += 32) {
+      const int k = r + lane;
+      const bool valid = k < total;
+      int j = 0;
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int cand = j + step;
+        const int ev = __shfl_sync(FULL, excl, cand & 31);
+        if (cand < 32 && ev <= k) j = cand;
+      }
+      const int64_t sj = __shfl_sync(FULL, st, j);
+      const int ej = __shfl_sync(FULL, excl, j);
+      const int uj = __shfl_sync(FULL, u, j);
+      const int v = valid ? __ldg(a.adj + sj + (k - ej)) : 0;
+      td_visit(a, c, v, uj, valid, ln, depth, parent, fbn);
+    }
+  }
+}
+
+// ----------------------------------------------------------- bottom-up ----
+struct Front {
+  const uint32_t* fb;
+  const int32_t* hub;
+  int hub_slots, shift;
+  __device__ __forceinline__ bool operator()(int u) const {
+    if (hub_slots && hub[hub_slot((uint32_t)u, shift)] == u) return true;
+    return (__ldg(fb + (u >> 5)) >> (u & 31)) & 1u;
+  }
+};
+
+__device__ __forceinline__ void bu_commit(const LevelArgs& a, int v, int pu, int ln, int32_t* depth, int32_t* parent,
+                                          uint32_t* fbn) {
+  depth[v] = ln;
+  if (parent) parent[v] = pu;
+  const uint32_t w = (uint32_t)v >> 5, b = 1u << (v & 31);
+  red_or(a.vis + w, b);
+  red_or(fbn + w, b);
+}
+
+__device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, int32_t* parent, int32_t* s_hub) {
+  const uint32_t* fbc = a.fb[L & 1];
+  uint32_t* fbn = a.fb[(L + 1) & 1];
+  if (a.hub_slots) {
+    const unsigned long long* ht = a.hub[L & 1];
+    for (int i = threadIdx.x; i < a.hub_slots; i += BT) {
+      const unsigned long long key = ht[i];
+      s_hub[i] = key ? (int)(uint32_t)key : -1;
+    }
+  }
+  __syncthreads();
+  const Front is_front{fbc, s_hub, a.hub_slots, a.hub_shift};
+  const int lane = threadIdx.x & 31;
+  const int64_t gtid = blockIdx.x * (int64_t)BT + threadIdx.x, nth = (int64_t)gridDim.x * BT;
+  const int gw = (int)(gtid >> 5), nw = (int)(nth >> 5);
+  const int ln = L + 1;
+
+  if (c->bu_sweep) {
+    // Every vertex; a warp owns 32 consecutive ids (one vis word).
+    const int64_t V = a.V;
+    for (int64_t base = (int64_t)gw * 32; base < V; base += (int64_t)nw * 32) {
+      const int64_t v = base + lane;
+      const uint32_t visw = a.vis[base >> 5];
+      bool todo = false;
+      int d = 0;
+      if (v < V && !((visw >> lane) & 1u)) {
+        d = a.deg[v];
+        todo = d > 0;
+      }
+      bool found = false;
+      int pu = -1;
+      if (todo && d < a.small_max) {
+        const int64_t e0 = a.off[v];
+        for (int64_t e = e0; e < e0 + d; ++e) {
+          const int u = __ldg(a.adj + e);
+          if (is_front(u)) { found = true; pu = u; break; }
+        }
+      }
+      unsigned heavy = __ballot_sync(FULL, todo && d >= a.small_max);
+      while (heavy) {
+        const int j = __ffs(heavy) - 1;
+        heavy &= heavy - 1;
+        const int64_t vj = base + j;
+        const int64_t beg = a.off[vj], end = a.off[vj + 1];
+        int hit = -1;
+        for (int64_t e0 = beg; e0 < end; e0 += 32) {
+          const int64_t e = e0 + lane;
+          const int u = e < end ? __ldg(a.adj + e) : -1;
+          const unsigned hm = __ballot_sync(FULL, e < end && is_front(u));
+          if (hm) { hit = __shfl_sync(FULL, u, __ffs(hm) - 1); break; }
+        }
+        if (lane == j && hit >= 0) { found = true; pu = hit; }
+      }
+      if (found) {
+        depth[v] = ln;
+        if (parent) parent[v] = pu;
+      }
+      const unsigned fm = __ballot_sync(FULL, found);
+      if (lane == 0 && fm) {
+        atomicOr(a.vis + (base >> 5), fm);
+        atomicOr(fbn + (base >> 5), fm);
+      }
+    }
+    return;
+  }
+
+  const int uc = c->ucur;
+  const int ns = c->n_u[0], nm = c->n_u[1], nl = c->n_u[2];
+  const int32_t* __restrict__ us = a.uq[uc][0];
+  const int32_t* __restrict__ um = a.uq[uc][1];
+  const int32_t* __restrict__ ul = a.uq[uc][2];
+  // Large tier: one CTA per unvisited vertex, early exit by block vote.
+  __shared__ int s_hit;
+  for (int i = blockIdx.x; i < nl; i += gridDim.x) {
+    const int v = ul[i];
+    const int64_t beg = a.off[v], end = a.off[v + 1];
+    if (threadIdx.x == 0) s_hit = -1;
+    __syncthreads();
+    for (int64_t e0 = beg; e0 < end; e0 += BT) {
+      const int64_t e = e0 + threadIdx.x;
+      bool h = false;
+      if (e < end) {
+        const int u = __ldg(a.adj + e);
+        if (is_front(u)) { h = true; s_hit = u; }
+      }
+      if (__syncthreads_or(h)) break;
+    }
+    if (threadIdx.x == 0 && s_hit >= 0) bu_commit(a, v, s_hit, ln, depth, parent, fbn);
+    __syncthreads();
+  }
+  // Mid tier: one warp per vertex, early exit by ballot.
+  for (int i = gw; i < nm; i += nw) {
+    const int v = um[i];
+    const int64_t beg = a.off[v], end = a.off[v + 1];
+    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+      const int64_t e = e0 + lane;
+      const int u = e < end ? __ldg(a.adj + e) : -1;
+      const unsigned hm = __ballot_sync(FULL, e < end && is_front(u));
+      if (hm) {
+        const int src = __ffs(hm) - 1;
+        const int pu = __shfl_sync(FULL, u, src);
+        if (lane == 0) bu_commit(a, v, pu, ln, depth, parent, fbn);
+        break;
+      }
+    }
+  }
+  // Small tier: one thread per vertex.
+  for (int64_t i = gtid; i < ns; i += nth) {
+    const int v = us[i];
+    const int64_t beg = a.off[v], end = a.off[v + 1];
+    for (int64_t e = beg; e < end; ++e) {
+      const int u = __ldg(a.adj + e);
+      if (is_front(u)) {
+        bu_commit(a, v, u, ln, depth, parent, fbn);
+        break;
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(BT) k_expand(LevelArgs a) {
+  extern __shared__ int32_t s_hub[];
+  BfsCtl* c = a.ctl;
+  if (c->done) return;
+  const int L = c->level;
+  if (a.hub_slots) {
+    unsigned long long* hn = a.hub[(L + 1) & 1];
+    for (int64_t i = blockIdx.x * (int64_t)BT + threadIdx.x; i < a.hub_slots; i += (int64_t)gridDim.x * BT) hn[i] = 0;
+  }
+  if (c->dir == TD) td_expand(a, c, L, c->depth, c->parent);
+  else bu_expand(a, c, L, c->depth, c->parent, s_hub);
+}
+
+// ----------------------------------------------------------- inspector ----
+// Reads the items of one tile in blocked order: thread t owns items
+// [t*IPT, t*IPT+IPT) of the tile, so per-thread output order = input order.
+__device__ __forceinline__ void load_tile(const int32_t* src, int64_t first, int64_t n, int32_t (&v)[IPT]) {
+  const int64_t i0 = first + (int64_t)threadIdx.x * IPT;
+  if (i0 + IPT <= n && ((((uintptr_t)(src + i0)) & 15) == 0)) {
+    const int4 x = *reinterpret_cast<const int4*>(src + i0);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  } else {
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) v[j] = (i0 + j < n) ? src[i0 + j] : -1;
+  }
+}
+
+template <class T>
+__device__ __forceinline__ T block_sum(T x, T* s_red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) s_red[warp] = x;
+  __syncthreads();
+  T r = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < BT / 32; ++w) r += s_red[w];
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+__device__ __forceinline__ uint32_t acquire_tile(BfsCtl* c, uint32_t* s_tile) {
+  if (threadIdx.x == 0) *s_tile = atomicAdd(&c->tile_ticket, 1u);
+  __syncthreads();
+  const uint32_t t = *s_tile;
+  __syncthreads();
+  return t;
+}
+
+__global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
+  __shared__ uint32_t s_scan[32 * KS];
+  __shared__ uint32_t s_excl[KS];
+  __shared__ uint32_t s_tile;
+  __shared__ int s_last;
+  __shared__ unsigned long long s_red[BT / 32];
+  BfsCtl* c = a.ctl;
+  if (c->done) return;
+  const int L = c->level, dir = c->dir, sweep = c->bu_sweep;
+  const uint32_t epoch = c->epoch;
+  const int qcur = c->qcur, ucur = c->ucur;
+  const int64_t gtid = blockIdx.x * (int64_t)BT + threadIdx.x, nth = (int64_t)gridDim.x * BT;
+  unsigned long long my_n = 0, my_m = 0, my_nu = 0, my_mu = 0;
+  unsigned long long* hub_next = a.hub[(L + 1) & 1];
+  int* err = &c->err;
+
+  if (dir == TD) {
+    // Frontier L is dead: zero its words in fb[L&1] (touching only its vertices).
+    uint32_t* fbo = a.fb[L & 1];
+    for (int k = 0; k < 3; ++k) {
+      const int32_t* qk = a.q[qcur][k];
+      for (int64_t i = gtid; i < c->n_q[k]; i += nth) fbo[(uint32_t)qk[i] >> 5] = 0;
+    }
+    // Classify the raw next frontier into q[qcur^1].
+    const int64_t n = c->n_raw;
+    const uint32_t ntiles = (uint32_t)((n + TILE - 1) / TILE);
+    int32_t* qo[3] = {a.q[qcur ^ 1][0], a.q[qcur ^ 1][1], a.q[qcur ^ 1][2]};
+    int32_t* qco = a.qc[qcur ^ 1];
+    while (true) {
+      const uint32_t tile = acquire_tile(c, &s_tile);
+      if (tile >= ntiles) break;
+      int32_t v[IPT];
+      load_tile(a.raw, (int64_t)tile * TILE, n, v);
+      int dg[IPT], cl[IPT];
+      uint32_t cnt[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int j = 0; j < IPT; ++j) {
+        dg[j] = v[j] >= 0 ? a.deg[v[j]] : 0;
+        cl[j] = v[j] >= 0 ? cls_of(dg[j], a) : -1;
+        if (cl[j] >= 0) {
+          cnt[cl[j]]++;
+          my_m += dg[j];
+          hub_insert(a, hub_next, v[j], dg[j]);
+          if (cl[j] == 2) cnt[3] += (uint32_t)((dg[j] + a.chunk - 1) / a.chunk);
+        }
+      }
+      uint32_t pre[4] = {cnt[0], cnt[1], cnt[2], cnt[3]}, agg[4], excl[4];
+      block_excl_scan<4>(pre, agg, s_scan);
+      lookback<4, KS>(a.tiles, tile, epoch, agg, excl, s_excl, err);
+      uint32_t pos[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) pos[k] = excl[k] + pre[k];
+#pragma unroll
+      for (int j = 0; j < IPT; ++j) {
+        if (cl[j] < 0) continue;
+        qo[cl[j]][pos[cl[j]]++] = v[j];
+        if (cl[j] == 2) {
+          qco[pos[2] - 1] = (int32_t)pos[3];
+          pos[3] += (uint32_t)((dg[j] + a.chunk - 1) / a.chunk);
+        }
+      }
+      if (tile == ntiles - 1 && threadIdx.x == 0) {
+        for (int k = 0; k < 4; ++k) c->tot[k] = excl[k] + agg[k];
+        __threadfence();
+      }
+    }
+  } else {
+    uint32_t* fbo = a.fb[L & 1];
+    const uint32_t* fbn = a.fb[(L + 1) & 1];
+    const int64_t W = (a.V + 31) >> 5;
+    for (int64_t i = gtid; i < W; i += nth) fbo[i] = 0;
+    if (sweep) {
+      // Build the unvisited queues from the status bitmaps (all vertices).
+      const int64_t n = a.V;
+      const uint32_t ntiles = (uint32_t)((n + TILE - 1) / TILE);
+      int32_t* uo[3] = {a.uq[ucur ^ 1][0], a.uq[ucur ^ 1][1], a.uq[ucur ^ 1][2]};
+      while (true) {
+        const uint32_t tile = acquire_tile(c, &s_tile);
+        if (tile >= ntiles) break;
+        const int64_t v0 = (int64_t)tile * TILE + (int64_t)threadIdx.x * IPT;
+        int cl[IPT];
+        uint32_t cnt[3] = {0, 0, 0};
+        uint32_t visw = 0, fnw = 0;
+        if (v0 < n) {
+          visw = ld_cg(a.vis + (v0 >> 5));
+          fnw = ld_cg(fbn + (v0 >> 5));
+        }
+#pragma unroll
+        for (int j = 0; j < IPT; ++j) {
+          const int64_t v = v0 + j;
+          cl[j] = -1;
+          if (v >= n) continue;
+          const int bit = (int)(v & 31);
+          if ((fnw >> bit) & 1u) {
+            const int d = a.deg[v];
+            my_n++;
+            my_m += d;
+            hub_insert(a, hub_next, (int)v, d);
+          } else if (!((visw >> bit) & 1u)) {
+            const int d = a.deg[v];
+            if (d > 0) {
+              cl[j] = cls_of(d, a);
+              cnt[cl[j]]++;
+              my_nu++;
+              my_mu += d;
+            }
+          }
+        }
+        uint32_t pre[3] = {cnt[0], cnt[1], cnt[2]}, agg[3], excl[3];
+        block_excl_scan<3>(pre, agg, s_scan);
+        lookback<3, KS>(a.tiles, tile, epoch, agg, excl, s_excl, err);
+        uint32_t pos[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) pos[k] = excl[k] + pre[k];
+#pragma unroll
+        for (int j = 0; j < IPT; ++j)
+          if (cl[j] >= 0) uo[cl[j]][pos[cl[j]]++] = (int32_t)(v0 + j);
+        if (tile == ntiles - 1 && threadIdx.x == 0) {
+          for (int k = 0; k < 3; ++k) c->tot[k] = excl[k] + agg[k];
+          __threadfence();
+        }
+      }
+    } else {
+      // Partition each unvisited queue: still unvisited -> uq[ucur^1][s];
+      // found this level -> TD queue q[qcur^1][s] (same degree class).
+      uint32_t nt[3], first[3];
+      uint32_t total_tiles = 0;
+      for (int s = 0; s < 3; ++s) {
+        nt[s] = (uint32_t)((c->n_u[s] + TILE - 1) / TILE);
+        first[s] = total_tiles;
+        total_tiles += nt[s];
+      }
+      while (true) {
+        const uint32_t ticket = acquire_tile(c, &s_tile);
+        if (ticket >= total_tiles) break;
+        const int s = ticket >= first[2] && nt[2] ? 2 : (ticket >= first[1] && nt[1] ? 1 : 0);
+        const uint32_t tile = ticket - first[s];
+        const int64_t n = c->n_u[s];
+        int32_t v[IPT];
+        load_tile(a.uq[ucur][s], (int64_t)tile * TILE, n, v);
+        int st[IPT], dg[IPT];
+        uint32_t cnt[3] = {0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < IPT; ++j) {
+          st[j] = -1;
+          dg[j] = 0;
+          if (v[j] < 0) continue;
+          dg[j] = a.deg[v[j]];
+          const bool fnd = (ld_cg(fbn + ((uint32_t)v[j] >> 5)) >> (v[j] & 31)) & 1u;
+          if (fnd) {
+            st[j] = 1;
+            cnt[1]++;
+            if (s == 2) cnt[2] += (uint32_t)((dg[j] + a.chunk - 1) / a.chunk);
+            my_n++;
+            my_m += dg[j];
+            hub_insert(a, hub_next, v[j], dg[j]);
+          } else {
+            st[j] = 0;
+            cnt[0]++;
+            my_nu++;
+            my_mu += dg[j];
+          }
+        }
+        uint32_t pre[3] = {cnt[0], cnt[1], cnt[2]}, agg[3], excl[3];
+        block_excl_scan<3>(pre, agg, s_scan);
+        lookback<3, KS>(a.tiles + (size_t)s * a.seg_tiles * KS, tile, epoch, agg, excl, s_excl, err);
+        uint32_t pos[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) pos[k] = excl[k] + pre[k];
+        int32_t* uo = a.uq[ucur ^ 1][s];
+        int32_t* qo = a.q[qcur ^ 1][s];
+        int32_t* qco = a.qc[qcur ^ 1];
+#pragma unroll
+        for (int j = 0; j < IPT; ++j) {
+          if (st[j] == 0) {
+            uo[pos[0]++] = v[j];
+          } else if (st[j] == 1) {
+            qo[pos[1]++] = v[j];
+            if (s == 2) {
+              qco[pos[1] - 1] = (int32_t)pos[2];
+              pos[2] += (uint32_t)((dg[j] + a.chunk - 1) / a.chunk);
+            }
+          }
+        }
+        if (tile == nt[s] - 1 && threadIdx.x == 0) {
+          for (int k = 0; k < 3; ++k) c->tot[s * KS + k] = excl[k] + agg[k];
+          __threadfence();
+        }
+      }
+    }
+  }
+
+  // Publish this CTA's counters, then the last CTA to finish runs the policy.
+  unsigned long long r;
+  r = block_sum(my_n, s_red);
+  if (threadIdx.x == 0 && r) atomicAdd(&c->acc_n, r);
+  r = block_sum(my_m, s_red);
+  if (threadIdx.x == 0 && r) atomicAdd(&c->acc_m, r);
+  r = block_sum(my_nu, s_red);
+  if (threadIdx.x == 0 && r) atomicAdd(&c->acc_nu, r);
+  r = block_sum(my_mu, s_red);
+  if (threadIdx.x == 0 && r) atomicAdd(&c->acc_mu, r);
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&c->finished, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  volatile BfsCtl* vc = c;
+  const int64_t nf_cur = vc->n_f;
+  int64_t n_next, m_next;
+  int next_dir = dir, next_sweep = 0;
+  if (dir == TD) {
+    n_next = vc->n_raw;
+    m_next = (int64_t)vc->acc_m;
+    vc->td_levels = vc->td_levels + 1;
+    vc->qcur = qcur ^ 1;
+    for (int k = 0; k < 3; ++k) vc->n_q[k] = (int32_t)vc->tot[k];
+    vc->n_chunks = (int32_t)vc->tot[3];
+    const int64_t m_vis = vc->m_vis + m_next;
+    const double m_u = (double)(a.E - m_vis);
+    if (a.policy == ENT_POLICY_BEAMER && (double)m_next > m_u / a.alpha) next_dir = BU;
+    if (a.policy == ENT_POLICY_REFERENCE && (double)m_next >= a.ref_ratio * (double)a.E) next_dir = BU;
+    next_sweep = next_dir == BU;
+  } else if (sweep) {
+    n_next = (int64_t)vc->acc_n;
+    m_next = (int64_t)vc->acc_m;
+    vc->bu_levels = vc->bu_levels + 1;
+    vc->ucur = ucur ^ 1;
+    for (int k = 0; k < 3; ++k) vc->n_u[k] = (int32_t)vc->tot[k];
+    next_dir = BU;
+  } else {
+    n_next = (int64_t)vc->acc_n;
+    m_next = (int64_t)vc->acc_m;
+    vc->bu_levels = vc->bu_levels + 1;
+    const bool to_td = a.policy == ENT_POLICY_BEAMER && (double)n_next < (double)a.V / a.beta && n_next < nf_cur;
+    if (to_td) {
+      next_dir = TD;
+      vc->qcur = qcur ^ 1;
+      for (int s = 0; s < 3; ++s) vc->n_q[s] = (int32_t)vc->tot[s * KS + 1];
+      vc->n_chunks = (int32_t)vc->tot[2 * KS + 2];
+    } else {
+      next_dir = BU;
+      vc->ucur = ucur ^ 1;
+      for (int s = 0; s < 3; ++s) vc->n_u[s] = (int32_t)vc->tot[s * KS + 0];
+    }
+  }
+  vc->n_vis = vc->n_vis + n_next;
+  vc->m_vis = vc->m_vis + m_next;
+  vc->n_f = n_next;
+  vc->m_f = m_next;
+  vc->dir = next_dir;
+  vc->bu_sweep = next_sweep;
+  vc->level = L + 1;
+  int done = n_next == 0;
+  if (L + 1 >= a.max_levels && !done) {
+    vc->err = vc->err | 4;
+    done = 1;
+  }
+  if (vc->n_vis > a.V) {  // a vertex counted twice: stop instead of looping on
+    vc->err = vc->err | 8;
+    done = 1;
+  }
+  vc->done = done;
+  vc->n_raw = 0;
+  vc->acc_n = 0;
+  vc->acc_m = 0;
+  vc->acc_nu = 0;
+  vc->acc_mu = 0;
+  for (int k = 0; k < 3 * KS; ++k) vc->tot[k] = 0;
+  vc->tile_ticket = 0;
+  vc->finished = 0;
+  vc->epoch = epoch + 1;
+  __threadfence();
+  if (a.use_cond) cudaGraphSetConditional(a.cond, done ? 0u : 1u);
+}
+
+// ------------------------------------------------------------- host -------
+struct BfsWorkspace {
+  int device = 0;
+  int64_t V = 0;
+  BfsCtl* ctl = nullptr;
+  BfsCtl* ctl_h = nullptr;  // pinned mirror for stats
+  int32_t* depth = nullptr;
+  int32_t* parent = nullptr;
+  void* slab = nullptr;     // one allocation for all level state
+  LevelArgs args;
+  int grid_reset = 0, grid_expand = 0, grid_inspect = 0;
+  size_t smem_expand = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraphNode_t reset_node = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int kernels_per_iter = 2;
+};
+
+void destroy_bfs_workspace(BfsWorkspace* w) {
+  if (!w) return;
+  if (w->exec) cudaGraphExecDestroy(w->exec);
+  if (w->graph) cudaGraphDestroy(w->graph);
+  if (w->slab) cudaFree(w->slab);
+  if (w->ctl) cudaFree(w->ctl);
+  if (w->ctl_h) cudaFreeHost(w->ctl_h);
+  if (w->depth) cudaFree(w->depth);
+  if (w->parent) cudaFree(w->parent);
+  if (w->ev0) cudaEventDestroy(w->ev0);
+  if (w->ev1) cudaEventDestroy(w->ev1);
+  delete w;
+}
+
+static int build_graph(ent_graph* g, BfsWorkspace* w) {
+  cudaGraph_t graph;
+  ENT_CUDA(cudaGraphCreate(&graph, 0));
+  w->graph = graph;
+  LevelArgs ra = w->args;
+  ra.use_cond = 0;
+  int32_t src0 = 0;
+  int32_t* d0 = w->depth;
+  int32_t* p0 = nullptr;
+  void* rargs[4] = {&ra, &src0, &d0, &p0};
+  cudaKernelNodeParams kp = {};
+  kp.func = (void*)k_reset;
+  kp.gridDim = dim3(w->grid_reset);
+  kp.blockDim = dim3(BT);
+  kp.sharedMemBytes = 0;
+  kp.kernelParams = rargs;
+  ENT_CUDA(cudaGraphAddKernelNode(&w->reset_node, graph, nullptr, 0, &kp));
+  cudaGraphConditionalHandle handle;
+  ENT_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cond_node;
+  ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &w->reset_node, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  LevelArgs la = w->args;
+  la.cond = handle;
+  la.use_cond = 1;
+  ENT_CUDA(cudaStreamBeginCaptureToGraph(g->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  k_expand<<<w->grid_expand, BT, w->smem_expand, g->stream>>>(la);
+  k_inspect<<<w->grid_inspect, BT, 0, g->stream>>>(la);
+  cudaGraph_t captured;
+  cudaError_t e = cudaStreamEndCapture(g->stream, &captured);
+  if (e != cudaSuccess) return fail(ENT_ERR_CUDA, "level-loop capture failed: %s", cudaGetErrorString(e));
+  ENT_CUDA(cudaGraphInstantiate(&w->exec, graph, 0));
+  return ENT_OK;
+}
+
+static int create_workspace(ent_graph* g, BfsWorkspace** out) {
+  BfsWorkspace* w = new BfsWorkspace();
+  w->device = g->device;
+  w->V = g->V;
+  const int64_t V = g->V;
+  const int64_t W = (V + 31) / 32;
+  const int64_t seg_tiles = (V + TILE - 1) / TILE + 1;
+  const ent_bfs_opts& o = g->opts;
+  int hub = o.hub_slots;
+  if (hub > 0 && hub < 16) hub = 16;
+  // Slab layout (all 256-byte aligned): vis, fb0, fb1, q[2][3], qc[2], uq[2][3], raw, hub[2], tiles.
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  size_t sz_bits = al(sizeof(uint32_t) * (W + 1));
+  size_t sz_q = al(sizeof(int32_t) * (V + 4));
+  size_t sz_hub = al(sizeof(unsigned long long) * (hub > 0 ? hub : 1));
+  size_t sz_tiles = al(sizeof(unsigned long long) * 3 * seg_tiles * KS);
+  size_t total = 3 * sz_bits + 15 * sz_q + 2 * sz_hub + sz_tiles;
+  cudaError_t e = cudaMalloc(&w->slab, total);
+  if (e != cudaSuccess) { destroy_bfs_workspace(w); return fail(ENT_ERR_OOM, "workspace allocation (%zu bytes) failed", total); }
+  e = cudaMemset(w->slab, 0, total);
+  if (e == cudaSuccess) e = cudaMalloc(&w->ctl, sizeof(BfsCtl));
+  if (e == cudaSuccess) e = cudaMemset(w->ctl, 0, sizeof(BfsCtl));
+  if (e == cudaSuccess) e = cudaMallocHost(&w->ctl_h, sizeof(BfsCtl));
+  if (e == cudaSuccess) e = cudaMalloc(&w->depth, sizeof(int32_t) * V);
+  if (e == cudaSuccess) e = cudaMalloc(&w->parent, sizeof(int32_t) * V);
+  if (e == cudaSuccess) e = cudaEventCreate(&w->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&w->ev1);
+  if (e != cudaSuccess) { destroy_bfs_workspace(w); return fail(ENT_ERR_OOM, "workspace setup failed: %s", cudaGetErrorString(e)); }
+  char* p = (char*)w->slab;
+  LevelArgs& a = w->args;
+  memset(&a, 0, sizeof(a));
+  a.ctl = w->ctl;
+  a.off = g->off;
+  a.adj = g->adj;
+  a.deg = g->deg;
+  a.V = V;
+  a.E = g->E;
+  a.vis = (uint32_t*)p; p += sz_bits;
+  a.fb[0] = (uint32_t*)p; p += sz_bits;
+  a.fb[1] = (uint32_t*)p; p += sz_bits;
+  for (int i = 0; i < 2; ++i)
+    for (int k = 0; k < 3; ++k) { a.q[i][k] = (int32_t*)p; p += sz_q; }
+  for (int i = 0; i < 2; ++i) { a.qc[i] = (int32_t*)p; p += sz_q; }
+  for (int i = 0; i < 2; ++i)
+    for (int k = 0; k < 3; ++k) { a.uq[i][k] = (int32_t*)p; p += sz_q; }
+  a.raw = (int32_t*)p; p += sz_q;
+  a.hub[0] = (unsigned long long*)p; p += sz_hub;
+  a.hub[1] = (unsigned long long*)p; p += sz_hub;
+  a.tiles = (unsigned long long*)p; p += sz_tiles;
+  a.seg_tiles = seg_tiles;
+  a.small_max = o.small_max;
+  a.large_min = o.large_min;
+  a.chunk = o.chunk_edges;
+  a.hub_slots = hub;
+  int lg = 0;
+  while ((1 << lg) < hub) ++lg;
+  a.hub_shift = 32 - lg;
+  a.hub_min_deg = o.small_max;
+  a.policy = o.policy;
+  a.alpha = o.alpha;
+  a.beta = o.beta;
+  a.ref_ratio = o.ref_ratio;
+  a.max_levels = (int32_t)std::min<int64_t>(V + 2, 0x7ffffff0);
+  w->smem_expand = sizeof(int32_t) * (hub > 0 ? hub : 1);
+  int occ_e = 0, occ_i = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e, k_expand, BT, w->smem_expand);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_i, k_inspect, BT, 0);
+  if (occ_e < 1) occ_e = 1;
+  if (occ_i < 1) occ_i = 1;
+  if (o.blocks_per_sm > 0) occ_e = std::min(occ_e, o.blocks_per_sm);
+  w->grid_expand = g->num_sms * occ_e;
+  w->grid_inspect = g->num_sms * std::min(occ_i, 4);
+  w->grid_reset = g->num_sms * 4;
+  if (o.loop == ENT_LOOP_GRAPH) {
+    int rc = build_graph(g, w);
+    if (rc != ENT_OK) { destroy_bfs_workspace(w); return rc; }
+  }
+  *out = w;
+  return ENT_OK;
+}
+
+int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, cudaStream_t stream, ent_stats* stats) {
+  if (!g->ws) {
+    int rc = create_workspace(g, &g->ws);
+    if (rc != ENT_OK) return rc;
+  }
+  BfsWorkspace* w = g->ws;
+  cudaStream_t s = stream ? stream : g->stream;
+  if (stats) ENT_CUDA(cudaEventRecord(w->ev0, s));
+  if (g->opts.loop == ENT_LOOP_GRAPH) {
+    LevelArgs ra = w->args;
+    ra.use_cond = 0;
+    void* rargs[4] = {&ra, &src, &depth, &parent};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void*)k_reset;
+    kp.gridDim = dim3(w->grid_reset);
+    kp.blockDim = dim3(BT);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = rargs;
+    ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec, w->reset_node, &kp));
+    ENT_CUDA(cudaGraphLaunch(w->exec, s));
+  } else {
+    LevelArgs la = w->args;
+    la.use_cond = 0;
+    k_reset<<<w->grid_reset, BT, 0, s>>>(la, src, depth, parent);
+    g_kernel_launches++;
+    ENT_CUDA(cudaGetLastError());
+    int32_t* done_h = &w->ctl_h->done;
+    for (int64_t it = 0;; ++it) {
+      k_expand<<<w->grid_expand, BT, w->smem_expand, s>>>(la);
+      k_inspect<<<w->grid_inspect, BT, 0, s>>>(la);
+      g_kernel_launches += 2;
+      ENT_CUDA(cudaGetLastError());
+      ENT_CUDA(cudaMemcpyAsync(done_h, &w->ctl->done, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      ENT_CUDA(cudaStreamSynchronize(s));
+      if (*done_h) break;
+      if (it > w->V + 2) return fail(ENT_ERR_INTERNAL, "level loop did not terminate");
+    }
+  }
+  if (stats) {
+    ENT_CUDA(cudaEventRecord(w->ev1, s));
+    ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));
+    ENT_CUDA(cudaStreamSynchronize(s));
+    const BfsCtl& h = *w->ctl_h;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, w->ev0, w->ev1);
+    stats->reached_vertices = h.n_vis;
+    stats->traversed_edges = h.m_vis;
+    stats->levels = h.level;
+    stats->td_levels = h.td_levels;
+    stats->bu_levels = h.bu_levels;
+    stats->status = h.err;
+    stats->device_ms = ms;
+    if (g->opts.loop == ENT_LOOP_GRAPH) g_kernel_launches += 1 + 2 * (int64_t)h.level;
+    if (h.err) return fail(ENT_ERR_TIMEOUT, "device traversal reported error flags 0x%x", h.err);
+  } else if (g->opts.loop == ENT_LOOP_GRAPH) {
+    g_kernel_launches += 1;  // level kernels are counted when stats are read
+  }
+  return ENT_OK;
+}
+
+}  // namespace ent
+
+using namespace ent;
+
+extern "C" {
+
+int ent_bfs_device(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* parent_dev, void* stream, ent_stats* stats) {
+  clear_error();
+  if (!g || !depth_dev) return fail(ENT_ERR_INVALID_ARG, "null argument");
+  if (src < 0 || src >= g->V) return fail(ENT_ERR_INVALID_ARG, "source %d out of range [0,%lld)", src, (long long)g->V);
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard dg(g->device);
+  return run_bfs_single(g, src, depth_dev, parent_dev, (cudaStream_t)stream, stats);
+}
+
+int ent_bfs(ent_graph* g, int32_t src, int32_t* depth_out, int32_t* parent_out, ent_stats* stats) {
+  clear_error();
+  if (!g) return fail(ENT_ERR_INVALID_ARG, "null graph");
+  if (src < 0 || src >= g->V) return fail(ENT_ERR_INVALID_ARG, "source %d out of range [0,%lld)", src, (long long)g->V);
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard dg(g->device);
+  if (!g->ws) {
+    int rc = create_workspace(g, &g->ws);
+    if (rc != ENT_OK) return rc;
+  }
+  BfsWorkspace* w = g->ws;
+  ent_stats local;
+  int rc = run_bfs_single(g, src, w->depth, parent_out ? w->parent : nullptr, g->stream, stats ? stats : &local);
+  if (rc != ENT_OK) return rc;
+  if (depth_out)
+    ENT_CUDA(cudaMemcpyAsync(depth_out, w->depth, sizeof(int32_t) * g->V, cudaMemcpyDeviceToHost, g->stream));
+  if (parent_out)
+    ENT_CUDA(cudaMemcpyAsync(parent_out, w->parent, sizeof(int32_t) * g->V, cudaMemcpyDeviceToHost, g->stream));
+  ENT_CUDA(cudaStreamSynchronize(g->stream));
+  return ENT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,65 @@
+// Device-resident graph handle and the traversal workspaces hanging off it.
+#pragma once
+#include <cuda_runtime.h>
+#include <mutex>
+#include <stdint.h>
+#include "ent_internal.h"
+
+namespace ent {
+struct BfsWorkspace;    // single-source direction-optimising traversal
+struct BatchWorkspace;  // bitwise multi-source traversal
+void destroy_bfs_workspace(BfsWorkspace* w);
+void destroy_batch_workspace(BatchWorkspace* w);
+}  // namespace ent
+
+// Device memory layout of one graph (all on `device`):
+//   off  int64[V+1]   row offsets (reference strt_pos + adj_card, allocator.cuh:107-114)
+//   adj  int32[E]     column ids, rows ascending (reference adj_list, allocator.cuh:116-120)
+//   deg  int32[V]     degrees, read by the classifier (reference adj_card)
+struct ent_graph {
+  int device = 0;
+  int num_sms = 0;
+  int64_t V = 0, E = 0;
+  int64_t* off = nullptr;
+  int32_t* adj = nullptr;
+  int32_t* deg = nullptr;
+  cudaStream_t stream = nullptr;
+  ent_bfs_opts opts;
+  std::mutex mu;
+  ent::BfsWorkspace* ws = nullptr;
+  ent::BatchWorkspace* bws = nullptr;
+};
+
+namespace ent {
+
+// RAII device guard: switches to `dev`, restores the previous device.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+#define ENT_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t _e = (call);                                                                \
+    if (_e != cudaSuccess)                                                                  \
+      return ::ent::fail(_e == cudaErrorMemoryAllocation ? ENT_ERR_OOM : ENT_ERR_CUDA,      \
+                         "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__, \
+                         __LINE__);                                                         \
+  } while (0)
+
+int graph_alloc(ent_graph* g, int64_t V, int64_t E);
+int graph_finish(ent_graph* g);  // computes deg, creates stream
+int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* parent_dev, cudaStream_t stream,
+                   ent_stats* stats);
+int run_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, cudaStream_t stream,
+                  ent_stats* stats);
+
+}  // namespace ent

@@ -1,0 +1,377 @@
+// Device graph: upload (replaces allocator<>::alloc_array, allocator.cuh:35-150),
+// on-GPU generation of the seeded synthetic graphs, download and teardown.
+//
+// The GPU builder produces exactly the CSR of the host builder
+// (host_graph.cpp): the same counter-based edge draws, then a radix sort of
+// packed (u, v) keys, duplicate removal and offset search. Sorting uses CUB
+// (graph construction only; it is not on the traversal path).
+#include <cub/cub.cuh>
+#include <string.h>
+#include <omp.h>
+#include <vector>
+
+#include "dev_graph.h"
+#include "gen_common.h"
+
+namespace ent {
+
+RmatParams make_rmat_params(int scale, int ef, double a, double b, double c, uint64_t seed);
+GridParams make_grid_params(int64_t w, int64_t h, double drop, uint64_t seed);
+ErParams make_er_params(int64_t n, double mean_degree, uint64_t seed);
+
+__global__ void k_degrees(const int64_t* __restrict__ off, int32_t* __restrict__ deg, int64_t V) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x)
+    deg[v] = (int32_t)(off[v + 1] - off[v]);
+}
+
+int graph_alloc(ent_graph* g, int64_t V, int64_t E) {
+  g->V = V;
+  g->E = E;
+  ENT_CUDA(cudaMalloc(&g->off, sizeof(int64_t) * (V + 1)));
+  ENT_CUDA(cudaMalloc(&g->adj, sizeof(int32_t) * (E > 0 ? E : 1)));
+  ENT_CUDA(cudaMalloc(&g->deg, sizeof(int32_t) * V));
+  return ENT_OK;
+}
+
+int graph_finish(ent_graph* g) {
+  ENT_CUDA(cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device));
+  if (!g->stream) ENT_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+  int blocks = (int)std::min<int64_t>((g->V + 255) / 256, (int64_t)g->num_sms * 16);
+  k_degrees<<<blocks, 256, 0, g->stream>>>(g->off, g->deg, g->V);
+  g_kernel_launches++;
+  ENT_CUDA(cudaGetLastError());
+  ENT_CUDA(cudaStreamSynchronize(g->stream));
+  ent_bfs_opts_default(&g->opts);
+  return ENT_OK;
+}
+
+static void graph_free(ent_graph* g) {
+  if (!g) return;
+  DeviceGuard dg(g->device);
+  if (g->ws) destroy_bfs_workspace(g->ws);
+  if (g->bws) destroy_batch_workspace(g->bws);
+  if (g->off) cudaFree(g->off);
+  if (g->adj) cudaFree(g->adj);
+  if (g->deg) cudaFree(g->deg);
+  if (g->stream) cudaStreamDestroy(g->stream);
+  delete g;
+}
+
+// ----------------------------------------------------------- generators ---
+// Key layout: (u << b) | v with b = ceil_log2(V); dropped draws and self
+// loops get the sentinel (V << b), which sorts after every real key.
+struct KeyCodec {
+  int b;
+  uint64_t V;
+  __host__ __device__ uint64_t pack(uint64_t u, uint64_t v) const { return (u << b) | v; }
+  __host__ __device__ uint64_t sentinel() const { return V << b; }
+};
+
+template <class Draw>
+__global__ void k_gen_keys(Draw draw, uint64_t n_draws, KeyCodec kc, uint64_t* __restrict__ keys) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_draws; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t u, v;
+    bool keep = draw(i, &u, &v);
+    if (!keep || u == v) {
+      keys[2 * i] = kc.sentinel();
+      keys[2 * i + 1] = kc.sentinel();
+    } else {
+      keys[2 * i] = kc.pack(u, v);
+      keys[2 * i + 1] = kc.pack(v, u);
+    }
+  }
+}
+
+__global__ void k_offsets_from_keys(const uint64_t* __restrict__ keys, int64_t n, KeyCodec kc, int64_t* __restrict__ off,
+                                    int64_t V) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r <= V; r += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t target = (uint64_t)r << kc.b;
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if (keys[mid] < target) lo = mid + 1; else hi = mid;
+    }
+    off[r] = lo;
+  }
+}
+
+__global__ void k_adj_from_keys(const uint64_t* __restrict__ keys, int64_t n, uint64_t mask, int32_t* __restrict__ adj) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    adj[i] = (int32_t)(keys[i] & mask);
+}
+
+struct RmatDraw {
+  RmatParams rp;
+  __device__ bool operator()(uint64_t i, uint64_t* u, uint64_t* v) const {
+    uint64_t x, y;
+    rmat_edge(rp, i, &x, &y);
+    *u = perm_pow2(rp.perm, x);
+    *v = perm_pow2(rp.perm, y);
+    return true;
+  }
+};
+struct GridDraw {
+  GridParams gp;
+  __device__ bool operator()(uint64_t e, uint64_t* u, uint64_t* v) const {
+    uint64_t x, y;
+    bool keep = grid_edge(gp, e, &x, &y);
+    *u = perm_apply(gp.perm, gp.n, x);
+    *v = perm_apply(gp.perm, gp.n, y);
+    return keep;
+  }
+};
+struct ErDraw {
+  ErParams ep;
+  __device__ bool operator()(uint64_t i, uint64_t* u, uint64_t* v) const {
+    uint64_t x, y;
+    er_edge(ep, i, &x, &y);
+    *u = perm_apply(ep.perm, ep.n, x);
+    *v = perm_apply(ep.perm, ep.n, y);
+    return true;
+  }
+};
+
+template <class Draw>
+static int build_on_device(Draw draw, uint64_t n_draws, int64_t V, int gpu, ent_graph** out) {
+  DeviceGuard dg(gpu);
+  ent_graph* g = new ent_graph();
+  g->device = gpu;
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, gpu);
+  cudaStream_t s;
+  if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+    delete g;
+    return fail(ENT_ERR_CUDA, "stream create failed");
+  }
+  g->stream = s;
+  KeyCodec kc;
+  kc.V = (uint64_t)V;
+  kc.b = ceil_log2((uint64_t)V + 1);
+  int end_bit = 2 * kc.b + 1;
+  if (end_bit > 64) { graph_free(g); return fail(ENT_ERR_UNSUPPORTED, "graph too large for packed keys"); }
+  int64_t n_keys = (int64_t)(2 * n_draws);
+  uint64_t *k0 = nullptr, *k1 = nullptr;
+  void* tmp = nullptr;
+  size_t tmp_bytes = 0, tmp2 = 0;
+  int64_t* d_nsel = nullptr;
+  int rc = ENT_OK;
+  auto cleanup = [&]() {
+    if (k0) cudaFree(k0);
+    if (k1) cudaFree(k1);
+    if (tmp) cudaFree(tmp);
+    if (d_nsel) cudaFree(d_nsel);
+  };
+#define GEN_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t _e = (call);                                                                    \
+    if (_e != cudaSuccess) {                                                                    \
+      rc = fail(_e == cudaErrorMemoryAllocation ? ENT_ERR_OOM : ENT_ERR_CUDA, "%s: %s", #call, \
+                cudaGetErrorString(_e));                                                        \
+      cleanup();                                                                                \
+      graph_free(g);                                                                            \
+      return rc;                                                                                \
+    }                                                                                           \
+  } while (0)
+  GEN_CUDA(cudaMalloc(&k0, sizeof(uint64_t) * std::max<int64_t>(n_keys, 1)));
+  GEN_CUDA(cudaMalloc(&k1, sizeof(uint64_t) * std::max<int64_t>(n_keys, 1)));
+  GEN_CUDA(cudaMalloc(&d_nsel, sizeof(int64_t)));
+  int blocks = nsm * 16;
+  k_gen_keys<<<blocks, 256, 0, s>>>(draw, n_draws, kc, k0);
+  g_kernel_launches++;
+  GEN_CUDA(cudaGetLastError());
+  cub::DoubleBuffer<uint64_t> db(k0, k1);
+  GEN_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, db, n_keys, 0, end_bit, s));
+  GEN_CUDA(cub::DeviceSelect::Unique(nullptr, tmp2, k0, k1, d_nsel, n_keys, s));
+  tmp_bytes = std::max(tmp_bytes, tmp2);
+  GEN_CUDA(cudaMalloc(&tmp, tmp_bytes));
+  GEN_CUDA(cub::DeviceRadixSort::SortKeys(tmp, tmp_bytes, db, n_keys, 0, end_bit, s));
+  uint64_t* sorted = db.Current();
+  uint64_t* uniq = db.Alternate();
+  GEN_CUDA(cub::DeviceSelect::Unique(tmp, tmp_bytes, sorted, uniq, d_nsel, n_keys, s));
+  int64_t n_uniq = 0;
+  GEN_CUDA(cudaMemcpyAsync(&n_uniq, d_nsel, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  GEN_CUDA(cudaStreamSynchronize(s));
+  // Drop the sentinel (at most one survives Unique, and it sorts last).
+  if (n_uniq > 0) {
+    uint64_t last = 0;
+    GEN_CUDA(cudaMemcpy(&last, uniq + n_uniq - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    if (last == kc.sentinel()) --n_uniq;
+  }
+  if (graph_alloc(g, V, n_uniq) != ENT_OK) {
+    rc = fail(ENT_ERR_OOM, "device allocation failed for graph (V=%lld E=%lld)", (long long)V, (long long)n_uniq);
+    cleanup();
+    graph_free(g);
+    return rc;
+  }
+  k_offsets_from_keys<<<blocks, 256, 0, s>>>(uniq, n_uniq, kc, g->off, V);
+  k_adj_from_keys<<<blocks, 256, 0, s>>>(uniq, n_uniq, (1ull << kc.b) - 1, g->adj);
+  g_kernel_launches += 2;
+  GEN_CUDA(cudaGetLastError());
+  GEN_CUDA(cudaStreamSynchronize(s));
+  cleanup();
+  k0 = k1 = nullptr;
+  tmp = nullptr;
+  d_nsel = nullptr;
+  rc = graph_finish(g);
+  if (rc != ENT_OK) { graph_free(g); return rc; }
+  *out = g;
+  return ENT_OK;
+#undef GEN_CUDA
+}
+
+}  // namespace ent
+
+using namespace ent;
+
+extern "C" {
+
+void ent_bfs_opts_default(ent_bfs_opts* o) {
+  if (!o) return;
+  o->policy = ENT_POLICY_BEAMER;
+  o->loop = ENT_LOOP_GRAPH;
+  o->alpha = 14.0;
+  o->beta = 24.0;
+  o->ref_ratio = 0.3;
+  o->small_max = 32;
+  o->large_min = 1024;
+  o->hub_slots = 1024;
+  o->chunk_edges = 2048;
+  o->blocks_per_sm = 0;
+}
+
+int ent_graph_create(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E, int32_t gpu, ent_graph** out) {
+  clear_error();
+  if (!beg || (!csr && E > 0) || !out || V < 1 || E < 0) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
+  *out = nullptr;
+  if (V >= (1ll << 31) - 1) return fail(ENT_ERR_UNSUPPORTED, "V=%lld exceeds int32 ids", (long long)V);
+  if (beg[0] != 0 || beg[V] != E) return fail(ENT_ERR_FORMAT, "beg_pos[0] must be 0 and beg_pos[V] must equal E");
+  int64_t bad = -1;
+#pragma omp parallel for reduction(max : bad)
+  for (int64_t i = 0; i < V; ++i)
+    if (beg[i + 1] < beg[i]) bad = std::max(bad, i);
+  if (bad >= 0) return fail(ENT_ERR_FORMAT, "beg_pos not monotone at %lld", (long long)bad);
+#pragma omp parallel for reduction(max : bad)
+  for (int64_t k = 0; k < E; ++k)
+    if (csr[k] < 0 || csr[k] >= V) bad = std::max(bad, k);
+  if (bad >= 0) return fail(ENT_ERR_FORMAT, "csr entry %lld out of range [0,V)", (long long)bad);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(ENT_ERR_CUDA, "no CUDA device available");
+  if (gpu < 0 || gpu >= ndev) return fail(ENT_ERR_INVALID_ARG, "gpu_id %d out of range (%d devices)", gpu, ndev);
+  DeviceGuard dg(gpu);
+  ent_graph* g = new ent_graph();
+  g->device = gpu;
+  int rc = graph_alloc(g, V, E);
+  if (rc != ENT_OK) { graph_free(g); return rc; }
+  cudaError_t e1 = cudaMemcpy(g->off, beg, sizeof(int64_t) * (V + 1), cudaMemcpyHostToDevice);
+  cudaError_t e2 = E > 0 ? cudaMemcpy(g->adj, csr, sizeof(int32_t) * E, cudaMemcpyHostToDevice) : cudaSuccess;
+  if (e1 != cudaSuccess || e2 != cudaSuccess) {
+    graph_free(g);
+    return fail(ENT_ERR_CUDA, "CSR upload failed");
+  }
+  rc = graph_finish(g);
+  if (rc != ENT_OK) { graph_free(g); return rc; }
+  *out = g;
+  return ENT_OK;
+}
+
+int ent_graph_from_csr(const ent_csr* c, int32_t gpu, ent_graph** out) {
+  if (!c) return fail(ENT_ERR_INVALID_ARG, "null csr");
+  return ent_graph_create(c->off.data(), c->adj.data(), c->V, c->E, gpu, out);
+}
+
+static int check_gpu(int gpu) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(ENT_ERR_CUDA, "no CUDA device available");
+  if (gpu < 0 || gpu >= ndev) return fail(ENT_ERR_INVALID_ARG, "gpu_id %d out of range", gpu);
+  return ENT_OK;
+}
+
+int ent_graph_gen_rmat(int32_t scale, int32_t ef, double a, double b, double c, uint64_t seed, int32_t gpu,
+                       ent_graph** out) {
+  clear_error();
+  if (!out || scale < 1 || scale > 30 || ef < 1 || a < 0 || b < 0 || c < 0 || a + b + c > 1.0)
+    return fail(ENT_ERR_INVALID_ARG, "bad R-MAT parameters");
+  int rc = check_gpu(gpu);
+  if (rc) return rc;
+  RmatDraw d{make_rmat_params(scale, ef, a, b, c, seed)};
+  return build_on_device(d, d.rp.n_edges, 1ll << scale, gpu, out);
+}
+
+int ent_graph_gen_grid(int64_t w, int64_t h, double drop, uint64_t seed, int32_t gpu, ent_graph** out) {
+  clear_error();
+  if (!out || w < 2 || h < 2 || drop < 0 || drop > 1 || w * h >= (1ll << 31) - 1)
+    return fail(ENT_ERR_INVALID_ARG, "bad grid parameters");
+  int rc = check_gpu(gpu);
+  if (rc) return rc;
+  GridDraw d{make_grid_params(w, h, drop, seed)};
+  return build_on_device(d, d.gp.n_edges, (int64_t)d.gp.n, gpu, out);
+}
+
+int ent_graph_gen_er(int64_t n, double mean_degree, uint64_t seed, int32_t gpu, ent_graph** out) {
+  clear_error();
+  if (!out || n < 2 || n >= (1ll << 31) - 1 || mean_degree < 0) return fail(ENT_ERR_INVALID_ARG, "bad ER parameters");
+  int rc = check_gpu(gpu);
+  if (rc) return rc;
+  ErDraw d{make_er_params(n, mean_degree, seed)};
+  return build_on_device(d, d.ep.n_edges, n, gpu, out);
+}
+
+int64_t ent_graph_vert_count(const ent_graph* g) { return g ? g->V : -1; }
+int64_t ent_graph_edge_count(const ent_graph* g) { return g ? g->E : -1; }
+
+int ent_graph_download(const ent_graph* g, int64_t* beg, int32_t* csr) {
+  clear_error();
+  if (!g || !beg || (!csr && g->E > 0)) return fail(ENT_ERR_INVALID_ARG, "null argument");
+  DeviceGuard dg(g->device);
+  ENT_CUDA(cudaMemcpy(beg, g->off, sizeof(int64_t) * (g->V + 1), cudaMemcpyDeviceToHost));
+  if (g->E > 0) ENT_CUDA(cudaMemcpy(csr, g->adj, sizeof(int32_t) * g->E, cudaMemcpyDeviceToHost));
+  return ENT_OK;
+}
+
+int ent_graph_device_csr(const ent_graph* g, const int64_t** beg, const int32_t** csr) {
+  if (!g || !beg || !csr) return fail(ENT_ERR_INVALID_ARG, "null argument");
+  *beg = g->off;
+  *csr = g->adj;
+  return ENT_OK;
+}
+
+int ent_graph_set_opts(ent_graph* g, const ent_bfs_opts* o) {
+  clear_error();
+  if (!g || !o) return fail(ENT_ERR_INVALID_ARG, "null argument");
+  if (o->policy < 0 || o->policy > 3) return fail(ENT_ERR_INVALID_ARG, "unknown policy %d", o->policy);
+  if (o->loop < 0 || o->loop > 1) return fail(ENT_ERR_INVALID_ARG, "unknown loop mode %d", o->loop);
+  if (o->small_max < 1 || o->large_min < o->small_max) return fail(ENT_ERR_INVALID_ARG, "need 1 <= small_max <= large_min");
+  if (o->hub_slots < 0 || o->hub_slots > 4096 || (o->hub_slots & (o->hub_slots - 1)))
+    return fail(ENT_ERR_INVALID_ARG, "hub_slots must be 0 or a power of two <= 4096");
+  if (o->chunk_edges < 32) return fail(ENT_ERR_INVALID_ARG, "chunk_edges must be >= 32");
+  if (o->alpha <= 0 || o->beta <= 0 || o->ref_ratio < 0) return fail(ENT_ERR_INVALID_ARG, "alpha/beta must be > 0");
+  if (o->blocks_per_sm < 0 || o->blocks_per_sm > 32) return fail(ENT_ERR_INVALID_ARG, "blocks_per_sm out of range");
+  std::lock_guard<std::mutex> lk(g->mu);
+  g->opts = *o;
+  if (g->ws) {  // workspace graphs were captured with the old options
+    DeviceGuard dg(g->device);
+    cudaStreamSynchronize(g->stream);
+    destroy_bfs_workspace(g->ws);
+    g->ws = nullptr;
+  }
+  return ENT_OK;
+}
+
+int ent_graph_get_opts(const ent_graph* g, ent_bfs_opts* o) {
+  if (!g || !o) return fail(ENT_ERR_INVALID_ARG, "null argument");
+  *o = g->opts;
+  return ENT_OK;
+}
+
+int ent_graph_destroy(ent_graph* g) {
+  clear_error();
+  if (!g) return ENT_OK;
+  {
+    DeviceGuard dg(g->device);
+    if (g->stream) cudaStreamSynchronize(g->stream);
+  }
+  graph_free(g);
+  return ENT_OK;
+}
+
+}  // extern "C"

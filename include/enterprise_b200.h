@@ -1,0 +1,198 @@
+/*
+ * enterprise_b200 — C ABI of the B200-native (sm_100a) breadth-first search.
+ *
+ * This is the drop-in boundary for Enterprise's GPU BFS. The reference
+ * exposes one host entry point,
+ *     template<vertex_t,index_t> int bfs_gpu_coalescing_mem(
+ *         vertex_t* src_list, index_t* beg_pos, vertex_t* csr,
+ *         index_t vert_count, index_t edge_count, index_t gpu_id)
+ * (bfs_gpu_opt.cuh:293-300), fed by the CSR loader graph<...>::graph
+ * (graph.hpp:33-118) and called from main.cu:80-86. That function uploads
+ * the CSR (allocator.cuh:35-150), runs 64 BFS traversals and only prints.
+ * Here the same work is split into explicit steps a foreign-function layer
+ * can bind: load / create a device graph, run one or many traversals,
+ * read depths (and optionally parents) back, destroy.
+ *
+ * Conventions
+ *  - Every function returns an int status (ENT_OK == 0). Nothing calls
+ *    exit(); the reference's H_ERR (comm.h:34-45) aborted the process.
+ *    ent_last_error() returns a thread-local message for the last failure.
+ *  - Host arrays passed in are borrowed (read-only, never freed).
+ *  - Depths are int32; unreached vertices hold -1 (all ones, mirroring the
+ *    reference's INFTY = 0xFF for its uint8 depth_t, comm.h:69, comm.h:131).
+ *  - Parents are int32; parent[src] == src; unreached vertices hold -1.
+ *  - A graph handle owns its device memory. Calls on one handle are
+ *    serialised internally; distinct handles may be used from different
+ *    host threads.
+ *  - Vertex ids are int32 (V < 2^31). Offsets are int64 (E may exceed 2^31).
+ */
+#ifndef ENTERPRISE_B200_H
+#define ENTERPRISE_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ENT_ABI_VERSION 1
+
+enum ent_status {
+  ENT_OK = 0,
+  ENT_ERR_INVALID_ARG = 1,
+  ENT_ERR_CUDA = 2,
+  ENT_ERR_OOM = 3,
+  ENT_ERR_IO = 4,
+  ENT_ERR_FORMAT = 5,
+  ENT_ERR_TIMEOUT = 6,
+  ENT_ERR_INTERNAL = 7,
+  ENT_ERR_UNSUPPORTED = 8,
+  ENT_ERR_ADMISSION = 9
+};
+
+/* Direction policy (reference rule: inspector.cuh:486-521). */
+enum ent_policy {
+  ENT_POLICY_BEAMER = 0,    /* alpha/beta direction switching, both ways  */
+  ENT_POLICY_REFERENCE = 1, /* TD->BU once when frontier edges >= ratio*E */
+  ENT_POLICY_TD_ONLY = 2,   /* top-down every level                       */
+  ENT_POLICY_BU_ONLY = 3    /* bottom-up every level                      */
+};
+
+/* How the level loop is driven. */
+enum ent_loop {
+  ENT_LOOP_GRAPH = 0, /* whole traversal = one CUDA graph launch with a
+                         device-side while node (no host round trip)   */
+  ENT_LOOP_HOST = 1   /* host launches each level and polls a flag     */
+};
+
+typedef struct ent_bfs_opts {
+  int32_t policy;        /* enum ent_policy                                */
+  int32_t loop;          /* enum ent_loop                                  */
+  double alpha;          /* Beamer: TD->BU when m_f > m_u / alpha          */
+  double beta;           /* Beamer: BU->TD when n_f < V / beta (shrinking) */
+  double ref_ratio;      /* reference rule ratio (0.3, inspector.cuh:497)  */
+  int32_t small_max;     /* degree <  small_max -> thread tier (ref 32)    */
+  int32_t large_min;     /* degree >  large_min -> CTA tier (ref 1024)     */
+  int32_t hub_slots;     /* shared-memory hub cache slots, power of two,
+                            0 disables (ref 1536/1920, comm.h:176-177)     */
+  int32_t chunk_edges;   /* edges per CTA chunk of a large TD vertex       */
+  int32_t blocks_per_sm; /* resident CTAs per SM for the level kernels,
+                            0 = occupancy maximum                          */
+} ent_bfs_opts;
+
+typedef struct ent_stats {
+  int64_t reached_vertices; /* reference report(): agg_tr_v (validate.h:106-127) */
+  int64_t traversed_edges;  /* reference report(): agg_tr_edges = sum of degrees of
+                               reached vertices (directed CSR entries)           */
+  int32_t levels;           /* number of non-empty levels = max depth + 1         */
+  int32_t td_levels;        /* levels expanded top-down                           */
+  int32_t bu_levels;        /* levels expanded bottom-up                          */
+  int32_t status;           /* device status word (0 ok)                          */
+  double device_ms;         /* CUDA-event time of the traversal on the device     */
+} ent_stats;
+
+typedef struct ent_graph ent_graph; /* device-resident CSR + traversal state */
+typedef struct ent_csr ent_csr;     /* host-resident CSR owned by the library */
+
+/* ---------------------------------------------------------------- misc --- */
+const char* ent_last_error(void);
+int ent_abi_version(void);
+void ent_bfs_opts_default(ent_bfs_opts* opts);
+/* Number of kernels this library has launched in this process (all devices). */
+int64_t ent_kernel_launch_count(void);
+
+/* ------------------------------------------------------- host CSR ------- */
+/* Replaces graph<long,long,double,int,int,double>(beg,csr,NULL)
+ * (graph.hpp:33-118): reads <X>_beg_pos.bin (int64[V+1]) and <X>_csr.bin.
+ * The csr file may hold int64 (the reference's format, graph.hpp:46-47) or
+ * int32 entries; the width is detected from file size vs beg_pos[V].
+ * Offsets are validated (monotone, beg_pos[0]==0) and ids checked < V. */
+int ent_csr_load(const char* beg_pos_path, const char* csr_path, ent_csr** out);
+/* Writes the reference's int64 format (both files int64). */
+int ent_csr_save(const ent_csr* g, const char* beg_pos_path, const char* csr_path);
+/* Builds a CSR from caller arrays (copied). */
+int ent_csr_from_arrays(const int64_t* beg_pos, const int32_t* csr, int64_t vert_count,
+                        int64_t edge_count, ent_csr** out);
+/* Builds a canonical undirected CSR from an edge list: both directions added,
+ * self loops and duplicates removed, rows sorted ascending. */
+int ent_csr_from_edges(const int64_t* src, const int64_t* dst, int64_t n_edges,
+                       int64_t vert_count, ent_csr** out);
+int64_t ent_csr_vert_count(const ent_csr* g);
+int64_t ent_csr_edge_count(const ent_csr* g);
+const int64_t* ent_csr_beg_pos(const ent_csr* g);
+const int32_t* ent_csr_adj(const ent_csr* g);
+void ent_csr_free(ent_csr* g);
+
+/* Seeded generators on the host (OpenMP). Output: canonical undirected CSR
+ * with vertex ids scrambled by a seeded bijection. */
+int ent_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c,
+                 uint64_t seed, ent_csr** out);
+int ent_gen_grid(int64_t width, int64_t height, double drop_prob, uint64_t seed,
+                 ent_csr** out);
+int ent_gen_er(int64_t vert_count, double mean_degree, uint64_t seed, ent_csr** out);
+/* Seeded distinct non-isolated sources (count <= number of such vertices). */
+int ent_pick_sources(const int64_t* beg_pos, int64_t vert_count, uint64_t seed,
+                     int32_t count, int32_t* out);
+/* The reference's source rule (main.cu:55-78): glibc rand()%V from the
+ * process's current rand() state, distinct, non-isolated. */
+int ent_pick_sources_compat(const int64_t* beg_pos, int64_t vert_count, int32_t count,
+                            int32_t* out);
+
+/* ------------------------------------------------------- device graph --- */
+/* Uploads a CSR to GPU `gpu_id` and allocates traversal state
+ * (replaces allocator<>::alloc_array, allocator.cuh:35-150). */
+int ent_graph_create(const int64_t* beg_pos, const int32_t* csr, int64_t vert_count,
+                     int64_t edge_count, int32_t gpu_id, ent_graph** out);
+int ent_graph_from_csr(const ent_csr* g, int32_t gpu_id, ent_graph** out);
+/* Generates a graph directly on the GPU (same edges as the host generators,
+ * bit-identical CSR). */
+int ent_graph_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c,
+                       uint64_t seed, int32_t gpu_id, ent_graph** out);
+int ent_graph_gen_grid(int64_t width, int64_t height, double drop_prob, uint64_t seed,
+                       int32_t gpu_id, ent_graph** out);
+int ent_graph_gen_er(int64_t vert_count, double mean_degree, uint64_t seed,
+                     int32_t gpu_id, ent_graph** out);
+int64_t ent_graph_vert_count(const ent_graph* g);
+int64_t ent_graph_edge_count(const ent_graph* g);
+/* Copies the device CSR to caller host arrays (V+1 and E entries). */
+int ent_graph_download(const ent_graph* g, int64_t* beg_pos, int32_t* csr);
+/* Device pointers of the resident CSR (for callers that keep work on GPU). */
+int ent_graph_device_csr(const ent_graph* g, const int64_t** beg_pos_dev,
+                         const int32_t** csr_dev);
+int ent_graph_set_opts(ent_graph* g, const ent_bfs_opts* opts);
+int ent_graph_get_opts(const ent_graph* g, ent_bfs_opts* opts);
+int ent_graph_destroy(ent_graph* g);
+
+/* ------------------------------------------------------- traversal ------ */
+/* One direction-optimising BFS from `src`. depth_out / parent_out are HOST
+ * arrays of V int32 (either may be NULL). stats may be NULL. */
+int ent_bfs(ent_graph* g, int32_t src, int32_t* depth_out, int32_t* parent_out,
+            ent_stats* stats);
+/* Same traversal; results stay on the device. depth_dev / parent_dev are
+ * device arrays of V int32 on the graph's GPU (parent_dev may be NULL).
+ * The call is asynchronous on `stream` (a cudaStream_t, NULL = the graph's
+ * own stream) unless stats is non-NULL, which synchronises. */
+int ent_bfs_device(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* parent_dev,
+                   void* stream, ent_stats* stats);
+
+/* Many sources at once with bitwise frontiers (one bit per source per vertex
+ * in a shared status word). depth_out: HOST array n_src x V int32, source-major
+ * (row s is the depth array of src[s]); may be NULL. stats: n_src entries or
+ * NULL. Depths are identical to n_src calls of ent_bfs. */
+int ent_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_out,
+                  ent_stats* stats);
+/* Batched traversal with device-resident output (n_src x V int32 on the GPU). */
+int ent_bfs_batch_device(ent_graph* g, const int32_t* src, int32_t n_src,
+                         int32_t* depth_dev, void* stream, ent_stats* stats);
+
+/* Many graphs of uneven sizes in one launch: graphs[k] gets n_src[k] sources
+ * from src (concatenated). depth_out[k] is a HOST array n_src[k] x V_k or
+ * NULL. All graphs must live on the same GPU. */
+int ent_bfs_multi(ent_graph* const* graphs, int32_t n_graphs, const int32_t* src,
+                  const int32_t* n_src, int32_t* const* depth_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ENTERPRISE_B200_H */
