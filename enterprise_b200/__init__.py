@@ -60,6 +60,14 @@ class _Stats(C.Structure):
     ]
 
 
+class _Trace(C.Structure):
+    _fields_ = [
+        ("level", C.c_int32), ("direction", C.c_int32), ("bu_sweep", C.c_int32), ("pad", C.c_int32),
+        ("frontier_vertices", C.c_int64), ("frontier_edges", C.c_int64), ("unvisited_queued", C.c_int64),
+        ("expand_ms", C.c_double), ("inspect_ms", C.c_double),
+    ]
+
+
 @dataclass
 class BfsOpts:
     """Tuning knobs of one graph's traversals (mirror of ``ent_bfs_opts``)."""
@@ -70,7 +78,7 @@ class BfsOpts:
     ref_ratio: float = 0.3
     small_max: int = 32
     large_min: int = 1024
-    hub_slots: int = 1024
+    hub_slots: int = 0
     chunk_edges: int = 2048
     blocks_per_sm: int = 0
 
@@ -155,6 +163,7 @@ def lib() -> C.CDLL:
         "ent_graph_destroy": (C.c_int, [_P]),
         "ent_bfs": (C.c_int, [_P, C.c_int32, _I32P, _I32P, C.POINTER(_Stats)]),
         "ent_bfs_device": (C.c_int, [_P, C.c_int32, _P, _P, _P, C.POINTER(_Stats)]),
+        "ent_bfs_trace": (C.c_int, [_P, C.c_int32, C.POINTER(_Trace), C.c_int32, _I32P, C.POINTER(_Stats)]),
         "ent_bfs_batch": (C.c_int, [_P, _I32P, C.c_int32, _I32P, C.POINTER(_Stats)]),
         "ent_bfs_batch_device": (C.c_int, [_P, _I32P, C.c_int32, _P, _P, C.POINTER(_Stats)]),
         "ent_bfs_multi": (C.c_int, [C.POINTER(_P), C.c_int32, _I32P, _I32P, C.POINTER(_I32P)]),
@@ -380,6 +389,15 @@ class Graph:
         _check(lib().ent_bfs_device(self.handle, int(src), C.c_void_p(depth_ptr), C.c_void_p(parent_ptr or None),
                                     C.c_void_p(stream or None), C.byref(st) if stats else None))
         return Stats._from_c(st) if stats else None
+
+    def trace(self, src: int, max_levels: int = 100000):
+        """Per-level trace (direction, frontier size/edges, kernel times) of one BFS."""
+        buf = (_Trace * max_levels)()
+        n = C.c_int32()
+        st = _Stats()
+        _check(lib().ent_bfs_trace(self.handle, int(src), buf, max_levels, C.byref(n), C.byref(st)))
+        rows = [{f[0]: getattr(buf[i], f[0]) for f in _Trace._fields_ if f[0] != "pad"} for i in range(n.value)]
+        return rows, Stats._from_c(st)
 
     def bfs_batch(self, sources: Iterable[int], depth_out: Optional[np.ndarray] = None):
         """Bitwise multi-source BFS; returns (depth int32[n_src, V], [Stats])."""

@@ -6,27 +6,33 @@
 // expanders) and synchronises the host >= 5 times.
 //
 // Design here:
-//  * Status lives in bitmaps: `vis` (visited, 1 bit/vertex) and two frontier
-//    bitmaps fb[level & 1]. At s24 each is 2 MB and stays in L2.
+//  * Status lives in bitmaps: `vis` (visited, 1 bit/vertex), the graph's
+//    `active` bitmap (degree > 0) and two frontier bitmaps fb[level & 1].
+//    At s24 each is 2 MB and stays in L2.
 //  * Top-down (TD) levels expand classified frontier queues (small: < small_max,
 //    warp-cooperative gather; mid: warp per vertex; large: CTA per chunk of
 //    chunk_edges edges), claim vertices with atomicOr on `vis`, and append
 //    discoveries to a raw queue with warp-aggregated atomics
 //    (reference expanders K2-K4, expander.cuh:74-423).
-//  * The inspector (reference K8/K9/K11, inspector.cuh:36-432) classifies the
-//    raw queue (TD) or the unvisited set (BU) into small/mid/large queues with
-//    one single-pass decoupled look-back scan, order-preserving.
-//  * Bottom-up (BU) levels scan unvisited vertices (thread / warp / CTA tiers
-//    with early exit) against the frontier bitmap and a shared-memory hub
-//    cache of the frontier's highest-degree vertices
+//  * Bottom-up (BU) levels sweep the status bitmaps: a warp owns one word
+//    (32 consecutive ids) and checks only unvisited, non-isolated vertices,
+//    each lane serially for small degrees, the whole warp together for large
+//    ones, stopping at the first neighbour in the frontier bitmap or in a
+//    shared-memory hub cache of the frontier's highest-degree vertices
 //    (reference K5-K7, expander.cuh:431-819; hub cache comm.h:172-177).
+//    Rows are ordered by descending neighbour degree, so the first check
+//    usually meets a hub.
+//  * The inspector (reference K8/K9/K11, inspector.cuh:36-432) classifies the
+//    next frontier into small/mid/large queues with one single-pass
+//    decoupled look-back scan, order-preserving: from the raw discovery queue
+//    after a TD level, from the frontier bitmap (the status array) when a BU
+//    level hands over to TD.
 //  * The direction policy runs on the device in the inspector's last CTA
 //    (reference rule inspector.cuh:486-521 is one option; Beamer alpha/beta
 //    with switch-back is the default).
 //  * The whole traversal is one CUDA graph: a reset kernel, then a while node
 //    whose body is [expand, inspect]; the inspector sets the loop condition.
 #include <algorithm>
-#include <cooperative_groups.h>
 #include <string.h>
 
 #include "dev_common.cuh"
@@ -41,7 +47,8 @@ constexpr int KS = 4;            // look-back status words per tile
 constexpr int TD = 0, BU = 1;
 
 // Device-resident loop state. Written only by the reset kernel's and the
-// inspector's last CTA; read by every kernel at start.
+// inspector's last CTA (plus atomics on the acc_* counters and n_raw); read
+// by every kernel at start.
 struct BfsCtl {
   int32_t src;
   int32_t pad0;
@@ -49,22 +56,18 @@ struct BfsCtl {
   int32_t* parent;
   int32_t level;      // the frontier holds the vertices at depth `level`
   int32_t dir;        // direction used to expand `level`
-  int32_t bu_sweep;   // BU expand scans all vertices (first BU level)
   int32_t qcur;       // ping-pong index of TD queues
-  int32_t ucur;       // ping-pong index of BU unvisited queues
   int32_t n_q[3];     // TD frontier queue sizes (small, mid, large)
   int32_t n_chunks;   // chunks of the large TD queue
-  int32_t n_u[3];     // BU unvisited queue sizes
   int32_t n_raw;      // TD raw next-frontier count (atomic append)
   int32_t done;
-  int32_t err;        // bit 1: look-back wait timed out, bit 2: level overflow
+  int32_t err;        // bit 1: look-back wait timed out, 2: level overflow, 3: count overflow
   int32_t td_levels;
   int32_t bu_levels;
-  int32_t pad1;
   int64_t n_f, m_f;   // frontier size and degree sum
   int64_t n_vis, m_vis;
-  unsigned long long acc_n, acc_m, acc_nu, acc_mu;
-  uint32_t tot[3 * KS];   // chain totals per segment, written by each segment's last tile
+  unsigned long long acc_n, acc_m;  // next frontier size / degree sum being accumulated
+  uint32_t tot[KS];   // chain totals, written by the last tile
   uint32_t tile_ticket;
   uint32_t finished;
   uint32_t epoch;
@@ -74,18 +77,17 @@ struct BfsCtl {
 struct LevelArgs {
   BfsCtl* ctl;
   const int64_t* off;
-  const int32_t* adj;
+  const int32_t* adj;      // traversal order (descending neighbour degree)
   const int32_t* deg;
+  const uint32_t* active;
   int64_t V, E;
   uint32_t* vis;
   uint32_t* fb[2];
   int32_t* q[2][3];
   int32_t* qc[2];
-  int32_t* uq[2][3];
   int32_t* raw;
   unsigned long long* hub[2];
-  unsigned long long* tiles;  // [3 segments][seg_tiles][KS]
-  int64_t seg_tiles;
+  unsigned long long* tiles;  // [tiles][KS]
   int32_t small_max, large_min, chunk, hub_slots, hub_shift, hub_min_deg;
   int32_t policy;
   double alpha, beta, ref_ratio;
@@ -97,11 +99,34 @@ struct LevelArgs {
 __device__ __forceinline__ int cls_of(int d, const LevelArgs& a) {
   return d < a.small_max ? 0 : (d > a.large_min ? 2 : 1);
 }
+__device__ __forceinline__ uint32_t n_chunks_of(int d, const LevelArgs& a) {
+  return (uint32_t)((d + a.chunk - 1) / a.chunk);
+}
 __device__ __forceinline__ uint32_t hub_slot(uint32_t v, int shift) { return (v * 0x9E3779B1u) >> shift; }
 
+// Direct-mapped table of the frontier's highest-degree vertices (the
+// reference keeps the max-degree vertex per slot, inspector.cuh:218-224, but
+// without atomics). Reading first keeps the atomics to the few keys that win.
 __device__ __forceinline__ void hub_insert(const LevelArgs& a, unsigned long long* ht, int v, int d) {
-  if (a.hub_slots && d >= a.hub_min_deg)
-    atomicMax(ht + hub_slot((uint32_t)v, a.hub_shift), ((unsigned long long)(uint32_t)d << 32) | (uint32_t)v);
+  if (a.hub_slots && d >= a.hub_min_deg) {
+    unsigned long long* slot = ht + hub_slot((uint32_t)v, a.hub_shift);
+    const unsigned long long key = ((unsigned long long)(uint32_t)d << 32) | (uint32_t)v;
+    if (__ldcg(slot) < key) atomicMax(slot, key);
+  }
+}
+
+template <class T>
+__device__ __forceinline__ T block_sum(T x, T* s_red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s_red[warp] = x;
+  __syncthreads();
+  T r = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < BT / 32; ++w) r += s_red[w];
+  return r;  // valid in thread 0
 }
 
 // --------------------------------------------------------------- reset ----
@@ -153,14 +178,12 @@ __global__ void __launch_bounds__(BT) k_reset(LevelArgs a, int32_t src, int32_t*
   c->parent = parent;
   c->level = 0;
   c->dir = a.policy == ENT_POLICY_BU_ONLY ? BU : TD;
-  c->bu_sweep = c->dir == BU;
   c->qcur = 0;
-  c->ucur = 0;
-  for (int k = 0; k < 3; ++k) { c->n_q[k] = 0; c->n_u[k] = 0; }
+  for (int k = 0; k < 3; ++k) c->n_q[k] = 0;
   c->n_q[cl] = 1;
   if (cl == 2) {
     a.qc[0][0] = 0;
-    c->n_chunks = (d + a.chunk - 1) / a.chunk;
+    c->n_chunks = (int32_t)n_chunks_of(d, a);
   } else {
     c->n_chunks = 0;
   }
@@ -173,8 +196,8 @@ __global__ void __launch_bounds__(BT) k_reset(LevelArgs a, int32_t src, int32_t*
   c->m_f = d;
   c->n_vis = 1;
   c->m_vis = d;
-  c->acc_n = c->acc_m = c->acc_nu = c->acc_mu = 0;
-  for (int k = 0; k < 3 * KS; ++k) c->tot[k] = 0;
+  c->acc_n = c->acc_m = 0;
+  for (int k = 0; k < KS; ++k) c->tot[k] = 0;
   c->tile_ticket = 0;
   c->finished = 0;
   __threadfence();
@@ -304,18 +327,11 @@ struct Front {
   }
 };
 
-__device__ __forceinline__ void bu_commit(const LevelArgs& a, int v, int pu, int ln, int32_t* depth, int32_t* parent,
-                                          uint32_t* fbn) {
-  depth[v] = ln;
-  if (parent) parent[v] = pu;
-  const uint32_t w = (uint32_t)v >> 5, b = 1u << (v & 31);
-  red_or(a.vis + w, b);
-  red_or(fbn + w, b);
-}
-
-__device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, int32_t* parent, int32_t* s_hub) {
+__device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, int32_t* parent, int32_t* s_hub,
+                          unsigned long long* s_red) {
   const uint32_t* fbc = a.fb[L & 1];
   uint32_t* fbn = a.fb[(L + 1) & 1];
+  unsigned long long* hub_next = a.hub[(L + 1) & 1];
   if (a.hub_slots) {
     const unsigned long long* ht = a.hub[L & 1];
     for (int i = threadIdx.x; i < a.hub_slots; i += BT) {
@@ -327,123 +343,76 @@ __device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, 
   const Front is_front{fbc, s_hub, a.hub_slots, a.hub_shift};
   const int lane = threadIdx.x & 31;
   const int64_t gtid = blockIdx.x * (int64_t)BT + threadIdx.x, nth = (int64_t)gridDim.x * BT;
-  const int gw = (int)(gtid >> 5), nw = (int)(nth >> 5);
+  const int64_t gw = gtid >> 5, nw = nth >> 5;
   const int ln = L + 1;
-
-  if (c->bu_sweep) {
-    // Every vertex; a warp owns 32 consecutive ids (one vis word).
-    const int64_t V = a.V;
-    for (int64_t base = (int64_t)gw * 32; base < V; base += (int64_t)nw * 32) {
-      const int64_t v = base + lane;
-      const uint32_t visw = a.vis[base >> 5];
-      bool todo = false;
-      int d = 0;
-      if (v < V && !((visw >> lane) & 1u)) {
-        d = a.deg[v];
-        todo = d > 0;
-      }
-      bool found = false;
-      int pu = -1;
-      if (todo && d < a.small_max) {
-        const int64_t e0 = a.off[v];
-        for (int64_t e = e0; e < e0 + d; ++e) {
-          const int u = __ldg(a.adj + e);
-          if (is_front(u)) { found = true; pu = u; break; }
-        }
-      }
-      unsigned heavy = __ballot_sync(FULL, todo && d >= a.small_max);
-      while (heavy) {
-        const int j = __ffs(heavy) - 1;
-        heavy &= heavy - 1;
-        const int64_t vj = base + j;
-        const int64_t beg = a.off[vj], end = a.off[vj + 1];
-        int hit = -1;
-        for (int64_t e0 = beg; e0 < end; e0 += 32) {
-          const int64_t e = e0 + lane;
-          const int u = e < end ? __ldg(a.adj + e) : -1;
-          const unsigned hm = __ballot_sync(FULL, e < end && is_front(u));
-          if (hm) { hit = __shfl_sync(FULL, u, __ffs(hm) - 1); break; }
-        }
-        if (lane == j && hit >= 0) { found = true; pu = hit; }
-      }
-      if (found) {
-        depth[v] = ln;
-        if (parent) parent[v] = pu;
-      }
-      const unsigned fm = __ballot_sync(FULL, found);
-      if (lane == 0 && fm) {
-        atomicOr(a.vis + (base >> 5), fm);
-        atomicOr(fbn + (base >> 5), fm);
+  const int64_t W = (a.V + 31) >> 5;
+  unsigned long long my_n = 0, my_m = 0;
+  // A warp owns one status word: 32 consecutive vertex ids.
+  for (int64_t wi = gw; wi < W; wi += nw) {
+    const uint32_t todo_mask = a.active[wi] & ~a.vis[wi];
+    if (!todo_mask) continue;
+    const int64_t v = wi * 32 + lane;
+    const bool todo = (todo_mask >> lane) & 1u;
+    int64_t e0 = 0;
+    int d = 0;
+    if (todo) {
+      e0 = a.off[v];
+      d = (int)(a.off[v + 1] - e0);
+    }
+    bool found = false;
+    int pu = -1;
+    if (todo && d < a.small_max) {
+      for (int k = 0; k < d; ++k) {
+        const int u = __ldg(a.adj + e0 + k);
+        if (is_front(u)) { found = true; pu = u; break; }
       }
     }
-    return;
-  }
-
-  const int uc = c->ucur;
-  const int ns = c->n_u[0], nm = c->n_u[1], nl = c->n_u[2];
-  const int32_t* __restrict__ us = a.uq[uc][0];
-  const int32_t* __restrict__ um = a.uq[uc][1];
-  const int32_t* __restrict__ ul = a.uq[uc][2];
-  // Large tier: one CTA per unvisited vertex, early exit by block vote.
-  __shared__ int s_hit;
-  for (int i = blockIdx.x; i < nl; i += gridDim.x) {
-    const int v = ul[i];
-    const int64_t beg = a.off[v], end = a.off[v + 1];
-    if (threadIdx.x == 0) s_hit = -1;
-    __syncthreads();
-    for (int64_t e0 = beg; e0 < end; e0 += BT) {
-      const int64_t e = e0 + threadIdx.x;
-      bool h = false;
-      if (e < end) {
-        const int u = __ldg(a.adj + e);
-        if (is_front(u)) { h = true; s_hit = u; }
+    unsigned heavy = __ballot_sync(FULL, todo && d >= a.small_max);
+    while (heavy) {
+      const int j = __ffs(heavy) - 1;
+      heavy &= heavy - 1;
+      const int64_t beg = __shfl_sync(FULL, e0, j);
+      const int64_t end = beg + __shfl_sync(FULL, d, j);
+      int hit = -1;
+      for (int64_t b0 = beg; b0 < end; b0 += 32) {
+        const int64_t e = b0 + lane;
+        const int u = e < end ? __ldg(a.adj + e) : -1;
+        const unsigned hm = __ballot_sync(FULL, e < end && is_front(u));
+        if (hm) { hit = __shfl_sync(FULL, u, __ffs(hm) - 1); break; }
       }
-      if (__syncthreads_or(h)) break;
+      if (lane == j && hit >= 0) { found = true; pu = hit; }
     }
-    if (threadIdx.x == 0 && s_hit >= 0) bu_commit(a, v, s_hit, ln, depth, parent, fbn);
-    __syncthreads();
-  }
-  // Mid tier: one warp per vertex, early exit by ballot.
-  for (int i = gw; i < nm; i += nw) {
-    const int v = um[i];
-    const int64_t beg = a.off[v], end = a.off[v + 1];
-    for (int64_t e0 = beg; e0 < end; e0 += 32) {
-      const int64_t e = e0 + lane;
-      const int u = e < end ? __ldg(a.adj + e) : -1;
-      const unsigned hm = __ballot_sync(FULL, e < end && is_front(u));
-      if (hm) {
-        const int src = __ffs(hm) - 1;
-        const int pu = __shfl_sync(FULL, u, src);
-        if (lane == 0) bu_commit(a, v, pu, ln, depth, parent, fbn);
-        break;
-      }
+    if (found) {
+      depth[v] = ln;
+      if (parent) parent[v] = pu;
+      my_n++;
+      my_m += (unsigned long long)d;
+      hub_insert(a, hub_next, (int)v, d);
+    }
+    const unsigned fm = __ballot_sync(FULL, found);
+    if (lane == 0 && fm) {
+      // this warp is the only writer of word wi during the level
+      a.vis[wi] = a.vis[wi] | fm;
+      fbn[wi] = fm;
     }
   }
-  // Small tier: one thread per vertex.
-  for (int64_t i = gtid; i < ns; i += nth) {
-    const int v = us[i];
-    const int64_t beg = a.off[v], end = a.off[v + 1];
-    for (int64_t e = beg; e < end; ++e) {
-      const int u = __ldg(a.adj + e);
-      if (is_front(u)) {
-        bu_commit(a, v, u, ln, depth, parent, fbn);
-        break;
-      }
-    }
+  const int any = __syncthreads_or(my_n != 0);
+  if (any) {
+    unsigned long long r = block_sum(my_n, s_red);
+    if (threadIdx.x == 0) atomicAdd(&c->acc_n, r);
+    r = block_sum(my_m, s_red);
+    if (threadIdx.x == 0) atomicAdd(&c->acc_m, r);
   }
 }
 
 __global__ void __launch_bounds__(BT) k_expand(LevelArgs a) {
   extern __shared__ int32_t s_hub[];
+  __shared__ unsigned long long s_red[BT / 32];
   BfsCtl* c = a.ctl;
   if (c->done) return;
   const int L = c->level;
-  if (a.hub_slots) {
-    unsigned long long* hn = a.hub[(L + 1) & 1];
-    for (int64_t i = blockIdx.x * (int64_t)BT + threadIdx.x; i < a.hub_slots; i += (int64_t)gridDim.x * BT) hn[i] = 0;
-  }
   if (c->dir == TD) td_expand(a, c, L, c->depth, c->parent);
-  else bu_expand(a, c, L, c->depth, c->parent, s_hub);
+  else bu_expand(a, c, L, c->depth, c->parent, s_hub, s_red);
 }
 
 // ----------------------------------------------------------- inspector ----
@@ -460,20 +429,6 @@ __device__ __forceinline__ void load_tile(const int32_t* src, int64_t first, int
   }
 }
 
-template <class T>
-__device__ __forceinline__ T block_sum(T x, T* s_red) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) s_red[warp] = x;
-  __syncthreads();
-  T r = 0;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < BT / 32; ++w) r += s_red[w];
-  __syncthreads();
-  return r;  // valid in thread 0
-}
-
 __device__ __forceinline__ uint32_t acquire_tile(BfsCtl* c, uint32_t* s_tile) {
   if (threadIdx.x == 0) *s_tile = atomicAdd(&c->tile_ticket, 1u);
   __syncthreads();
@@ -481,6 +436,19 @@ __device__ __forceinline__ uint32_t acquire_tile(BfsCtl* c, uint32_t* s_tile) {
   __syncthreads();
   return t;
 }
+
+// Appends one classified vertex to the next TD queues.
+struct QueueOut {
+  int32_t* q[3];
+  int32_t* qc;
+  __device__ __forceinline__ void put(const LevelArgs& a, int v, int cl, int d, uint32_t (&pos)[4]) const {
+    q[cl][pos[cl]++] = v;
+    if (cl == 2) {
+      qc[pos[2] - 1] = (int32_t)pos[3];
+      pos[3] += n_chunks_of(d, a);
+    }
+  }
+};
 
 __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   __shared__ uint32_t s_scan[32 * KS];
@@ -490,17 +458,24 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   __shared__ unsigned long long s_red[BT / 32];
   BfsCtl* c = a.ctl;
   if (c->done) return;
-  const int L = c->level, dir = c->dir, sweep = c->bu_sweep;
+  const int L = c->level, dir = c->dir;
   const uint32_t epoch = c->epoch;
-  const int qcur = c->qcur, ucur = c->ucur;
+  const int qcur = c->qcur;
   const int64_t gtid = blockIdx.x * (int64_t)BT + threadIdx.x, nth = (int64_t)gridDim.x * BT;
-  unsigned long long my_n = 0, my_m = 0, my_nu = 0, my_mu = 0;
-  unsigned long long* hub_next = a.hub[(L + 1) & 1];
   int* err = &c->err;
+  const QueueOut qo{{a.q[qcur ^ 1][0], a.q[qcur ^ 1][1], a.q[qcur ^ 1][2]}, a.qc[qcur ^ 1]};
+  // The hub table of frontier L was read by expand(L): clear it for level L+2.
+  if (a.hub_slots) {
+    unsigned long long* hd = a.hub[L & 1];
+    for (int64_t i = gtid; i < a.hub_slots; i += nth) hd[i] = 0;
+  }
+  uint32_t* fbo = a.fb[L & 1];
+  const uint32_t* fbn = a.fb[(L + 1) & 1];
+  unsigned long long my_m = 0;
+  bool to_td = false;
 
   if (dir == TD) {
     // Frontier L is dead: zero its words in fb[L&1] (touching only its vertices).
-    uint32_t* fbo = a.fb[L & 1];
     for (int k = 0; k < 3; ++k) {
       const int32_t* qk = a.q[qcur][k];
       for (int64_t i = gtid; i < c->n_q[k]; i += nth) fbo[(uint32_t)qk[i] >> 5] = 0;
@@ -508,8 +483,7 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
     // Classify the raw next frontier into q[qcur^1].
     const int64_t n = c->n_raw;
     const uint32_t ntiles = (uint32_t)((n + TILE - 1) / TILE);
-    int32_t* qo[3] = {a.q[qcur ^ 1][0], a.q[qcur ^ 1][1], a.q[qcur ^ 1][2]};
-    int32_t* qco = a.qc[qcur ^ 1];
+    unsigned long long* hub_next = a.hub[(L + 1) & 1];
     while (true) {
       const uint32_t tile = acquire_tile(c, &s_tile);
       if (tile >= ntiles) break;
@@ -525,7 +499,7 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
           cnt[cl[j]]++;
           my_m += dg[j];
           hub_insert(a, hub_next, v[j], dg[j]);
-          if (cl[j] == 2) cnt[3] += (uint32_t)((dg[j] + a.chunk - 1) / a.chunk);
+          if (cl[j] == 2) cnt[3] += n_chunks_of(dg[j], a);
         }
       }
       uint32_t pre[4] = {cnt[0], cnt[1], cnt[2], cnt[3]}, agg[4], excl[4];
@@ -535,139 +509,50 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) pos[k] = excl[k] + pre[k];
 #pragma unroll
-      for (int j = 0; j < IPT; ++j) {
-        if (cl[j] < 0) continue;
-        qo[cl[j]][pos[cl[j]]++] = v[j];
-        if (cl[j] == 2) {
-          qco[pos[2] - 1] = (int32_t)pos[3];
-          pos[3] += (uint32_t)((dg[j] + a.chunk - 1) / a.chunk);
-        }
-      }
+      for (int j = 0; j < IPT; ++j)
+        if (cl[j] >= 0) qo.put(a, v[j], cl[j], dg[j], pos);
       if (tile == ntiles - 1 && threadIdx.x == 0) {
         for (int k = 0; k < 4; ++k) c->tot[k] = excl[k] + agg[k];
         __threadfence();
       }
     }
   } else {
-    uint32_t* fbo = a.fb[L & 1];
-    const uint32_t* fbn = a.fb[(L + 1) & 1];
+    // BU level done: the expander counted the new frontier in acc_n/acc_m.
+    const int64_t n_next = (int64_t)c->acc_n;
+    to_td = a.policy == ENT_POLICY_BEAMER && n_next > 0 && (double)n_next < (double)a.V / a.beta &&
+            n_next < c->n_f;
     const int64_t W = (a.V + 31) >> 5;
     for (int64_t i = gtid; i < W; i += nth) fbo[i] = 0;
-    if (sweep) {
-      // Build the unvisited queues from the status bitmaps (all vertices).
-      const int64_t n = a.V;
-      const uint32_t ntiles = (uint32_t)((n + TILE - 1) / TILE);
-      int32_t* uo[3] = {a.uq[ucur ^ 1][0], a.uq[ucur ^ 1][1], a.uq[ucur ^ 1][2]};
+    if (to_td) {
+      // Hand over to TD: classify the frontier bitmap (ascending ids) into
+      // q[qcur^1]. A tile is BT words (BT*32 vertices), one word per thread.
+      const uint32_t ntiles = (uint32_t)((W + BT - 1) / BT);
       while (true) {
         const uint32_t tile = acquire_tile(c, &s_tile);
         if (tile >= ntiles) break;
-        const int64_t v0 = (int64_t)tile * TILE + (int64_t)threadIdx.x * IPT;
-        int cl[IPT];
-        uint32_t cnt[3] = {0, 0, 0};
-        uint32_t visw = 0, fnw = 0;
-        if (v0 < n) {
-          visw = ld_cg(a.vis + (v0 >> 5));
-          fnw = ld_cg(fbn + (v0 >> 5));
+        const int64_t wi = (int64_t)tile * BT + threadIdx.x;
+        const uint32_t word = wi < W ? ld_cg(fbn + wi) : 0u;
+        uint32_t cnt[4] = {0, 0, 0, 0};
+        for (uint32_t m = word; m; m &= m - 1) {
+          const int v = (int)(wi * 32 + __ffs(m) - 1);
+          const int d = a.deg[v];
+          const int cl = cls_of(d, a);
+          cnt[cl]++;
+          if (cl == 2) cnt[3] += n_chunks_of(d, a);
         }
+        uint32_t pre[4] = {cnt[0], cnt[1], cnt[2], cnt[3]}, agg[4], excl[4];
+        block_excl_scan<4>(pre, agg, s_scan);
+        lookback<4, KS>(a.tiles, tile, epoch, agg, excl, s_excl, err);
+        uint32_t pos[4];
 #pragma unroll
-        for (int j = 0; j < IPT; ++j) {
-          const int64_t v = v0 + j;
-          cl[j] = -1;
-          if (v >= n) continue;
-          const int bit = (int)(v & 31);
-          if ((fnw >> bit) & 1u) {
-            const int d = a.deg[v];
-            my_n++;
-            my_m += d;
-            hub_insert(a, hub_next, (int)v, d);
-          } else if (!((visw >> bit) & 1u)) {
-            const int d = a.deg[v];
-            if (d > 0) {
-              cl[j] = cls_of(d, a);
-              cnt[cl[j]]++;
-              my_nu++;
-              my_mu += d;
-            }
-          }
+        for (int k = 0; k < 4; ++k) pos[k] = excl[k] + pre[k];
+        for (uint32_t m = word; m; m &= m - 1) {
+          const int v = (int)(wi * 32 + __ffs(m) - 1);
+          const int d = a.deg[v];
+          qo.put(a, v, cls_of(d, a), d, pos);
         }
-        uint32_t pre[3] = {cnt[0], cnt[1], cnt[2]}, agg[3], excl[3];
-        block_excl_scan<3>(pre, agg, s_scan);
-        lookback<3, KS>(a.tiles, tile, epoch, agg, excl, s_excl, err);
-        uint32_t pos[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) pos[k] = excl[k] + pre[k];
-#pragma unroll
-        for (int j = 0; j < IPT; ++j)
-          if (cl[j] >= 0) uo[cl[j]][pos[cl[j]]++] = (int32_t)(v0 + j);
         if (tile == ntiles - 1 && threadIdx.x == 0) {
-          for (int k = 0; k < 3; ++k) c->tot[k] = excl[k] + agg[k];
-          __threadfence();
-        }
-      }
-    } else {
-      // Partition each unvisited queue: still unvisited -> uq[ucur^1][s];
-      // found this level -> TD queue q[qcur^1][s] (same degree class).
-      uint32_t nt[3], first[3];
-      uint32_t total_tiles = 0;
-      for (int s = 0; s < 3; ++s) {
-        nt[s] = (uint32_t)((c->n_u[s] + TILE - 1) / TILE);
-        first[s] = total_tiles;
-        total_tiles += nt[s];
-      }
-      while (true) {
-        const uint32_t ticket = acquire_tile(c, &s_tile);
-        if (ticket >= total_tiles) break;
-        const int s = ticket >= first[2] && nt[2] ? 2 : (ticket >= first[1] && nt[1] ? 1 : 0);
-        const uint32_t tile = ticket - first[s];
-        const int64_t n = c->n_u[s];
-        int32_t v[IPT];
-        load_tile(a.uq[ucur][s], (int64_t)tile * TILE, n, v);
-        int st[IPT], dg[IPT];
-        uint32_t cnt[3] = {0, 0, 0};
-#pragma unroll
-        for (int j = 0; j < IPT; ++j) {
-          st[j] = -1;
-          dg[j] = 0;
-          if (v[j] < 0) continue;
-          dg[j] = a.deg[v[j]];
-          const bool fnd = (ld_cg(fbn + ((uint32_t)v[j] >> 5)) >> (v[j] & 31)) & 1u;
-          if (fnd) {
-            st[j] = 1;
-            cnt[1]++;
-            if (s == 2) cnt[2] += (uint32_t)((dg[j] + a.chunk - 1) / a.chunk);
-            my_n++;
-            my_m += dg[j];
-            hub_insert(a, hub_next, v[j], dg[j]);
-          } else {
-            st[j] = 0;
-            cnt[0]++;
-            my_nu++;
-            my_mu += dg[j];
-          }
-        }
-        uint32_t pre[3] = {cnt[0], cnt[1], cnt[2]}, agg[3], excl[3];
-        block_excl_scan<3>(pre, agg, s_scan);
-        lookback<3, KS>(a.tiles + (size_t)s * a.seg_tiles * KS, tile, epoch, agg, excl, s_excl, err);
-        uint32_t pos[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) pos[k] = excl[k] + pre[k];
-        int32_t* uo = a.uq[ucur ^ 1][s];
-        int32_t* qo = a.q[qcur ^ 1][s];
-        int32_t* qco = a.qc[qcur ^ 1];
-#pragma unroll
-        for (int j = 0; j < IPT; ++j) {
-          if (st[j] == 0) {
-            uo[pos[0]++] = v[j];
-          } else if (st[j] == 1) {
-            qo[pos[1]++] = v[j];
-            if (s == 2) {
-              qco[pos[1] - 1] = (int32_t)pos[2];
-              pos[2] += (uint32_t)((dg[j] + a.chunk - 1) / a.chunk);
-            }
-          }
-        }
-        if (tile == nt[s] - 1 && threadIdx.x == 0) {
-          for (int k = 0; k < 3; ++k) c->tot[s * KS + k] = excl[k] + agg[k];
+          for (int k = 0; k < 4; ++k) c->tot[k] = excl[k] + agg[k];
           __threadfence();
         }
       }
@@ -675,15 +560,10 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   }
 
   // Publish this CTA's counters, then the last CTA to finish runs the policy.
-  unsigned long long r;
-  r = block_sum(my_n, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(&c->acc_n, r);
-  r = block_sum(my_m, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(&c->acc_m, r);
-  r = block_sum(my_nu, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(&c->acc_nu, r);
-  r = block_sum(my_mu, s_red);
-  if (threadIdx.x == 0 && r) atomicAdd(&c->acc_mu, r);
+  if (dir == TD && __syncthreads_or(my_m != 0)) {
+    const unsigned long long r = block_sum(my_m, s_red);
+    if (threadIdx.x == 0) atomicAdd(&c->acc_m, r);
+  }
   if (threadIdx.x == 0) {
     __threadfence();
     s_last = atomicAdd(&c->finished, 1u) == gridDim.x - 1;
@@ -693,41 +573,25 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   __threadfence();
   volatile BfsCtl* vc = c;
   const int64_t nf_cur = vc->n_f;
-  int64_t n_next, m_next;
-  int next_dir = dir, next_sweep = 0;
+  const int64_t n_next = dir == TD ? (int64_t)vc->n_raw : (int64_t)vc->acc_n;
+  const int64_t m_next = (int64_t)vc->acc_m;
+  int next_dir = dir;
   if (dir == TD) {
-    n_next = vc->n_raw;
-    m_next = (int64_t)vc->acc_m;
     vc->td_levels = vc->td_levels + 1;
     vc->qcur = qcur ^ 1;
     for (int k = 0; k < 3; ++k) vc->n_q[k] = (int32_t)vc->tot[k];
     vc->n_chunks = (int32_t)vc->tot[3];
-    const int64_t m_vis = vc->m_vis + m_next;
-    const double m_u = (double)(a.E - m_vis);
+    const double m_u = (double)(a.E - (vc->m_vis + m_next));
     if (a.policy == ENT_POLICY_BEAMER && (double)m_next > m_u / a.alpha) next_dir = BU;
     if (a.policy == ENT_POLICY_REFERENCE && (double)m_next >= a.ref_ratio * (double)a.E) next_dir = BU;
-    next_sweep = next_dir == BU;
-  } else if (sweep) {
-    n_next = (int64_t)vc->acc_n;
-    m_next = (int64_t)vc->acc_m;
-    vc->bu_levels = vc->bu_levels + 1;
-    vc->ucur = ucur ^ 1;
-    for (int k = 0; k < 3; ++k) vc->n_u[k] = (int32_t)vc->tot[k];
-    next_dir = BU;
+    if (a.policy == ENT_POLICY_BU_ONLY) next_dir = BU;
   } else {
-    n_next = (int64_t)vc->acc_n;
-    m_next = (int64_t)vc->acc_m;
     vc->bu_levels = vc->bu_levels + 1;
-    const bool to_td = a.policy == ENT_POLICY_BEAMER && (double)n_next < (double)a.V / a.beta && n_next < nf_cur;
     if (to_td) {
       next_dir = TD;
       vc->qcur = qcur ^ 1;
-      for (int s = 0; s < 3; ++s) vc->n_q[s] = (int32_t)vc->tot[s * KS + 1];
-      vc->n_chunks = (int32_t)vc->tot[2 * KS + 2];
-    } else {
-      next_dir = BU;
-      vc->ucur = ucur ^ 1;
-      for (int s = 0; s < 3; ++s) vc->n_u[s] = (int32_t)vc->tot[s * KS + 0];
+      for (int k = 0; k < 3; ++k) vc->n_q[k] = (int32_t)vc->tot[k];
+      vc->n_chunks = (int32_t)vc->tot[3];
     }
   }
   vc->n_vis = vc->n_vis + n_next;
@@ -735,7 +599,6 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   vc->n_f = n_next;
   vc->m_f = m_next;
   vc->dir = next_dir;
-  vc->bu_sweep = next_sweep;
   vc->level = L + 1;
   int done = n_next == 0;
   if (L + 1 >= a.max_levels && !done) {
@@ -750,9 +613,7 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   vc->n_raw = 0;
   vc->acc_n = 0;
   vc->acc_m = 0;
-  vc->acc_nu = 0;
-  vc->acc_mu = 0;
-  for (int k = 0; k < 3 * KS; ++k) vc->tot[k] = 0;
+  for (int k = 0; k < KS; ++k) vc->tot[k] = 0;
   vc->tile_ticket = 0;
   vc->finished = 0;
   vc->epoch = epoch + 1;
@@ -776,7 +637,6 @@ struct BfsWorkspace {
   cudaGraphExec_t exec = nullptr;
   cudaGraphNode_t reset_node = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  int kernels_per_iter = 2;
 };
 
 void destroy_bfs_workspace(BfsWorkspace* w) {
@@ -839,17 +699,17 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out) {
   w->V = g->V;
   const int64_t V = g->V;
   const int64_t W = (V + 31) / 32;
-  const int64_t seg_tiles = (V + TILE - 1) / TILE + 1;
+  const int64_t tiles = std::max((V + TILE - 1) / TILE, (W + BT - 1) / BT) + 1;
   const ent_bfs_opts& o = g->opts;
   int hub = o.hub_slots;
   if (hub > 0 && hub < 16) hub = 16;
-  // Slab layout (all 256-byte aligned): vis, fb0, fb1, q[2][3], qc[2], uq[2][3], raw, hub[2], tiles.
+  // Slab layout (all 256-byte aligned): vis, fb0, fb1, q[2][3], qc[2], raw, hub[2], tiles.
   auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
   size_t sz_bits = al(sizeof(uint32_t) * (W + 1));
   size_t sz_q = al(sizeof(int32_t) * (V + 4));
   size_t sz_hub = al(sizeof(unsigned long long) * (hub > 0 ? hub : 1));
-  size_t sz_tiles = al(sizeof(unsigned long long) * 3 * seg_tiles * KS);
-  size_t total = 3 * sz_bits + 15 * sz_q + 2 * sz_hub + sz_tiles;
+  size_t sz_tiles = al(sizeof(unsigned long long) * tiles * KS);
+  size_t total = 3 * sz_bits + 9 * sz_q + 2 * sz_hub + sz_tiles;
   cudaError_t e = cudaMalloc(&w->slab, total);
   if (e != cudaSuccess) { destroy_bfs_workspace(w); return fail(ENT_ERR_OOM, "workspace allocation (%zu bytes) failed", total); }
   e = cudaMemset(w->slab, 0, total);
@@ -866,8 +726,9 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out) {
   memset(&a, 0, sizeof(a));
   a.ctl = w->ctl;
   a.off = g->off;
-  a.adj = g->adj;
+  a.adj = g->trav;
   a.deg = g->deg;
+  a.active = g->active;
   a.V = V;
   a.E = g->E;
   a.vis = (uint32_t*)p; p += sz_bits;
@@ -876,13 +737,10 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out) {
   for (int i = 0; i < 2; ++i)
     for (int k = 0; k < 3; ++k) { a.q[i][k] = (int32_t*)p; p += sz_q; }
   for (int i = 0; i < 2; ++i) { a.qc[i] = (int32_t*)p; p += sz_q; }
-  for (int i = 0; i < 2; ++i)
-    for (int k = 0; k < 3; ++k) { a.uq[i][k] = (int32_t*)p; p += sz_q; }
   a.raw = (int32_t*)p; p += sz_q;
   a.hub[0] = (unsigned long long*)p; p += sz_hub;
   a.hub[1] = (unsigned long long*)p; p += sz_hub;
   a.tiles = (unsigned long long*)p; p += sz_tiles;
-  a.seg_tiles = seg_tiles;
   a.small_max = o.small_max;
   a.large_min = o.large_min;
   a.chunk = o.chunk_edges;
@@ -912,6 +770,16 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out) {
   }
   *out = w;
   return ENT_OK;
+}
+
+static void fill_stats(const BfsCtl& h, float ms, ent_stats* stats) {
+  stats->reached_vertices = h.n_vis;
+  stats->traversed_edges = h.m_vis;
+  stats->levels = h.level;
+  stats->td_levels = h.td_levels;
+  stats->bu_levels = h.bu_levels;
+  stats->status = h.err;
+  stats->device_ms = ms;
 }
 
 int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, cudaStream_t stream, ent_stats* stats) {
@@ -956,18 +824,11 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, c
     ENT_CUDA(cudaEventRecord(w->ev1, s));
     ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));
     ENT_CUDA(cudaStreamSynchronize(s));
-    const BfsCtl& h = *w->ctl_h;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, w->ev0, w->ev1);
-    stats->reached_vertices = h.n_vis;
-    stats->traversed_edges = h.m_vis;
-    stats->levels = h.level;
-    stats->td_levels = h.td_levels;
-    stats->bu_levels = h.bu_levels;
-    stats->status = h.err;
-    stats->device_ms = ms;
-    if (g->opts.loop == ENT_LOOP_GRAPH) g_kernel_launches += 1 + 2 * (int64_t)h.level;
-    if (h.err) return fail(ENT_ERR_TIMEOUT, "device traversal reported error flags 0x%x", h.err);
+    fill_stats(*w->ctl_h, ms, stats);
+    if (g->opts.loop == ENT_LOOP_GRAPH) g_kernel_launches += 1 + 2 * (int64_t)w->ctl_h->level;
+    if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "device traversal reported error flags 0x%x", w->ctl_h->err);
   } else if (g->opts.loop == ENT_LOOP_GRAPH) {
     g_kernel_launches += 1;  // level kernels are counted when stats are read
   }
@@ -987,6 +848,69 @@ int ent_bfs_device(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* paren
   std::lock_guard<std::mutex> lk(g->mu);
   DeviceGuard dg(g->device);
   return run_bfs_single(g, src, depth_dev, parent_dev, (cudaStream_t)stream, stats);
+}
+
+int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_levels, int32_t* n_levels,
+                  ent_stats* stats) {
+  clear_error();
+  if (!g || !out || !n_levels || max_levels < 1) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
+  if (src < 0 || src >= g->V) return fail(ENT_ERR_INVALID_ARG, "source %d out of range", src);
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard dg(g->device);
+  if (!g->ws) {
+    int rc = create_workspace(g, &g->ws);
+    if (rc != ENT_OK) return rc;
+  }
+  BfsWorkspace* w = g->ws;
+  cudaStream_t s = g->stream;
+  cudaEvent_t e[3];
+  for (int i = 0; i < 3; ++i) ENT_CUDA(cudaEventCreate(&e[i]));
+  LevelArgs la = w->args;
+  la.use_cond = 0;
+  ENT_CUDA(cudaEventRecord(w->ev0, s));
+  k_reset<<<w->grid_reset, BT, 0, s>>>(la, src, w->depth, nullptr);
+  g_kernel_launches++;
+  int n = 0;
+  for (;;) {
+    ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));
+    ENT_CUDA(cudaStreamSynchronize(s));
+    const BfsCtl h = *w->ctl_h;
+    if (h.done || n >= max_levels) break;
+    ent_level_trace& t = out[n];
+    t.level = h.level;
+    t.direction = h.dir;
+    t.bu_sweep = h.dir == BU;
+    t.pad = 0;
+    t.frontier_vertices = h.n_f;
+    t.frontier_edges = h.m_f;
+    t.unvisited_queued = 0;
+    ENT_CUDA(cudaEventRecord(e[0], s));
+    k_expand<<<w->grid_expand, BT, w->smem_expand, s>>>(la);
+    ENT_CUDA(cudaEventRecord(e[1], s));
+    k_inspect<<<w->grid_inspect, BT, 0, s>>>(la);
+    ENT_CUDA(cudaEventRecord(e[2], s));
+    g_kernel_launches += 2;
+    ENT_CUDA(cudaGetLastError());
+    ENT_CUDA(cudaEventSynchronize(e[2]));
+    float ta = 0, tb = 0;
+    cudaEventElapsedTime(&ta, e[0], e[1]);
+    cudaEventElapsedTime(&tb, e[1], e[2]);
+    t.expand_ms = ta;
+    t.inspect_ms = tb;
+    ++n;
+  }
+  ENT_CUDA(cudaEventRecord(w->ev1, s));
+  ENT_CUDA(cudaStreamSynchronize(s));
+  for (int i = 0; i < 3; ++i) cudaEventDestroy(e[i]);
+  *n_levels = n;
+  const BfsCtl& h = *w->ctl_h;
+  if (stats) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, w->ev0, w->ev1);
+    fill_stats(h, ms, stats);
+  }
+  if (h.err) return fail(ENT_ERR_TIMEOUT, "device traversal reported error flags 0x%x", h.err);
+  return ENT_OK;
 }
 
 int ent_bfs(ent_graph* g, int32_t src, int32_t* depth_out, int32_t* parent_out, ent_stats* stats) {

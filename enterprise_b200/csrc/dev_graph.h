@@ -16,6 +16,11 @@ void destroy_batch_workspace(BatchWorkspace* w);
 //   off  int64[V+1]   row offsets (reference strt_pos + adj_card, allocator.cuh:107-114)
 //   adj  int32[E]     column ids, rows ascending (reference adj_list, allocator.cuh:116-120)
 //   deg  int32[V]     degrees, read by the classifier (reference adj_card)
+//   active uint32[V/32] bit v set iff deg(v) > 0 (bottom-up skips isolated vertices)
+//   trav int32[E]     the rows of adj re-ordered by descending neighbour degree
+//                     (ties by id): the traversal's adjacency. A bottom-up check
+//                     then meets the likeliest parent, a hub, first. Equal to
+//                     adj when E >= 2^31 (no re-ordering).
 struct ent_graph {
   int device = 0;
   int num_sms = 0;
@@ -23,6 +28,8 @@ struct ent_graph {
   int64_t* off = nullptr;
   int32_t* adj = nullptr;
   int32_t* deg = nullptr;
+  uint32_t* active = nullptr;
+  int32_t* trav = nullptr;
   cudaStream_t stream = nullptr;
   ent_bfs_opts opts;
   std::mutex mu;

@@ -33,6 +33,69 @@ int graph_alloc(ent_graph* g, int64_t V, int64_t E) {
   return ENT_OK;
 }
 
+__global__ void k_active_bits(const int32_t* __restrict__ deg, uint32_t* __restrict__ active, int64_t V) {
+  const int64_t W = (V + 31) >> 5;
+  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < W; w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t bits = 0;
+    for (int b = 0; b < 32; ++b) {
+      const int64_t v = w * 32 + b;
+      if (v < V && deg[v] > 0) bits |= 1u << b;
+    }
+    active[w] = bits;
+  }
+}
+
+// Key that orders a row by descending neighbour degree, then ascending id.
+__global__ void k_degree_keys(const int32_t* __restrict__ adj, const int32_t* __restrict__ deg, int64_t E,
+                              unsigned long long* __restrict__ keys) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t u = adj[e];
+    keys[e] = ((unsigned long long)(uint32_t)(0x7fffffff - deg[u]) << 32) | (uint32_t)u;
+  }
+}
+
+__global__ void k_keys_to_ids(const unsigned long long* __restrict__ keys, int64_t E, int32_t* __restrict__ out) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = (int32_t)(uint32_t)keys[e];
+}
+
+// Builds the traversal adjacency (rows by descending neighbour degree).
+static int build_traversal_order(ent_graph* g) {
+  const int64_t E = g->E, V = g->V;
+  if (E == 0 || E > 0x7fffffffll || V > 0x7ffffffell) {
+    g->trav = g->adj;  // no re-ordering: traverse the canonical rows
+    return ENT_OK;
+  }
+  ENT_CUDA(cudaMalloc(&g->trav, sizeof(int32_t) * E));
+  unsigned long long *k0 = nullptr, *k1 = nullptr;
+  void* tmp = nullptr;
+  size_t tmp_bytes = 0;
+  cudaError_t e = cudaMalloc(&k0, sizeof(unsigned long long) * E);
+  if (e == cudaSuccess) e = cudaMalloc(&k1, sizeof(unsigned long long) * E);
+  const int blocks = g->num_sms * 16;
+  if (e == cudaSuccess) {
+    k_degree_keys<<<blocks, 256, 0, g->stream>>>(g->adj, g->deg, E, k0);
+    g_kernel_launches++;
+    e = cub::DeviceSegmentedSort::SortKeys(nullptr, tmp_bytes, k0, k1, (int)E, (int)V, g->off, g->off + 1,
+                                           g->stream);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes);
+  if (e == cudaSuccess)
+    e = cub::DeviceSegmentedSort::SortKeys(tmp, tmp_bytes, k0, k1, (int)E, (int)V, g->off, g->off + 1, g->stream);
+  if (e == cudaSuccess) {
+    k_keys_to_ids<<<blocks, 256, 0, g->stream>>>(k1, E, g->trav);
+    g_kernel_launches++;
+    e = cudaStreamSynchronize(g->stream);
+  }
+  if (k0) cudaFree(k0);
+  if (k1) cudaFree(k1);
+  if (tmp) cudaFree(tmp);
+  if (e != cudaSuccess)
+    return fail(e == cudaErrorMemoryAllocation ? ENT_ERR_OOM : ENT_ERR_CUDA, "traversal order build failed: %s",
+                cudaGetErrorString(e));
+  return ENT_OK;
+}
+
 int graph_finish(ent_graph* g) {
   ENT_CUDA(cudaDeviceGetAttribute(&g->num_sms, cudaDevAttrMultiProcessorCount, g->device));
   if (!g->stream) ENT_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
@@ -40,6 +103,14 @@ int graph_finish(ent_graph* g) {
   k_degrees<<<blocks, 256, 0, g->stream>>>(g->off, g->deg, g->V);
   g_kernel_launches++;
   ENT_CUDA(cudaGetLastError());
+  const int64_t W = (g->V + 31) >> 5;
+  ENT_CUDA(cudaMalloc(&g->active, sizeof(uint32_t) * (W + 1)));
+  k_active_bits<<<(int)std::min<int64_t>((W + 255) / 256, (int64_t)g->num_sms * 16), 256, 0, g->stream>>>(
+      g->deg, g->active, g->V);
+  g_kernel_launches++;
+  ENT_CUDA(cudaGetLastError());
+  int rc = build_traversal_order(g);
+  if (rc != ENT_OK) return rc;
   ENT_CUDA(cudaStreamSynchronize(g->stream));
   ent_bfs_opts_default(&g->opts);
   return ENT_OK;
@@ -50,6 +121,8 @@ static void graph_free(ent_graph* g) {
   DeviceGuard dg(g->device);
   if (g->ws) destroy_bfs_workspace(g->ws);
   if (g->bws) destroy_batch_workspace(g->bws);
+  if (g->trav && g->trav != g->adj) cudaFree(g->trav);
+  if (g->active) cudaFree(g->active);
   if (g->off) cudaFree(g->off);
   if (g->adj) cudaFree(g->adj);
   if (g->deg) cudaFree(g->deg);
@@ -234,7 +307,7 @@ void ent_bfs_opts_default(ent_bfs_opts* o) {
   o->ref_ratio = 0.3;
   o->small_max = 32;
   o->large_min = 1024;
-  o->hub_slots = 1024;
+  o->hub_slots = 0;
   o->chunk_edges = 2048;
   o->blocks_per_sm = 0;
 }

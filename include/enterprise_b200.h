@@ -176,6 +176,23 @@ int ent_bfs(ent_graph* g, int32_t src, int32_t* depth_out, int32_t* parent_out,
 int ent_bfs_device(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* parent_dev,
                    void* stream, ent_stats* stats);
 
+/* Per-level trace of one traversal (tracing / profiling aid). Runs the level
+ * loop host-driven with CUDA events around each kernel; depths are the same
+ * as ent_bfs. out holds max_levels entries; *n_levels gets the count. */
+typedef struct ent_level_trace {
+  int32_t level;             /* depth of the frontier expanded                */
+  int32_t direction;         /* 0 top-down, 1 bottom-up                       */
+  int32_t bu_sweep;          /* bottom-up over every vertex (first BU level)  */
+  int32_t pad;
+  int64_t frontier_vertices; /* n_f of the frontier expanded                  */
+  int64_t frontier_edges;    /* m_f                                           */
+  int64_t unvisited_queued;  /* BU: unvisited vertices in the tier queues     */
+  double expand_ms;
+  double inspect_ms;
+} ent_level_trace;
+int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_levels, int32_t* n_levels,
+                  ent_stats* stats);
+
 /* Many sources at once with bitwise frontiers (one bit per source per vertex
  * in a shared status word). depth_out: HOST array n_src x V int32, source-major
  * (row s is the depth array of src[s]); may be NULL. stats: n_src entries or
