@@ -167,6 +167,11 @@ def lib() -> C.CDLL:
         "ent_bfs_batch": (C.c_int, [_P, _I32P, C.c_int32, _I32P, C.POINTER(_Stats)]),
         "ent_bfs_batch_device": (C.c_int, [_P, _I32P, C.c_int32, _P, _P, C.POINTER(_Stats)]),
         "ent_bfs_multi": (C.c_int, [C.POINTER(_P), C.c_int32, _I32P, _I32P, C.POINTER(_I32P)]),
+        "ent_bfs_batch_trace": (C.c_int, [_P, _I32P, C.c_int32, _P, C.POINTER(_Trace), C.c_int32, _I32P]),
+        "ent_multi_create": (C.c_int, [C.POINTER(_P), C.c_int32, _I32P, _I32P, C.POINTER(_P)]),
+        "ent_multi_run": (C.c_int, [_P, C.POINTER(C.c_double)]),
+        "ent_multi_depths": (C.c_int, [_P, C.c_int32, _I32P]),
+        "ent_multi_destroy": (C.c_int, [_P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -409,6 +414,15 @@ class Graph:
         _check(lib().ent_bfs_batch(self.handle, _i32p(src), n, _i32p(depth), st))
         return depth, [Stats._from_c(st[i]) for i in range(n)]
 
+    def trace_batch(self, sources, depth_ptr: int, max_levels: int = 100000):
+        """Per-level trace of one batched run (host-driven, same kernels)."""
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        buf = (_Trace * max_levels)()
+        n = C.c_int32()
+        _check(lib().ent_bfs_batch_trace(self.handle, _i32p(src), len(src), C.c_void_p(depth_ptr), buf, max_levels,
+                                         C.byref(n)))
+        return [{f[0]: getattr(buf[i], f[0]) for f in _Trace._fields_ if f[0] != "pad"} for i in range(n.value)]
+
     def bfs_batch_device(self, sources, depth_ptr: int, stream: int = 0, stats: bool = True):
         src = np.ascontiguousarray(sources, dtype=np.int32)
         n = len(src)
@@ -427,6 +441,41 @@ class Graph:
 
     def __exit__(self, *exc):
         self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MultiPlan:
+    """Many graphs (one GPU) with their own sources, traversed by one launch."""
+
+    def __init__(self, graphs: Sequence[Graph], sources: Sequence[Sequence[int]]):
+        self.graphs = list(graphs)
+        self.counts = [len(s) for s in sources]
+        hs = (_P * len(graphs))(*[g.handle for g in graphs])
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(s, dtype=np.int32) for s in sources]), dtype=np.int32)
+        counts = np.array(self.counts, dtype=np.int32)
+        h = _P()
+        _check(lib().ent_multi_create(hs, len(graphs), _i32p(flat), _i32p(counts), C.byref(h)))
+        self._h = h
+
+    def run(self) -> float:
+        ms = C.c_double()
+        _check(lib().ent_multi_run(self._h, C.byref(ms)))
+        return ms.value
+
+    def depths(self, k: int) -> np.ndarray:
+        out = np.empty((self.counts[k], self.graphs[k].vert_count), dtype=np.int32)
+        _check(lib().ent_multi_depths(self._h, k, _i32p(out)))
+        return out
+
+    def close(self):
+        if self._h is not None:
+            lib().ent_multi_destroy(self._h)
+            self._h = None
 
     def __del__(self):
         try:

@@ -1,18 +1,1327 @@
-// Bitwise multi-source BFS (placeholder until the batched kernels land).
+// Bitwise multi-source BFS (many sources per launch) for sm_100a.
+//
+// No reference code exists for this path: the reference runs its 64 sources
+// one after another (bfs_gpu_opt.cuh:370-432) and only cites the iBFS paper
+// (readme.md:79). The design follows the published idea (Liu, Huang, Hu,
+// "iBFS: Concurrent Breadth-First Search on GPUs", SIGMOD'16): one bit per
+// source in a shared per-vertex status word, so one adjacency read serves
+// every source that reaches the vertex at that level.
+//
+// Layout (per graph, W = words per vertex, a power of two >= n_src/64):
+//   X    uint64[V][W]      visited bits
+//   log  uint64[K][V][W]   ring of K levels: log[L-base][v] = bits found at level L
+//   jf   int32[2][V]       joint frontier (vertices with any new bit), ping-pong
+//   heavy int32[2][V]      joint-frontier vertices of degree >= HEAVY
+//   done bit per vertex    every source has visited it (bottom-up skips it)
+//   jfb  bit per vertex    [2] joint-frontier membership of levels L and L+1:
+//                          dedups top-down claims and lets bottom-up skip the
+//                          frontier-word gather of neighbours outside the frontier
+// A level is top-down (frontier-driven, atomicOr of new bits, then a commit
+// pass) or bottom-up (every unfinished vertex ORs its neighbours' frontier
+// words, stopping once all its missing bits are covered). Depths are never
+// scattered during the traversal: a flush kernel turns the log into the
+// source-major int32 depth rows, 32 vertices x 64 sources per warp, with
+// coalesced 128-byte row writes.
+#include <algorithm>
+#include <string.h>
+#include <vector>
+
+#include "dev_common.cuh"
 #include "dev_graph.h"
+
 namespace ent {
-struct BatchWorkspace {};
-void destroy_batch_workspace(BatchWorkspace* w) { delete w; }
+
+constexpr int BB = 256;        // threads per CTA
+constexpr int HEAVY = 4096;    // top-down: degree at which all CTAs share a vertex
+constexpr int KMAX = 16;       // log slots (levels per flush window)
+constexpr int SMALLB = 32;     // bottom-up: below this degree a lane group owns a vertex
+constexpr int LARGEB = 1024;   // bottom-up: from this degree a CTA owns a vertex
+constexpr int WMAX = 32;       // words per vertex per launch (2048 sources)
+
+struct BatchCtl {
+  int32_t level;     // level of the frontier being expanded
+  int32_t dir;       // 0 top-down, 1 bottom-up
+  int32_t done;
+  int32_t err;
+  int32_t cur;       // jf / heavy ping-pong index
+  int32_t n_jf[2];
+  int32_t n_heavy[2];
+  int32_t base;      // level stored in log slot 0
+  int32_t windows;   // flush windows completed
+  int32_t flush_now; // the window is full: flush before the next level
+  int32_t td_levels, bu_levels;
+  int32_t n_src;
+  int32_t pad;
+  int32_t* depth;    // [n_src][V] output of this run
+  unsigned long long acc_m, acc_mdone;
+  int64_t m_f, m_done;
+  uint32_t finished;
+  uint32_t pad2;
+};
+
+struct BatchArgs {
+  BatchCtl* ctl;
+  const int64_t* off;
+  const int32_t* adj;
+  const int32_t* deg;
+  const uint32_t* active;
+  int64_t V, E;
+  int32_t W, lgW;       // words per vertex and log2(W)
+  int32_t K;            // log slots in use
+  unsigned long long* X;
+  unsigned long long* log;
+  const unsigned long long* mask;  // [W] valid source bits
+  uint32_t* donebits;
+  uint32_t* jfb[2];
+  const uint32_t* lightbits;  // degree in [1, SMALLB): bottom-up light tier
+  const int32_t* mid;         // vertices with SMALLB <= degree < LARGEB
+  const int32_t* large;       // vertices with degree >= LARGEB
+  int32_t n_mid, n_large;
+  int32_t* jf[2];
+  int32_t* heavy[2];
+  const int32_t* src;   // [n_src]
+  unsigned long long* st_edges;  // per source: sum of degrees of reached vertices
+  unsigned long long* st_verts;  // per source: reached vertices
+  int32_t* st_maxd;              // per source: max depth
+  double alpha;
+  cudaGraphConditionalHandle cond;
+  int32_t use_cond;
+  int32_t max_levels;
+};
+
+__device__ __forceinline__ unsigned long long* slot_ptr(const BatchArgs& a, int slot) {
+  return a.log + (size_t)slot * (size_t)a.V * a.W;
+}
+
+template <class T>
+__device__ __forceinline__ T bsum(T x, T* s_red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL, x, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = x;
+  __syncthreads();
+  T r = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < BB / 32; ++w) r += s_red[w];
+  return r;
+}
+
+// Warp-aggregated append of v (when `want`) to list, counter *n.
+__device__ __forceinline__ void wappend(bool want, int v, int32_t* list, int32_t* n) {
+  const unsigned m = __ballot_sync(FULL, want);
+  if (!m) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(n, __popc(m));
+  base = __shfl_sync(FULL, base, leader);
+  if (want) list[base + __popc(m & lanemask_lt())] = v;
+}
+
+// ------------------------------------------------------------ seeding -----
+// Runs after X, donebits and both jfb bitmaps are zeroed (memset nodes). One CTA.
+__global__ void k_b_seed(BatchArgs a) {
+  BatchCtl* c = a.ctl;
+  unsigned long long* s0 = slot_ptr(a, 0);
+  __shared__ int s_n, s_h;
+  __shared__ unsigned long long s_m;
+  if (threadIdx.x == 0) { s_n = 0; s_h = 0; s_m = 0; }
+  __syncthreads();
+  for (int s = threadIdx.x; s < c->n_src; s += blockDim.x) {
+    const int v = a.src[s];
+    const unsigned long long bit = 1ull << (s & 63);
+    atomicOr(&a.X[(size_t)v * a.W + (s >> 6)], bit);
+    atomicOr(&s0[(size_t)v * a.W + (s >> 6)], bit);
+    const uint32_t tb = 1u << (v & 31);
+    if (!(atomicOr(&a.jfb[0][v >> 5], tb) & tb)) {
+      a.jf[0][atomicAdd(&s_n, 1)] = v;
+      const int d = a.deg[v];
+      atomicAdd(&s_m, (unsigned long long)d);
+      if (d >= HEAVY) a.heavy[0][atomicAdd(&s_h, 1)] = v;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    c->level = 0;
+    c->dir = 0;
+    c->done = s_n == 0;
+    c->err = 0;
+    c->cur = 0;
+    c->n_jf[0] = s_n;
+    c->n_jf[1] = 0;
+    c->n_heavy[0] = s_h;
+    c->n_heavy[1] = 0;
+    c->base = 0;
+    c->windows = 0;
+    c->flush_now = 0;
+    c->td_levels = 0;
+    c->bu_levels = 0;
+    c->acc_m = 0;
+    c->acc_mdone = 0;
+    c->m_f = (int64_t)s_m;
+    c->m_done = 0;
+    c->finished = 0;
+    __threadfence();
+  }
+}
+
+// ----------------------------------------------------------- top-down -----
+// Claims the bits of frontier vertex u (frontier words fu) for neighbour v.
+__device__ __forceinline__ void td_edge(const BatchArgs& a, BatchCtl* c, const unsigned long long* fu, int v,
+                                        bool valid, unsigned long long* nb, int nxt) {
+  bool first = false;
+  if (valid) {
+    const unsigned long long* xv = a.X + (size_t)v * a.W;
+    bool any = false;
+    for (int w = 0; w < a.W; ++w) {
+      const unsigned long long f = fu[w];
+      if (!f) continue;
+      const unsigned long long b = f & ~__ldg(xv + w);
+      if (b) {
+        atomicOr(nb + (size_t)v * a.W + w, b);
+        any = true;
+      }
+    }
+    if (any) {
+      const uint32_t tb = 1u << (v & 31);
+      first = !(atomicOr(&a.jfb[nxt][v >> 5], tb) & tb);
+    }
+  }
+  wappend(first, v, a.jf[nxt], &c->n_jf[nxt]);
+}
+
+__device__ void b_td_expand(const BatchArgs& a, BatchCtl* c, unsigned long long* s_f) {
+  const int cur = c->cur, nxt = cur ^ 1;
+  const int slot = c->level - c->base;
+  const unsigned long long* F = slot_ptr(a, slot);
+  unsigned long long* NB = slot_ptr(a, slot + 1);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // Heavy frontier vertices: every CTA takes an interleaved slice of the edges.
+  const int nh = c->n_heavy[cur];
+  for (int h = 0; h < nh; ++h) {
+    const int u = a.heavy[cur][h];
+    __syncthreads();
+    for (int w = threadIdx.x; w < a.W; w += BB) s_f[w] = F[(size_t)u * a.W + w];
+    __syncthreads();
+    const int64_t beg = a.off[u], end = a.off[u + 1];
+    for (int64_t e0 = beg + (int64_t)blockIdx.x * BB; e0 < end; e0 += (int64_t)gridDim.x * BB) {
+      const int64_t e = e0 + threadIdx.x;
+      const bool valid = e < end;
+      td_edge(a, c, s_f, valid ? __ldg(a.adj + e) : 0, valid, NB, nxt);
+    }
+  }
+  // Light frontier vertices: one warp each; the warp keeps F[u] in shared memory.
+  __syncthreads();
+  unsigned long long* fw = s_f + (size_t)warp * a.W;
+  const int n = c->n_jf[cur];
+  const int gw = (blockIdx.x * BB + threadIdx.x) >> 5, nw = (gridDim.x * BB) >> 5;
+  for (int i = gw; i < n; i += nw) {
+    const int u = a.jf[cur][i];
+    const int64_t beg = a.off[u], end = a.off[u + 1];
+    if (end - beg >= HEAVY) continue;
+    __syncwarp();
+    for (int w = lane; w < a.W; w += 32) fw[w] = F[(size_t)u * a.W + w];
+    __syncwarp();
+    for (int64_t e0 = beg; e0 < end; e0 += 32) {
+      const int64_t e = e0 + lane;
+      const bool valid = e < end;
+      td_edge(a, c, fw, valid ? __ldg(a.adj + e) : 0, valid, NB, nxt);
+    }
+  }
+}
+
+// ----------------------------------------------------------- bottom-up ----
+// Reads WPL consecutive frontier words (8*WPL-byte aligned) with 16-byte loads.
+template <int WPL>
+__device__ __forceinline__ void load_words(const unsigned long long* p, unsigned long long (&f)[WPL]) {
+  if constexpr (WPL == 1) {
+    f[0] = __ldg(p);
+  } else {
+#pragma unroll
+    for (int j = 0; j < WPL; j += 2) {
+      const ulonglong2 x = __ldg(reinterpret_cast<const ulonglong2*>(p + j));
+      f[j] = x.x;
+      f[j + 1] = x.y;
+    }
+  }
+}
+
+// Records the outcome of one bottom-up vertex (called by the lane that owns
+// the vertex): frontier append, counters, completion bit.
+__device__ __forceinline__ void bu_finish_vertex(const BatchArgs& a, BatchCtl* c, int v, int nxt, bool gany,
+                                                 bool gfull, int64_t d, unsigned long long& my_m,
+                                                 unsigned long long& my_md) {
+  if (gany) {
+    my_m += (unsigned long long)d;
+    atomicOr(&a.jfb[nxt][v >> 5], 1u << (v & 31));
+    a.jf[nxt][atomicAdd(&c->n_jf[nxt], 1)] = v;
+    if (d >= HEAVY) a.heavy[nxt][atomicAdd(&c->n_heavy[nxt], 1)] = v;
+  }
+  if (gfull) {
+    atomicOr(&a.donebits[v >> 5], 1u << (v & 31));
+    if (gany) my_md += (unsigned long long)d;
+  }
+}
+
+// Mid tier (SMALLB <= degree < LARGEB): one warp per vertex. Lane = (word w,
+// neighbour slot k): lanes w, w+W, w+2W, ... OR word w of different
+// neighbours, so a lane keeps one accumulator and the W consecutive words of
+// a neighbour are read by W consecutive lanes.
+__device__ void b_bu_mid(const BatchArgs& a, BatchCtl* c, const unsigned long long* F, unsigned long long* NB,
+                         unsigned long long& my_m, unsigned long long& my_md) {
+  const int W = a.W;
+  const int lane = threadIdx.x & 31;
+  const int w = lane % W, k = lane / W, NS = 32 / W;
+  const int nxt = c->cur ^ 1;
+  const int gw = (blockIdx.x * BB + threadIdx.x) >> 5, nw = (gridDim.x * BB) >> 5;
+  const unsigned long long mk = a.mask[w];
+  const uint32_t* jfc = a.jfb[c->cur];
+  for (int i = gw; i < a.n_mid; i += nw) {
+    const int v = a.mid[i];
+    if ((a.donebits[v >> 5] >> (v & 31)) & 1u) continue;
+    const unsigned long long xv = a.X[(size_t)v * W + w];
+    const unsigned long long need = mk & ~xv;
+    if (!__any_sync(FULL, need != 0)) continue;
+    const int64_t beg = a.off[v], end = a.off[v + 1];
+    unsigned long long acc = 0, r = 0;
+    for (int64_t e0 = beg; e0 < end; e0 += NS) {
+      const int64_t e = e0 + k;
+      if (e < end) {
+        const int u = __ldg(a.adj + e);
+        if ((__ldg(jfc + (u >> 5)) >> (u & 31)) & 1u) acc |= __ldg(F + (size_t)u * W + w);
+      }
+      r = acc;
+      for (int o = W; o < 32; o <<= 1) r |= __shfl_xor_sync(FULL, r, o);
+      if (__all_sync(FULL, (r & need) == need)) break;
+    }
+    r = acc;
+    for (int o = W; o < 32; o <<= 1) r |= __shfl_xor_sync(FULL, r, o);
+    const unsigned long long nw_ = r & need;
+    if (k == 0 && nw_) {
+      NB[(size_t)v * W + w] = nw_;
+      a.X[(size_t)v * W + w] = xv | nw_;
+    }
+    const bool gany = __any_sync(FULL, nw_ != 0);
+    const bool gfull = __all_sync(FULL, ((xv | nw_) & mk) == mk);
+    if (lane == 0) bu_finish_vertex(a, c, v, nxt, gany, gfull, end - beg, my_m, my_md);
+  }
+}
+
+// Large tier (degree >= LARGEB): one CTA per vertex, reduced through shared
+// memory, early exit by block vote.
+__device__ void b_bu_large(const BatchArgs& a, BatchCtl* c, const unsigned long long* F, unsigned long long* NB,
+                           unsigned long long& my_m, unsigned long long& my_md) {
+  __shared__ unsigned long long s_acc[32], s_need[32], s_x[32];
+  __shared__ int s_skip;
+  const int W = a.W;
+  const int t = threadIdx.x, w = t % W, k = t / W, NS = BB / W;
+  const int nxt = c->cur ^ 1;
+  const uint32_t* jfc = a.jfb[c->cur];
+  for (int i = blockIdx.x; i < a.n_large; i += gridDim.x) {
+    const int v = a.large[i];
+    __syncthreads();
+    if (t < W) {
+      const unsigned long long x = a.X[(size_t)v * W + t];
+      s_x[t] = x;
+      s_need[t] = a.mask[t] & ~x;
+      s_acc[t] = 0;
+    }
+    if (t == 0) s_skip = (a.donebits[v >> 5] >> (v & 31)) & 1u;
+    __syncthreads();
+    bool need_any = t < W && s_need[t] != 0;
+    if (s_skip || !__syncthreads_or(need_any)) continue;
+    const int64_t beg = a.off[v], end = a.off[v + 1];
+    for (int64_t e0 = beg; e0 < end; e0 += NS) {
+      const int64_t e = e0 + k;
+      if (e < end) {
+        const int u = __ldg(a.adj + e);
+        if ((__ldg(jfc + (u >> 5)) >> (u & 31)) & 1u) {
+          const unsigned long long f = __ldg(F + (size_t)u * W + w);
+          if (f) atomicOr(&s_acc[w], f);
+        }
+      }
+      __syncthreads();
+      const bool open = t < W && (s_acc[t] & s_need[t]) != s_need[t];
+      if (!__syncthreads_or(open)) break;
+    }
+    __syncthreads();
+    bool got = false, full = true;
+    if (t < W) {
+      const unsigned long long nw_ = s_acc[t] & s_need[t];
+      if (nw_) {
+        NB[(size_t)v * W + t] = nw_;
+        a.X[(size_t)v * W + t] = s_x[t] | nw_;
+        got = true;
+      }
+      full = ((s_x[t] | nw_) & a.mask[t]) == a.mask[t];
+    }
+    const bool gany = __syncthreads_or(got);
+    const bool gfull = !__syncthreads_or(!full);
+    if (t == 0) bu_finish_vertex(a, c, v, nxt, gany, gfull, end - beg, my_m, my_md);
+  }
+}
+
+// Light tier (degree < SMALLB): a group of G = W / WPL lanes handles one
+// vertex; each lane owns WPL words.
+template <int WPL>
+__device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long* s_red) {
+  const int cur = c->cur, nxt = cur ^ 1;
+  const int slot = c->level - c->base;
+  const unsigned long long* F = slot_ptr(a, slot);
+  unsigned long long* NB = slot_ptr(a, slot + 1);
+  const int G = a.W / WPL;  // lanes per vertex (1..32)
+  const int VPW = 32 / G;   // vertices per warp round
+  const int lane = threadIdx.x & 31;
+  const int gl = lane % G;  // lane within group
+  const int grp = lane / G;
+  const unsigned gmask = (G == 32) ? FULL : (((1u << G) - 1) << (grp * G));
+  const int64_t gtid = blockIdx.x * (int64_t)BB + threadIdx.x, nth = (int64_t)gridDim.x * BB;
+  const int64_t gw = gtid >> 5, nw = nth >> 5;
+  const int64_t Wd = (a.V + 31) >> 5;
+  unsigned long long mk[WPL];
+#pragma unroll
+  for (int j = 0; j < WPL; ++j) mk[j] = a.mask[gl * WPL + j];
+  const uint32_t* jfc = a.jfb[cur];
+  unsigned long long my_m = 0, my_md = 0;
+  for (int64_t wi = gw; wi < Wd; wi += nw) {
+    const uint32_t todo_word = a.lightbits[wi] & ~a.donebits[wi];
+    if (!todo_word) continue;
+    uint32_t full_bits = 0, front_bits = 0;
+    for (int r = 0; r < G; ++r) {
+      const int vl = r * VPW + grp;
+      if (!((todo_word >> (r * VPW)) & (VPW == 32 ? FULL : ((1u << VPW) - 1)))) continue;
+      const bool todo = (todo_word >> vl) & 1u;
+      const int64_t v = wi * 32 + vl;
+      unsigned long long need[WPL], acc[WPL];
+      bool any_need = false;
+      int64_t e0 = 0, e1 = 0;
+      if (todo) {
+        const unsigned long long* xv = a.X + (size_t)v * a.W + gl * WPL;
+#pragma unroll
+        for (int j = 0; j < WPL; ++j) {
+          need[j] = mk[j] & ~xv[j];
+          acc[j] = 0;
+          any_need |= need[j] != 0;
+        }
+        e0 = a.off[v];
+        e1 = a.off[v + 1];
+      }
+      // the whole group scans the row together (same trip count)
+      if (todo) {
+        bool cover = !(__ballot_sync(gmask, any_need) & gmask);
+        // two neighbours per step: both gathers are in flight together
+        for (int64_t e = e0; e < e1 && !cover; e += 2) {
+          const int u0 = __ldg(a.adj + e);
+          const int u1 = e + 1 < e1 ? __ldg(a.adj + e + 1) : u0;
+          unsigned long long f0[WPL], f1[WPL];
+#pragma unroll
+          for (int j = 0; j < WPL; ++j) f0[j] = f1[j] = 0;
+          if ((__ldg(jfc + (u0 >> 5)) >> (u0 & 31)) & 1u) load_words<WPL>(F + (size_t)u0 * a.W + gl * WPL, f0);
+          if ((__ldg(jfc + (u1 >> 5)) >> (u1 & 31)) & 1u) load_words<WPL>(F + (size_t)u1 * a.W + gl * WPL, f1);
+          bool mine = true;
+#pragma unroll
+          for (int j = 0; j < WPL; ++j) {
+            acc[j] |= f0[j] | f1[j];
+            mine &= (acc[j] & need[j]) == need[j];
+          }
+          cover = (__ballot_sync(gmask, mine) & gmask) == gmask;
+        }
+        bool got = false, full = true;
+        unsigned long long* nbv = NB + (size_t)v * a.W + gl * WPL;
+        unsigned long long* xw = a.X + (size_t)v * a.W + gl * WPL;
+#pragma unroll
+        for (int j = 0; j < WPL; ++j) {
+          const unsigned long long nw_ = acc[j] & need[j];
+          if (nw_) {
+            nbv[j] = nw_;
+            xw[j] = (mk[j] & ~need[j]) | nw_ | (xw[j] & ~mk[j]);
+            got = true;
+          }
+          full &= (need[j] & ~nw_) == 0;
+        }
+        const bool gany = (__ballot_sync(gmask, got) & gmask) != 0;
+        const bool gfull = (__ballot_sync(gmask, full) & gmask) == gmask;
+        if (gl == 0 && gany) my_m += (unsigned long long)(e1 - e0);
+        if (gl == 0 && gfull) {
+          full_bits |= 1u << vl;
+          if (gany) my_md += (unsigned long long)(e1 - e0);
+        }
+        if (gl == 0 && gany && e1 - e0 >= HEAVY) {
+          const int at = atomicAdd(&c->n_heavy[nxt], 1);
+          a.heavy[nxt][at] = (int)v;
+        }
+        // append v to the next joint frontier (one lane per group)
+        if (gl == 0 && gany) {
+          const int at = atomicAdd(&c->n_jf[nxt], 1);
+          a.jf[nxt][at] = (int)v;
+          front_bits |= 1u << vl;
+        }
+      }
+    }
+    // vertices found complete (every source) become done
+    full_bits = __reduce_or_sync(FULL, full_bits);
+    front_bits = __reduce_or_sync(FULL, front_bits);
+    if (lane == 0 && full_bits) atomicOr(&a.donebits[wi], full_bits);
+    if (lane == 0 && front_bits) atomicOr(&a.jfb[nxt][wi], front_bits);
+  }
+  b_bu_mid(a, c, F, NB, my_m, my_md);
+  b_bu_large(a, c, F, NB, my_m, my_md);
+  const int any = __syncthreads_or(my_m != 0 || my_md != 0);
+  if (any) {
+    unsigned long long r = bsum(my_m, s_red);
+    if (threadIdx.x == 0) atomicAdd(&c->acc_m, r);
+    r = bsum(my_md, s_red);
+    if (threadIdx.x == 0) atomicAdd(&c->acc_mdone, r);
+  }
+}
+
+__global__ void __launch_bounds__(BB, 4) k_b_expand(BatchArgs a) {
+  extern __shared__ unsigned long long s_f[];
+  __shared__ unsigned long long s_red[BB / 32];
+  BatchCtl* c = a.ctl;
+  if (c->done) return;
+  if (c->dir == 0) {
+    b_td_expand(a, c, s_f);
+  } else {
+    if (a.W == 1) b_bu_expand<1>(a, c, s_red);
+    else if (a.W == 2) b_bu_expand<2>(a, c, s_red);
+    else b_bu_expand<4>(a, c, s_red);
+  }
+}
+
+// ----------------------------------------------------------- commit -------
+// Top-down: fold the claimed bits into X and count. Both directions: clear
+// the frontier bitmap of level L (jfb[cur], its words hold only jf[cur]). Then the
+// last CTA advances the level and picks the next direction.
+__global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
+  __shared__ unsigned long long s_red[BB / 32];
+  __shared__ int s_last;
+  BatchCtl* c = a.ctl;
+  if (c->done) return;
+  const int cur = c->cur, nxt = cur ^ 1;
+  const int dir = c->dir;
+  {
+    // frontier bitmap of level L: only words of jf[cur] vertices are set
+    const int64_t gtid = blockIdx.x * (int64_t)BB + threadIdx.x, nth = (int64_t)gridDim.x * BB;
+    const int nc = c->n_jf[cur];
+    for (int64_t i = gtid; i < nc; i += nth) a.jfb[cur][(uint32_t)a.jf[cur][i] >> 5] = 0;
+  }
+  if (dir == 0) {
+    const int slot = c->level - c->base;
+    const unsigned long long* NB = slot_ptr(a, slot + 1);
+    const int n = c->n_jf[nxt];
+    unsigned long long my_m = 0, my_md = 0;
+    const int64_t gtid = blockIdx.x * (int64_t)BB + threadIdx.x, nth = (int64_t)gridDim.x * BB;
+    for (int64_t i = gtid; i < n; i += nth) {
+      const int v = a.jf[nxt][i];
+      bool full = true;
+      for (int w = 0; w < a.W; ++w) {
+        const unsigned long long x = a.X[(size_t)v * a.W + w] | NB[(size_t)v * a.W + w];
+        a.X[(size_t)v * a.W + w] = x;
+        full &= (x & a.mask[w]) == a.mask[w];
+      }
+      const int d = a.deg[v];
+      my_m += d;
+      if (full) {
+        atomicOr(&a.donebits[v >> 5], 1u << (v & 31));
+        my_md += d;
+      }
+      if (d >= HEAVY) a.heavy[nxt][atomicAdd(&c->n_heavy[nxt], 1)] = v;
+    }
+    if (__syncthreads_or(my_m != 0 || my_md != 0)) {
+      unsigned long long r = bsum(my_m, s_red);
+      if (threadIdx.x == 0) atomicAdd(&c->acc_m, r);
+      r = bsum(my_md, s_red);
+      if (threadIdx.x == 0) atomicAdd(&c->acc_mdone, r);
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&c->finished, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  volatile BatchCtl* vc = c;
+  const int64_t n_next = vc->n_jf[nxt];
+  const int64_t m_next = (int64_t)vc->acc_m;
+  vc->m_done = vc->m_done + (int64_t)vc->acc_mdone;
+  if (dir == 0) vc->td_levels = vc->td_levels + 1; else vc->bu_levels = vc->bu_levels + 1;
+  const int L = vc->level + 1;
+  vc->level = L;
+  vc->cur = nxt;
+  vc->n_jf[cur] = 0;
+  vc->n_heavy[cur] = 0;
+  vc->m_f = m_next;
+  const double m_u = (double)(a.E - vc->m_done);
+  vc->dir = ((double)m_next * a.alpha > m_u) ? 1 : 0;
+  int done = n_next == 0;
+  if (L >= a.max_levels && !done) {
+    vc->err = vc->err | 4;
+    done = 1;
+  }
+  vc->done = done;
+  // The next level writes slot L+1-base: flush first if it would not fit.
+  vc->flush_now = !done && (L + 1 - vc->base >= a.K);
+  vc->acc_m = 0;
+  vc->acc_mdone = 0;
+  vc->finished = 0;
+  __threadfence();
+  if (a.use_cond) cudaGraphSetConditional(a.cond, done ? 0u : 1u);
+}
+
+// ----------------------------------------------------------- flush --------
+// Converts log slots [first, last] (levels base+first .. base+last) into the
+// source-major depth rows. A CTA takes a span of vertices and walks the W
+// word columns in groups of CG = min(W, 4): it reads each vertex's CG words
+// of a slot with one 8*CG-byte load (whole sectors), decodes the 64*CG
+// sources into a shared byte tile [source][vertex] (slot index or 0xFF), then
+// each warp writes whole row segments (VS int32 contiguous, 16-byte stores)
+// and reduces that row's statistics once. The first window writes every
+// (source, vertex) pair (-1 where not found); later windows only the pairs
+// they found. Recycling the slots (zeroing, carrying the last one into slot
+// 0) is left to k_b_recycle, which streams them contiguously.
+constexpr int TILE_BYTES = 64 * 1024;  // 64*CG rows x VS vertices
+constexpr int FLUSH_TILE_BYTES = TILE_BYTES + 1024 * 4;
+
+template <int CG>
+__device__ __forceinline__ void load_cols(const unsigned long long* p, unsigned long long (&w)[CG]) {
+  if constexpr (CG == 1) {
+    w[0] = *p;
+  } else {
+#pragma unroll
+    for (int j = 0; j < CG; j += 2) {
+      const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(p + j);
+      w[j] = x.x;
+      w[j + 1] = x.y;
+    }
+  }
+}
+
+template <int CG>
+__device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, int last, int base, int windows,
+                           int nsrc, int32_t* depth, bool vec_ok, unsigned char* tile, const int* s_deg,
+                           unsigned* s_cnt, int* s_maxd, unsigned long long* s_edg) {
+  constexpr int VS = TILE_BYTES / (64 * CG);  // vertices per pass
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t sub = 0; sub < nv; sub += VS) {
+    const int nsub = (int)min((int64_t)VS, (int64_t)nv - sub);
+    for (int cg = 0; cg < a.W; cg += CG) {
+      if (cg * 64 >= nsrc) break;
+      int4* t4 = reinterpret_cast<int4*>(tile);
+      for (int i = threadIdx.x; i < TILE_BYTES / 16; i += BB) t4[i] = make_int4(-1, -1, -1, -1);
+      __syncthreads();
+      for (int vi = threadIdx.x; vi < nsub; vi += BB) {
+        const size_t at = (size_t)(v0 + sub + vi) * a.W + cg;
+        for (int k0 = first; k0 <= last; k0 += 4) {
+          unsigned long long w[4][CG];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if (k0 + q <= last) load_cols<CG>(slot_ptr(a, k0 + q) + at, w[q]);
+            else
+#pragma unroll
+              for (int cc = 0; cc < CG; ++cc) w[q][cc] = 0;
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int cc = 0; cc < CG; ++cc)
+              for (unsigned long long m = w[q][cc]; m; m &= m - 1)
+                tile[(cc * 64 + __ffsll((long long)m) - 1) * VS + vi] = (unsigned char)(k0 + q);
+        }
+      }
+      __syncthreads();
+      for (int r = warp; r < 64 * CG; r += BB / 32) {
+        const int s = cg * 64 + r;
+        if (s >= nsrc) break;
+        const uint32_t* row = reinterpret_cast<const uint32_t*>(tile + r * VS);
+        int32_t* out = depth + (size_t)s * a.V + v0 + sub;
+        const int* dg = s_deg + sub;
+        unsigned cnt = 0;
+        unsigned long long edg = 0;
+        int mx = -1;
+        for (int q = lane; q * 4 < nsub; q += 32) {
+          const uint32_t wq = row[q];
+          int dq[4];
+          bool fq[4];
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int vi = q * 4 + b;
+            const uint32_t byte = (wq >> (8 * b)) & 0xFFu;
+            fq[b] = vi < nsub && byte != 0xFFu;
+            dq[b] = fq[b] ? base + (int)byte : -1;
+            if (fq[b]) {
+              ++cnt;
+              edg += (unsigned long long)dg[vi];
+              mx = max(mx, dq[b]);
+            }
+          }
+          if (windows == 0 && vec_ok && q * 4 + 4 <= nsub) {
+            *reinterpret_cast<int4*>(out + q * 4) = make_int4(dq[0], dq[1], dq[2], dq[3]);
+          } else {
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+              if ((windows == 0 && q * 4 + b < nsub) || fq[b]) out[q * 4 + b] = dq[b];
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          cnt += __shfl_xor_sync(FULL, cnt, o);
+          edg += __shfl_xor_sync(FULL, edg, o);
+          mx = max(mx, __shfl_xor_sync(FULL, mx, o));
+        }
+        if (lane == 0 && cnt) {
+          s_cnt[s] += cnt;
+          s_edg[s] += edg;
+          s_maxd[s] = max(s_maxd[s], mx);
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void __launch_bounds__(BB) k_b_flush(BatchArgs a, int final_flush) {
+  extern __shared__ __align__(16) unsigned char s_flush[];
+  BatchCtl* c = a.ctl;
+  if (!final_flush && !c->flush_now) return;
+  const int base = c->base, windows = c->windows;
+  // final: levels base .. level-1 are in slots 0 .. level-1-base
+  const int last = final_flush ? (c->level - 1 - base) : (a.K - 1);
+  const int first = windows == 0 ? 0 : 1;
+  const int nsrc = c->n_src;
+  const int NSRC = a.W * 64;
+  unsigned char* tile = s_flush;
+  int* s_deg = reinterpret_cast<int*>(s_flush + TILE_BYTES);  // [1024]
+  unsigned* s_cnt = reinterpret_cast<unsigned*>(s_flush + FLUSH_TILE_BYTES);
+  int* s_maxd = reinterpret_cast<int*>(s_cnt + NSRC);
+  unsigned long long* s_edg = reinterpret_cast<unsigned long long*>(s_maxd + NSRC);
+  for (int i = threadIdx.x; i < NSRC; i += BB) { s_cnt[i] = 0; s_maxd[i] = -1; s_edg[i] = 0; }
+  int32_t* depth = c->depth;
+  const bool vec_ok = (a.V % 4 == 0) && ((((uintptr_t)depth) & 15) == 0);
+  const int64_t units = (a.V + 1023) / 1024;
+  for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+    const int64_t v0 = u * 1024;
+    const int nv = (int)min((int64_t)1024, a.V - v0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 1024; i += BB) s_deg[i] = i < nv ? a.deg[v0 + i] : 0;
+    __syncthreads();
+    if (a.W == 1) flush_span<1>(a, v0, nv, first, last, base, windows, nsrc, depth, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
+    else if (a.W == 2) flush_span<2>(a, v0, nv, first, last, base, windows, nsrc, depth, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
+    else flush_span<4>(a, v0, nv, first, last, base, windows, nsrc, depth, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < nsrc; s += BB) {
+    if (s_cnt[s]) {
+      atomicAdd(&a.st_verts[s], (unsigned long long)s_cnt[s]);
+      atomicAdd(&a.st_edges[s], s_edg[s]);
+      atomicMax(&a.st_maxd[s], s_maxd[s]);
+    }
+  }
+}
+
+// Recycles the log after a flush with contiguous streams: a window flush
+// copies slot K-1 (the next window's frontier) into slot 0 and zeroes slots
+// 1..K-1, then moves the window; the final flush zeroes slots 0..last.
+__global__ void __launch_bounds__(BB) k_b_recycle(BatchArgs a, int final_flush) {
+  BatchCtl* c = a.ctl;
+  if (!final_flush && !c->flush_now) return;
+  const int last = final_flush ? (c->level - 1 - c->base) : (a.K - 1);
+  const int64_t words = a.V * a.W;  // per slot
+  const int64_t tid = blockIdx.x * (int64_t)BB + threadIdx.x, nth = (int64_t)gridDim.x * BB;
+  // A slot starts at log + k*V*W words: 16-byte aligned for every k only when
+  // V*W is even (the log base is 256-byte aligned). Otherwise use 8-byte accesses.
+  const bool vec = (words & 1) == 0;
+  const ulonglong2 z = make_ulonglong2(0ull, 0ull);
+  for (int k = 0; k <= last; ++k) {
+    const bool copy = !final_flush && k == 0;
+    if (vec) {
+      ulonglong2* d = reinterpret_cast<ulonglong2*>(slot_ptr(a, k));
+      const ulonglong2* sp = reinterpret_cast<const ulonglong2*>(slot_ptr(a, last));
+      for (int64_t i = tid; i < words / 2; i += nth) d[i] = copy ? sp[i] : z;
+    } else {
+      unsigned long long* d = slot_ptr(a, k);
+      const unsigned long long* sp = slot_ptr(a, last);
+      for (int64_t i = tid; i < words; i += nth) d[i] = copy ? sp[i] : 0ull;
+    }
+  }
+  if (final_flush) return;
+  // the last CTA to finish moves the window
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&c->finished, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  volatile BatchCtl* vc = c;
+  vc->base = vc->base + a.K - 1;
+  vc->windows = vc->windows + 1;
+  vc->flush_now = 0;
+  vc->finished = 0;
+  __threadfence();
+}
+
+// Static degree tiers of a graph for the bottom-up pass (degrees never change).
+__global__ void k_b_tiers(const int32_t* __restrict__ deg, int64_t V, uint32_t* __restrict__ lightbits,
+                          int32_t* __restrict__ mid, int32_t* __restrict__ large, int32_t* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) & ~31ll; base < V; base += nth) {
+    const int64_t v = base + lane;
+    const int d = v < V ? deg[v] : 0;
+    const unsigned lb = __ballot_sync(FULL, d >= 1 && d < SMALLB);
+    if (lane == 0) lightbits[base >> 5] = lb;
+    wappend(d >= SMALLB && d < LARGEB, (int)v, mid, &counts[0]);
+    wappend(d >= LARGEB, (int)v, large, &counts[1]);
+  }
+}
+
+// ------------------------------------------------------------- host -------
+struct BatchWorkspace {
+  int64_t V = 0;
+  int W = 0, K = 0, cap_src = 0;
+  void* slab = nullptr;
+  BatchCtl* ctl = nullptr;
+  BatchCtl* ctl_h = nullptr;
+  int32_t* depth = nullptr;  // internal output for host-destination calls
+  size_t depth_cap = 0;
+  BatchArgs args;
+  int grid = 0, grid_flush = 0, grid_recycle = 0;
+  size_t smem = 0, smem_flush = 0;
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<unsigned long long> h_edges, h_verts;
+  std::vector<int32_t> h_maxd;
+  size_t x_bytes = 0, small_bytes = 0, stats_bytes = 0;
+  void* x_ptr = nullptr;      // X (memset per run)
+  void* small_ptr = nullptr;  // donebits + jfb[0..1] (memset per run)
+  void* stats_ptr = nullptr;  // per-source stats (memset per run)
+};
+
+void destroy_batch_workspace(BatchWorkspace* w) {
+  if (!w) return;
+  if (w->exec) cudaGraphExecDestroy(w->exec);
+  if (w->graph) cudaGraphDestroy(w->graph);
+  if (w->slab) cudaFree(w->slab);
+  if (w->ctl) cudaFree(w->ctl);
+  if (w->ctl_h) cudaFreeHost(w->ctl_h);
+  if (w->depth) cudaFree(w->depth);
+  if (w->ev0) cudaEventDestroy(w->ev0);
+  if (w->ev1) cudaEventDestroy(w->ev1);
+  delete w;
+}
+
+static int words_for(int n_src) {
+  int w = 1;
+  while (w * 64 < n_src) w <<= 1;
+  return w;
+}
+constexpr int MAX_BATCH = WMAX * 64;
+
+// Appends this graph's whole batched traversal to `graph` as an independent
+// branch: memsets -> seed -> while { expand, commit, flush } -> final flush.
+static int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream_t cap_stream) {
+  cudaGraphNode_t prev = nullptr;
+  auto add_memset = [&](void* p, size_t bytes) -> int {
+    cudaMemsetParams mp = {};
+    mp.dst = p;
+    mp.value = 0;
+    mp.elementSize = 1;
+    mp.width = bytes;
+    mp.height = 1;
+    cudaGraphNode_t n;
+    ENT_CUDA(cudaGraphAddMemsetNode(&n, graph, prev ? &prev : nullptr, prev ? 1 : 0, &mp));
+    prev = n;
+    return ENT_OK;
+  };
+  int rc;
+  if ((rc = add_memset(w->x_ptr, w->x_bytes))) return rc;
+  if ((rc = add_memset(w->small_ptr, w->small_bytes))) return rc;
+  if ((rc = add_memset(w->stats_ptr, w->stats_bytes))) return rc;
+  BatchArgs a0 = w->args;
+  a0.use_cond = 0;
+  {
+    void* kargs[1] = {&a0};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void*)k_b_seed;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(BB);
+    kp.kernelParams = kargs;
+    cudaGraphNode_t n;
+    ENT_CUDA(cudaGraphAddKernelNode(&n, graph, &prev, 1, &kp));
+    prev = n;
+  }
+  cudaGraphConditionalHandle handle;
+  ENT_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cond_node;
+  ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &prev, 1, &cp));
+  prev = cond_node;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  BatchArgs la = w->args;
+  la.cond = handle;
+  la.use_cond = 1;
+  ENT_CUDA(cudaStreamBeginCaptureToGraph(cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  k_b_expand<<<w->grid, BB, w->smem, cap_stream>>>(la);
+  k_b_commit<<<w->grid, BB, 0, cap_stream>>>(la);
+  k_b_flush<<<w->grid_flush, BB, w->smem_flush, cap_stream>>>(la, 0);
+  k_b_recycle<<<w->grid_recycle, BB, 0, cap_stream>>>(la, 0);
+  cudaGraph_t captured;
+  cudaError_t e = cudaStreamEndCapture(cap_stream, &captured);
+  if (e != cudaSuccess) return fail(ENT_ERR_CUDA, "batched level-loop capture failed: %s", cudaGetErrorString(e));
+  {
+    int fin = 1;
+    void* kargs[2] = {&a0, &fin};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void*)k_b_flush;
+    kp.gridDim = dim3(w->grid_flush);
+    kp.blockDim = dim3(BB);
+    kp.sharedMemBytes = (unsigned)w->smem_flush;
+    kp.kernelParams = kargs;
+    cudaGraphNode_t n;
+    ENT_CUDA(cudaGraphAddKernelNode(&n, graph, &prev, 1, &kp));
+    prev = n;
+    kp.func = (void*)k_b_recycle;
+    kp.gridDim = dim3(w->grid_recycle);
+    kp.sharedMemBytes = 0;
+    ENT_CUDA(cudaGraphAddKernelNode(&n, graph, &prev, 1, &kp));
+  }
+  return ENT_OK;
+}
+
+static int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
+  BatchWorkspace* w = new BatchWorkspace();
+  const int64_t V = g->V;
+  const int W = words_for(n_src);
+  w->V = V;
+  w->W = W;
+  w->K = KMAX;
+  w->cap_src = W * 64;
+  const int64_t Wd = (V + 31) / 32;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t sz_x = al(sizeof(unsigned long long) * V * W);
+  const size_t sz_log = al(sizeof(unsigned long long) * V * W * (size_t)w->K);
+  const size_t sz_bits = al(sizeof(uint32_t) * (Wd + 1));
+  const size_t sz_q = al(sizeof(int32_t) * (V + 4));
+  const size_t sz_mask = al(sizeof(unsigned long long) * W);
+  const size_t sz_src = al(sizeof(int32_t) * w->cap_src);
+  const size_t sz_st = al(sizeof(unsigned long long) * w->cap_src) * 2 + al(sizeof(int32_t) * w->cap_src);
+  const size_t total = sz_x + sz_log + 4 * sz_bits + 6 * sz_q + sz_mask + sz_src + sz_st + 256;
+  cudaError_t e = cudaMalloc(&w->slab, total);
+  if (e != cudaSuccess) { destroy_batch_workspace(w); return fail(ENT_ERR_OOM, "batch workspace (%zu bytes) failed", total); }
+  e = cudaMemset(w->slab, 0, total);
+  if (e == cudaSuccess) e = cudaMalloc(&w->ctl, sizeof(BatchCtl));
+  if (e == cudaSuccess) e = cudaMemset(w->ctl, 0, sizeof(BatchCtl));
+  if (e == cudaSuccess) e = cudaMallocHost(&w->ctl_h, sizeof(BatchCtl));
+  if (e == cudaSuccess) e = cudaEventCreate(&w->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&w->ev1);
+  if (e != cudaSuccess) { destroy_batch_workspace(w); return fail(ENT_ERR_OOM, "batch workspace setup failed"); }
+  char* p = (char*)w->slab;
+  BatchArgs& a = w->args;
+  memset(&a, 0, sizeof(a));
+  a.ctl = w->ctl;
+  a.off = g->off;
+  a.adj = g->trav;
+  a.deg = g->deg;
+  a.active = g->active;
+  a.V = V;
+  a.E = g->E;
+  a.W = W;
+  int lg = 0;
+  while ((1 << lg) < W) ++lg;
+  a.lgW = lg;
+  a.K = w->K;
+  a.X = (unsigned long long*)p; w->x_ptr = p; w->x_bytes = sz_x; p += sz_x;
+  a.log = (unsigned long long*)p; p += sz_log;
+  a.donebits = (uint32_t*)p; w->small_ptr = p; w->small_bytes = 3 * sz_bits; p += sz_bits;
+  a.jfb[0] = (uint32_t*)p; p += sz_bits;
+  a.jfb[1] = (uint32_t*)p; p += sz_bits;
+  for (int i = 0; i < 2; ++i) { a.jf[i] = (int32_t*)p; p += sz_q; }
+  for (int i = 0; i < 2; ++i) { a.heavy[i] = (int32_t*)p; p += sz_q; }
+  uint32_t* lightbits = (uint32_t*)p; p += sz_bits;
+  int32_t* mid = (int32_t*)p; p += sz_q;
+  int32_t* large = (int32_t*)p; p += sz_q;
+  int32_t* counts = (int32_t*)p; p += 256;
+  a.lightbits = lightbits;
+  a.mid = mid;
+  a.large = large;
+  a.mask = (const unsigned long long*)p; p += sz_mask;
+  a.src = (const int32_t*)p; p += sz_src;
+  w->stats_ptr = p;
+  w->stats_bytes = sz_st;
+  a.st_edges = (unsigned long long*)p; p += al(sizeof(unsigned long long) * w->cap_src);
+  a.st_verts = (unsigned long long*)p; p += al(sizeof(unsigned long long) * w->cap_src);
+  a.st_maxd = (int32_t*)p; p += al(sizeof(int32_t) * w->cap_src);
+  a.alpha = 4.0;
+  a.max_levels = (int32_t)std::min<int64_t>(V + 2, 0x7ffffff0);
+  w->smem = sizeof(unsigned long long) * std::max(W * (BB / 32), W);
+  {
+    const int blocks = (int)std::min<int64_t>((V + BB - 1) / BB, (int64_t)g->num_sms * 8);
+    k_b_tiers<<<blocks, BB, 0, g->stream>>>(g->deg, V, lightbits, mid, large, counts);
+    g_kernel_launches++;
+    int32_t hc[2] = {0, 0};
+    e = cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, g->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+    if (e != cudaSuccess) { destroy_batch_workspace(w); return fail(ENT_ERR_CUDA, "tier build failed: %s", cudaGetErrorString(e)); }
+    a.n_mid = hc[0];
+    a.n_large = hc[1];
+  }
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_expand, BB, w->smem);
+  if (occ < 1) occ = 1;
+  // small graphs get small grids so that the branches of a multi-graph
+  // launch can run side by side
+  const int64_t want = std::max<int64_t>(1, (V + BB * 8 - 1) / (BB * 8));
+  w->grid = (int)std::min<int64_t>((int64_t)g->num_sms * occ, want);
+  w->grid_flush = (int)std::min<int64_t>((int64_t)g->num_sms * 3, std::max<int64_t>(1, (V + 1023) / 1024));
+  w->grid_recycle = (int)std::min<int64_t>((int64_t)g->num_sms * 4, std::max<int64_t>(1, (V * W / 2 + BB - 1) / BB));
+  w->smem_flush = FLUSH_TILE_BYTES + (size_t)W * 64 * (4 + 4 + 8) + 16;
+  {
+    e = cudaFuncSetAttribute(k_b_flush, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->smem_flush);
+    if (e != cudaSuccess) { destroy_batch_workspace(w); return fail(ENT_ERR_CUDA, "flush smem attribute failed"); }
+  }
+  w->h_edges.resize(w->cap_src);
+  w->h_verts.resize(w->cap_src);
+  w->h_maxd.resize(w->cap_src);
+  *out = w;
+  return ENT_OK;
+}
+
+static int ensure_batch(ent_graph* g, int n_src) {
+  if (g->bws && g->bws->cap_src >= n_src && g->bws->W == words_for(n_src)) return ENT_OK;
+  if (g->bws) {
+    cudaStreamSynchronize(g->stream);
+    destroy_batch_workspace(g->bws);
+    g->bws = nullptr;
+  }
+  int rc = create_batch_workspace(g, n_src, &g->bws);
+  if (rc != ENT_OK) return rc;
+  BatchWorkspace* w = g->bws;
+  ENT_CUDA(cudaGraphCreate(&w->graph, 0));
+  rc = append_branch(g, w, w->graph, g->stream);
+  if (rc != ENT_OK) return rc;
+  ENT_CUDA(cudaGraphInstantiate(&w->exec, w->graph, 0));
+  return ENT_OK;
+}
+
+// Uploads sources, mask and the output pointer (the kernels read them from
+// device memory, so one instantiated graph serves every batch).
+static int stage_request(ent_graph*, BatchWorkspace* w, const int32_t* src, int32_t n_src, int32_t* depth_dev,
+                         cudaStream_t s) {
+  std::vector<unsigned long long> mask(w->W, 0);
+  for (int i = 0; i < n_src; ++i) mask[i >> 6] |= 1ull << (i & 63);
+  ENT_CUDA(cudaMemcpyAsync((void*)w->args.mask, mask.data(), sizeof(unsigned long long) * w->W, cudaMemcpyHostToDevice, s));
+  ENT_CUDA(cudaMemcpyAsync((void*)w->args.src, src, sizeof(int32_t) * n_src, cudaMemcpyHostToDevice, s));
+  BatchCtl init = {};
+  init.n_src = n_src;
+  init.depth = depth_dev;
+  ENT_CUDA(cudaMemcpyAsync(w->ctl, &init, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
+  return ENT_OK;
+}
+
+static int read_batch_stats(ent_graph* g, BatchWorkspace* w, int32_t n_src, cudaStream_t s, ent_stats* stats) {
+  ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+  ENT_CUDA(cudaMemcpyAsync(w->h_edges.data(), w->args.st_edges, sizeof(unsigned long long) * n_src, cudaMemcpyDeviceToHost, s));
+  ENT_CUDA(cudaMemcpyAsync(w->h_verts.data(), w->args.st_verts, sizeof(unsigned long long) * n_src, cudaMemcpyDeviceToHost, s));
+  ENT_CUDA(cudaMemcpyAsync(w->h_maxd.data(), w->args.st_maxd, sizeof(int32_t) * n_src, cudaMemcpyDeviceToHost, s));
+  ENT_CUDA(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, w->ev0, w->ev1);
+  for (int i = 0; i < n_src; ++i) {
+    stats[i].reached_vertices = (int64_t)w->h_verts[i];
+    stats[i].traversed_edges = (int64_t)w->h_edges[i];
+    stats[i].levels = w->h_maxd[i] + 1;
+    stats[i].td_levels = w->ctl_h->td_levels;
+    stats[i].bu_levels = w->ctl_h->bu_levels;
+    stats[i].status = w->ctl_h->err;
+    stats[i].device_ms = ms;
+  }
+  g_kernel_launches += 3 + 4 * (int64_t)w->ctl_h->level;
+  if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "batched traversal reported error flags 0x%x", w->ctl_h->err);
+  return ENT_OK;
+}
+
+int run_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, cudaStream_t stream,
+                  ent_stats* stats) {
+  for (int i = 0; i < n_src; ++i)
+    if (src[i] < 0 || src[i] >= g->V) return fail(ENT_ERR_INVALID_ARG, "source %d out of range", src[i]);
+  int rc = ensure_batch(g, n_src);
+  if (rc != ENT_OK) return rc;
+  BatchWorkspace* w = g->bws;
+  cudaStream_t s = stream ? stream : g->stream;
+  rc = stage_request(g, w, src, n_src, depth_dev, s);
+  if (rc != ENT_OK) return rc;
+  ENT_CUDA(cudaEventRecord(w->ev0, s));
+  ENT_CUDA(cudaGraphLaunch(w->exec, s));
+  ENT_CUDA(cudaEventRecord(w->ev1, s));
+  if (stats) return read_batch_stats(g, w, n_src, s, stats);
+  g_kernel_launches += 2;
+  return ENT_OK;
+}
+
 }  // namespace ent
+
 using namespace ent;
+
 extern "C" {
-int ent_bfs_batch(ent_graph*, const int32_t*, int32_t, int32_t*, ent_stats*) {
-  return fail(ENT_ERR_UNSUPPORTED, "batched traversal not built yet");
+
+int ent_bfs_batch_device(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, void* stream,
+                         ent_stats* stats) {
+  clear_error();
+  if (!g || !src || !depth_dev || n_src < 1) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
+  if (n_src > MAX_BATCH) return fail(ENT_ERR_UNSUPPORTED, "at most %d sources per batch", MAX_BATCH);
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard dg(g->device);
+  return run_bfs_batch(g, src, n_src, depth_dev, (cudaStream_t)stream, stats);
 }
-int ent_bfs_batch_device(ent_graph*, const int32_t*, int32_t, int32_t*, void*, ent_stats*) {
-  return fail(ENT_ERR_UNSUPPORTED, "batched traversal not built yet");
+
+int ent_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_out, ent_stats* stats) {
+  clear_error();
+  if (!g || !src || n_src < 1) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
+  if (n_src > MAX_BATCH) return fail(ENT_ERR_UNSUPPORTED, "at most %d sources per batch", MAX_BATCH);
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard dg(g->device);
+  int rc = ensure_batch(g, n_src);
+  if (rc != ENT_OK) return rc;
+  BatchWorkspace* w = g->bws;
+  const size_t need = sizeof(int32_t) * (size_t)n_src * g->V;
+  if (w->depth_cap < need) {
+    if (w->depth) cudaFree(w->depth);
+    w->depth = nullptr;
+    w->depth_cap = 0;
+    ENT_CUDA(cudaMalloc(&w->depth, need));
+    w->depth_cap = need;
+  }
+  std::vector<ent_stats> local(stats ? 0 : n_src);
+  rc = run_bfs_batch(g, src, n_src, w->depth, g->stream, stats ? stats : local.data());
+  if (rc != ENT_OK) return rc;
+  if (depth_out) ENT_CUDA(cudaMemcpyAsync(depth_out, w->depth, need, cudaMemcpyDeviceToHost, g->stream));
+  ENT_CUDA(cudaStreamSynchronize(g->stream));
+  return ENT_OK;
 }
-int ent_bfs_multi(ent_graph* const*, int32_t, const int32_t*, const int32_t*, int32_t* const*) {
-  return fail(ENT_ERR_UNSUPPORTED, "multi-graph traversal not built yet");
+
+// Host-driven run of a batch with CUDA events per level (tracing aid; same
+// kernels and results as ent_bfs_batch_device).
+int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, ent_level_trace* out,
+                        int32_t max_levels, int32_t* n_levels) {
+  clear_error();
+  if (!g || !src || !depth_dev || !out || !n_levels || n_src < 1 || max_levels < 1)
+    return fail(ENT_ERR_INVALID_ARG, "bad arguments");
+  if (n_src > MAX_BATCH) return fail(ENT_ERR_UNSUPPORTED, "at most %d sources per batch", MAX_BATCH);
+  for (int i = 0; i < n_src; ++i)
+    if (src[i] < 0 || src[i] >= g->V) return fail(ENT_ERR_INVALID_ARG, "source %d out of range", src[i]);
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard dg(g->device);
+  int rc = ensure_batch(g, n_src);
+  if (rc != ENT_OK) return rc;
+  BatchWorkspace* w = g->bws;
+  cudaStream_t s = g->stream;
+  rc = stage_request(g, w, src, n_src, depth_dev, s);
+  if (rc != ENT_OK) return rc;
+  ENT_CUDA(cudaMemsetAsync(w->x_ptr, 0, w->x_bytes, s));
+  ENT_CUDA(cudaMemsetAsync(w->small_ptr, 0, w->small_bytes, s));
+  ENT_CUDA(cudaMemsetAsync(w->stats_ptr, 0, w->stats_bytes, s));
+  BatchArgs a = w->args;
+  a.use_cond = 0;
+  k_b_seed<<<1, BB, 0, s>>>(a);
+  cudaEvent_t e[4];
+  for (int i = 0; i < 4; ++i) ENT_CUDA(cudaEventCreate(&e[i]));
+  int n = 0;
+  for (;;) {
+    ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+    ENT_CUDA(cudaStreamSynchronize(s));
+    const BatchCtl h = *w->ctl_h;
+    if (h.done || n >= max_levels) break;
+    ent_level_trace& t = out[n];
+    t.level = h.level;
+    t.direction = h.dir;
+    t.bu_sweep = h.dir;
+    t.pad = 0;
+    t.frontier_vertices = h.n_jf[h.cur];
+    t.frontier_edges = h.m_f;
+    t.unvisited_queued = (int64_t)g->E - h.m_done;
+    ENT_CUDA(cudaEventRecord(e[0], s));
+    k_b_expand<<<w->grid, BB, w->smem, s>>>(a);
+    ENT_CUDA(cudaEventRecord(e[1], s));
+    k_b_commit<<<w->grid, BB, 0, s>>>(a);
+    k_b_flush<<<w->grid_flush, BB, w->smem_flush, s>>>(a, 0);
+    k_b_recycle<<<w->grid_recycle, BB, 0, s>>>(a, 0);
+    ENT_CUDA(cudaEventRecord(e[2], s));
+    ENT_CUDA(cudaGetLastError());
+    ENT_CUDA(cudaEventSynchronize(e[2]));
+    float ta = 0, tb = 0;
+    cudaEventElapsedTime(&ta, e[0], e[1]);
+    cudaEventElapsedTime(&tb, e[1], e[2]);
+    t.expand_ms = ta;
+    t.inspect_ms = tb;
+    ++n;
+  }
+  ENT_CUDA(cudaEventRecord(e[0], s));
+  k_b_flush<<<w->grid_flush, BB, w->smem_flush, s>>>(a, 1);
+  k_b_recycle<<<w->grid_recycle, BB, 0, s>>>(a, 1);
+  ENT_CUDA(cudaEventRecord(e[1], s));
+  ENT_CUDA(cudaStreamSynchronize(s));
+  float tf = 0;
+  cudaEventElapsedTime(&tf, e[0], e[1]);
+  if (n < max_levels) {
+    ent_level_trace& t = out[n];
+    memset(&t, 0, sizeof(t));
+    t.level = -1;  // the final flush (depth rows + per-source stats)
+    t.inspect_ms = tf;
+    ++n;
+  }
+  for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]);
+  g_kernel_launches += 3 + 4 * (int64_t)n;
+  *n_levels = n;
+  if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "batched traversal error flags 0x%x", w->ctl_h->err);
+  return ENT_OK;
 }
+
+}  // extern "C"
+
+// Many graphs, one launch: each graph's batched traversal is an independent
+// branch (its own while node) of one CUDA graph.
+struct ent_multi {
+  std::vector<ent_graph*> graphs;
+  std::vector<int32_t> n_src;
+  std::vector<std::vector<int32_t>> src;
+  std::vector<int32_t*> depth;  // device outputs, one per graph
+  std::vector<BatchWorkspace*> ws;  // the plan's own traversal state per graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int device = 0;
+};
+
+static void multi_free(ent_multi* m) {
+  if (!m) return;
+  DeviceGuard dg(m->device);
+  if (m->exec) cudaGraphExecDestroy(m->exec);
+  if (m->graph) cudaGraphDestroy(m->graph);
+  for (int32_t* p : m->depth)
+    if (p) cudaFree(p);
+  for (BatchWorkspace* w : m->ws) destroy_batch_workspace(w);
+  if (m->ev0) cudaEventDestroy(m->ev0);
+  if (m->ev1) cudaEventDestroy(m->ev1);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
 }
+
+extern "C" {
+
+int ent_multi_create(ent_graph* const* graphs, int32_t n_graphs, const int32_t* src, const int32_t* n_src,
+                     ent_multi** out) {
+  clear_error();
+  if (!graphs || !src || !n_src || !out || n_graphs < 1) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
+  *out = nullptr;
+  const int dev = graphs[0]->device;
+  for (int k = 0; k < n_graphs; ++k) {
+    if (!graphs[k]) return fail(ENT_ERR_INVALID_ARG, "graph %d is null", k);
+    if (graphs[k]->device != dev) return fail(ENT_ERR_INVALID_ARG, "all graphs must be on one GPU");
+    if (n_src[k] < 1 || n_src[k] > MAX_BATCH) return fail(ENT_ERR_INVALID_ARG, "graph %d: bad source count", k);
+    for (int j = k + 1; j < n_graphs; ++j)
+      if (graphs[j] == graphs[k]) return fail(ENT_ERR_INVALID_ARG, "graph %d listed twice", k);
+  }
+  DeviceGuard dg(dev);
+  ent_multi* m = new ent_multi();
+  m->device = dev;
+  int64_t at = 0;
+  for (int k = 0; k < n_graphs; ++k) {
+    m->graphs.push_back(graphs[k]);
+    m->n_src.push_back(n_src[k]);
+    m->src.emplace_back(src + at, src + at + n_src[k]);
+    for (int32_t s : m->src.back())
+      if (s < 0 || s >= graphs[k]->V) {
+        multi_free(m);
+        return fail(ENT_ERR_INVALID_ARG, "graph %d: source %d out of range", k, s);
+      }
+    at += n_src[k];
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&m->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&m->ev1);
+  if (e == cudaSuccess) e = cudaGraphCreate(&m->graph, 0);
+  if (e != cudaSuccess) { multi_free(m); return fail(ENT_ERR_CUDA, "multi setup: %s", cudaGetErrorString(e)); }
+  for (int k = 0; k < n_graphs; ++k) {
+    ent_graph* g = graphs[k];
+    BatchWorkspace* w = nullptr;
+    int rc = create_batch_workspace(g, n_src[k], &w);
+    if (rc != ENT_OK) { multi_free(m); return rc; }
+    m->ws.push_back(w);
+    int32_t* d = nullptr;
+    e = cudaMalloc(&d, sizeof(int32_t) * (size_t)n_src[k] * g->V);
+    if (e != cudaSuccess) { multi_free(m); return fail(ENT_ERR_OOM, "multi output allocation failed"); }
+    m->depth.push_back(d);
+    rc = append_branch(g, w, m->graph, m->stream);
+    if (rc != ENT_OK) { multi_free(m); return rc; }
+  }
+  e = cudaGraphInstantiate(&m->exec, m->graph, 0);
+  if (e != cudaSuccess) { multi_free(m); return fail(ENT_ERR_CUDA, "multi instantiate: %s", cudaGetErrorString(e)); }
+  *out = m;
+  return ENT_OK;
+}
+
+int ent_multi_run(ent_multi* m, double* device_ms) {
+  clear_error();
+  if (!m) return fail(ENT_ERR_INVALID_ARG, "null plan");
+  DeviceGuard dg(m->device);
+  // hold every graph for the whole launch (pointer order avoids lock cycles)
+  std::vector<ent_graph*> order(m->graphs);
+  std::sort(order.begin(), order.end());
+  std::vector<std::unique_lock<std::mutex>> locks;
+  for (ent_graph* g : order) locks.emplace_back(g->mu);
+  for (size_t k = 0; k < m->graphs.size(); ++k) {
+    int rc = stage_request(m->graphs[k], m->ws[k], m->src[k].data(), m->n_src[k], m->depth[k], m->stream);
+    if (rc != ENT_OK) return rc;
+  }
+  ENT_CUDA(cudaEventRecord(m->ev0, m->stream));
+  ENT_CUDA(cudaGraphLaunch(m->exec, m->stream));
+  ENT_CUDA(cudaEventRecord(m->ev1, m->stream));
+  ENT_CUDA(cudaStreamSynchronize(m->stream));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, m->ev0, m->ev1);
+  if (device_ms) *device_ms = ms;
+  for (size_t k = 0; k < m->graphs.size(); ++k) {
+    BatchWorkspace* w = m->ws[k];
+    ENT_CUDA(cudaMemcpy(w->ctl_h, w->ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost));
+    g_kernel_launches += 3 + 4 * (int64_t)w->ctl_h->level;
+    if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "graph %zu: batched traversal error flags 0x%x", k, w->ctl_h->err);
+  }
+  return ENT_OK;
+}
+
+int ent_multi_depths(ent_multi* m, int32_t k, int32_t* depth_out) {
+  clear_error();
+  if (!m || !depth_out || k < 0 || k >= (int32_t)m->graphs.size()) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
+  DeviceGuard dg(m->device);
+  ENT_CUDA(cudaMemcpy(depth_out, m->depth[k], sizeof(int32_t) * (size_t)m->n_src[k] * m->graphs[k]->V,
+                      cudaMemcpyDeviceToHost));
+  return ENT_OK;
+}
+
+int ent_multi_destroy(ent_multi* m) {
+  multi_free(m);
+  return ENT_OK;
+}
+
+int ent_bfs_multi(ent_graph* const* graphs, int32_t n_graphs, const int32_t* src, const int32_t* n_src,
+                  int32_t* const* depth_out) {
+  ent_multi* m = nullptr;
+  int rc = ent_multi_create(graphs, n_graphs, src, n_src, &m);
+  if (rc != ENT_OK) return rc;
+  rc = ent_multi_run(m, nullptr);
+  for (int k = 0; rc == ENT_OK && k < n_graphs; ++k)
+    if (depth_out && depth_out[k]) rc = ent_multi_depths(m, k, depth_out[k]);
+  multi_free(m);
+  return rc;
+}
+
+}  // extern "C"

@@ -203,11 +203,27 @@ int ent_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* dept
 int ent_bfs_batch_device(ent_graph* g, const int32_t* src, int32_t n_src,
                          int32_t* depth_dev, void* stream, ent_stats* stats);
 
+/* Host-driven batched run with CUDA events per level (tracing aid). Entry
+ * n-1 with level == -1 times the final depth flush. */
+int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev,
+                        ent_level_trace* out, int32_t max_levels, int32_t* n_levels);
+
 /* Many graphs of uneven sizes in one launch: graphs[k] gets n_src[k] sources
  * from src (concatenated). depth_out[k] is a HOST array n_src[k] x V_k or
  * NULL. All graphs must live on the same GPU. */
 int ent_bfs_multi(ent_graph* const* graphs, int32_t n_graphs, const int32_t* src,
                   const int32_t* n_src, int32_t* const* depth_out);
+
+/* The same as a reusable plan: create once (allocates the plan's own
+ * traversal state and device outputs, builds one CUDA graph with one branch
+ * per graph), run many times (one graph launch; device_ms may be NULL),
+ * read each graph's n_src[k] x V_k depths, destroy. */
+typedef struct ent_multi ent_multi;
+int ent_multi_create(ent_graph* const* graphs, int32_t n_graphs, const int32_t* src,
+                     const int32_t* n_src, ent_multi** out);
+int ent_multi_run(ent_multi* plan, double* device_ms);
+int ent_multi_depths(ent_multi* plan, int32_t k, int32_t* depth_out);
+int ent_multi_destroy(ent_multi* plan);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,118 @@
+"""GPU parity tests of the bitwise multi-source traversal: every source's
+int32 depth row is bit-exact against a single-source CPU BFS (the oracle),
+and per-source statistics follow the reference's report() convention."""
+import numpy as np
+import pytest
+
+from conftest import hand_graphs, tier_graph
+
+pytestmark = pytest.mark.gpu
+
+
+def _check_rows(eb, orc, csr, depth, stats, srcs):
+    assert depth.shape == (len(srcs), csr.vert_count)
+    for i, s in enumerate(srcs):
+        exp, _ = orc.bfs(csr.beg_pos, csr.csr, int(s))
+        np.testing.assert_array_equal(depth[i], exp, err_msg=f"row {i} (source {s})")
+        e, v = orc.report(csr.beg_pos, exp)
+        assert (stats[i].traversed_edges, stats[i].reached_vertices) == (e, v), f"stats row {i}"
+        assert stats[i].levels == int(exp.max()) + 1
+
+
+def test_hand_graphs_every_vertex_as_source(eb, orc):
+    for name, V, edges in hand_graphs():
+        e = np.array(edges, dtype=np.int64)
+        csr = eb.Csr.from_edges(e[:, 0], e[:, 1], V)
+        with eb.Graph.from_csr(csr) as g:
+            srcs = list(range(V))
+            depth, stats = g.bfs_batch(srcs)
+            _check_rows(eb, orc, csr, depth, stats, srcs)
+
+
+@pytest.mark.parametrize("n", [1, 63, 64, 65, 128, 200, 256, 511, 1024])
+def test_widths_rmat(eb, orc, n):
+    """n sources -> 1..16 words per vertex (thread and lane-group bottom-up)."""
+    csr = eb.Csr.rmat(12, 16, seed=100 + n)
+    srcs = eb.pick_sources(csr.beg_pos, n, min(n, 1500))
+    with eb.Graph.from_csr(csr) as g:
+        depth, stats = g.bfs_batch(srcs)
+        check = srcs if n <= 128 else srcs[:: max(1, n // 96)]
+        idx = [list(srcs).index(s) for s in check]
+        for i in idx:
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, int(srcs[i]))
+            np.testing.assert_array_equal(depth[i], exp, err_msg=f"row {i}")
+            assert stats[i].reached_vertices == (exp >= 0).sum()
+
+
+def test_duplicate_and_isolated_sources(eb, orc):
+    csr = eb.Csr.from_edges([0, 1, 2, 3], [1, 2, 3, 4], 8)  # 5..7 isolated
+    with eb.Graph.from_csr(csr) as g:
+        srcs = [2, 2, 0, 7, 4, 2, 6]
+        depth, stats = g.bfs_batch(srcs)
+        _check_rows(eb, orc, csr, depth, stats, srcs)
+
+
+def test_tier_graph_deep_levels(eb, orc):
+    """~1000 levels: the level log wraps through many flush windows."""
+    V, s, d = tier_graph()
+    csr = eb.Csr.from_edges(s, d, V)
+    srcs = [0, 1, 3000, 3041, 4999, 5999, 5500, 2, 2]
+    with eb.Graph.from_csr(csr) as g:
+        depth, stats = g.bfs_batch(srcs)
+        _check_rows(eb, orc, csr, depth, stats, srcs)
+
+
+def test_grid_batch(eb, orc):
+    csr = eb.Csr.grid(48, 40, 0.1, seed=4)
+    srcs = eb.pick_sources(csr.beg_pos, 3, 100)
+    with eb.Graph.from_csr(csr) as g:
+        depth, stats = g.bfs_batch(srcs)
+        _check_rows(eb, orc, csr, depth, stats, srcs)
+
+
+def test_batch_matches_single_and_repeats(eb, orc):
+    csr = eb.Csr.rmat(14, 16, seed=77)
+    srcs = eb.pick_sources(csr.beg_pos, 9, 256)
+    with eb.Graph.from_csr(csr) as g:
+        d1, _ = g.bfs_batch(srcs)
+        d2, _ = g.bfs_batch(srcs[::-1])
+        np.testing.assert_array_equal(d1, d2[::-1])
+        for i in range(0, 256, 37):
+            np.testing.assert_array_equal(d1[i], g.bfs(int(srcs[i]))[0])
+
+
+def test_batch_device_output(eb, orc):
+    import torch
+    csr = eb.Csr.rmat(13, 8, seed=5)
+    srcs = eb.pick_sources(csr.beg_pos, 2, 70)
+    with eb.Graph.from_csr(csr) as g:
+        out = torch.empty((len(srcs), g.vert_count), dtype=torch.int32, device="cuda")
+        stats = g.bfs_batch_device(srcs, out.data_ptr())
+        host = out.cpu().numpy()
+        for i in range(0, len(srcs), 7):
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, int(srcs[i]))
+            np.testing.assert_array_equal(host[i], exp)
+        assert len(stats) == len(srcs)
+
+
+def test_multi_graph_one_launch(eb, orc):
+    """Graphs of uneven sizes and widths, each with its own sources, in one launch."""
+    specs = [(9, 8, 3), (11, 16, 70), (12, 32, 130), (10, 8, 1), (13, 16, 64)]
+    csrs = [eb.Csr.rmat(s, ef, seed=500 + i) for i, (s, ef, _) in enumerate(specs)]
+    graphs = [eb.Graph.from_csr(c) for c in csrs]
+    srcs = [eb.pick_sources(c.beg_pos, 600 + i, n) for i, (c, (_, _, n)) in enumerate(zip(csrs, specs))]
+    outs = eb.bfs_multi(graphs, srcs)
+    for c, s, d in zip(csrs, srcs, outs):
+        for i in range(0, len(s), max(1, len(s) // 8)):
+            exp, _ = orc.bfs(c.beg_pos, c.csr, int(s[i]))
+            np.testing.assert_array_equal(d[i], exp)
+    plan = eb.MultiPlan(graphs, srcs)
+    for _ in range(2):
+        plan.run()
+        for k, (c, s) in enumerate(zip(csrs, srcs)):
+            d = plan.depths(k)
+            exp, _ = orc.bfs(c.beg_pos, c.csr, int(s[-1]))
+            np.testing.assert_array_equal(d[-1], exp)
+    plan.close()
+    for g in graphs:
+        g.close()
