@@ -34,6 +34,7 @@ SOURCES = [
     "device_graph.cu",
     "bfs_single.cu",
     "bfs_batch.cu",
+    "bfs_noalloc.cu",
     "serve.cpp",
     "tune.cpp",
 ]

@@ -193,6 +193,24 @@ typedef struct ent_level_trace {
 int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_levels, int32_t* n_levels,
                   ent_stats* stats);
 
+/* BFS that allocates nothing. No counterpart in the reference: it exists for
+ * callers that may not allocate GPU memory when they traverse — code on a
+ * latency-critical path, where cudaMalloc/cudaFree can synchronise the device
+ * and stall other streams, and plug-ins in processes whose GPU memory is
+ * owned by another allocator or a fixed budget. The caller passes the CSR
+ * (beg_pos: V+1 int64, csr: int32, valid ids, e.g. from ent_graph_device_csr)
+ * and depth_dev (V int32) in device memory of the current device; the
+ * traversal's scratch is a static array inside this library on every GPU that
+ * loads it (about 8.5 MB) and limits V to ENT_NOALLOC_MAX_VERTICES; larger
+ * graphs return ENT_ERR_INVALID_ARG. The first call on a device looks up the
+ * array's device address, so make that first call before any stream capture.
+ * All calls share the array: calls whose work overlaps on one GPU race and
+ * give wrong results, so serialise them. Synchronous on `stream` (NULL = the
+ * default stream). */
+#define ENT_NOALLOC_MAX_VERTICES (1 << 20)
+int ent_bfs_noalloc(const int64_t* beg_pos_dev, const int32_t* csr_dev, int64_t vert_count,
+                    int32_t src, int32_t* depth_dev, void* stream);
+
 /* Many sources at once with bitwise frontiers (one bit per source per vertex
  * in a shared status word). depth_out: HOST array n_src x V int32, source-major
  * (row s is the depth array of src[s]); may be NULL. stats: n_src entries or
