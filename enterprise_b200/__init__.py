@@ -68,6 +68,23 @@ class _Trace(C.Structure):
     ]
 
 
+class _ServerOpts(C.Structure):
+    _fields_ = [("max_batch", C.c_int32), ("slots_per_graph", C.c_int32), ("rows_per_graph", C.c_int32),
+                ("max_pending", C.c_int32), ("hbm_budget_bytes", C.c_int64)]
+
+
+class _QueryResult(C.Structure):
+    _fields_ = [("query_id", C.c_int64), ("graph", C.c_int32), ("src", C.c_int32),
+                ("reached_vertices", C.c_int64), ("traversed_edges", C.c_int64), ("levels", C.c_int32),
+                ("status", C.c_int32), ("latency_ms", C.c_double), ("queue_ms", C.c_double)]
+
+
+class _ServerCounters(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("submitted", "rejected", "completed", "released", "batches", "launched",
+                                         "pending", "rows_total", "rows_free")] + \
+               [("max_batch_seen", C.c_int32), ("pad", C.c_int32)]
+
+
 @dataclass
 class BfsOpts:
     """Tuning knobs of one graph's traversals (mirror of ``ent_bfs_opts``)."""
@@ -172,6 +189,15 @@ def lib() -> C.CDLL:
         "ent_multi_run": (C.c_int, [_P, C.POINTER(C.c_double)]),
         "ent_multi_depths": (C.c_int, [_P, C.c_int32, _I32P]),
         "ent_multi_destroy": (C.c_int, [_P]),
+        "ent_server_opts_default": (None, [C.POINTER(_ServerOpts)]),
+        "ent_server_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_ServerOpts), C.POINTER(_P)]),
+        "ent_server_submit": (C.c_int, [_P, C.c_int32, C.c_int32, _I64P]),
+        "ent_server_poll": (C.c_int, [_P, C.POINTER(_QueryResult), C.c_int32, _I32P, C.c_int32]),
+        "ent_server_depth": (C.c_int, [_P, C.c_int64, _I32P]),
+        "ent_server_depth_device": (C.c_int, [_P, C.c_int64, C.POINTER(_P)]),
+        "ent_server_release": (C.c_int, [_P, C.c_int64]),
+        "ent_server_get_counters": (C.c_int, [_P, C.POINTER(_ServerCounters)]),
+        "ent_server_destroy": (C.c_int, [_P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -495,3 +521,66 @@ def bfs_multi(graphs: Sequence[Graph], sources: Sequence[Sequence[int]]) -> list
     ptrs = (_I32P * n)(*[_i32p(o) for o in outs])
     _check(lib().ent_bfs_multi(hs, n, _i32p(flat), _i32p(counts), ptrs))
     return outs
+
+
+class Server:
+    """Continuous-batching BFS query server over device-resident graphs
+    (mirror of ``ent_server``)."""
+
+    def __init__(self, graphs: Sequence[Graph], max_batch: int = 64, slots_per_graph: int = 2,
+                 rows_per_graph: int = 0, max_pending: int = 1 << 20, hbm_budget_bytes: int = 0):
+        self.graphs = list(graphs)
+        o = _ServerOpts(max_batch, slots_per_graph, rows_per_graph, max_pending, hbm_budget_bytes)
+        hs = (_P * len(graphs))(*[g.handle for g in graphs])
+        h = _P()
+        _check(lib().ent_server_create(hs, len(graphs), C.byref(o), C.byref(h)))
+        self._h = h
+        self._buf = (_QueryResult * 4096)()
+        self._graph_of: dict[int, int] = {}
+
+    def submit(self, graph: int, src: int) -> int:
+        q = C.c_int64()
+        _check(lib().ent_server_submit(self._h, graph, int(src), C.byref(q)))
+        self._graph_of[q.value] = graph
+        return q.value
+
+    def poll(self, wait_us: int = 0, max_results: int = 4096) -> list[dict]:
+        n = C.c_int32()
+        _check(lib().ent_server_poll(self._h, self._buf, min(max_results, 4096), C.byref(n), wait_us))
+        return [{f[0]: getattr(self._buf[i], f[0]) for f in _QueryResult._fields_} for i in range(n.value)]
+
+    def depth(self, query_id: int) -> np.ndarray:
+        out = np.empty(self.graphs[self._graph_of[query_id]].vert_count, dtype=np.int32)
+        _check(lib().ent_server_depth(self._h, query_id, _i32p(out)))
+        return out
+
+    def depth_device(self, query_id: int) -> int:
+        p = _P()
+        _check(lib().ent_server_depth_device(self._h, query_id, C.byref(p)))
+        return int(p.value or 0)
+
+    def release(self, query_id: int) -> None:
+        _check(lib().ent_server_release(self._h, query_id))
+        self._graph_of.pop(query_id, None)
+
+    def counters(self) -> dict:
+        c = _ServerCounters()
+        _check(lib().ent_server_get_counters(self._h, C.byref(c)))
+        return {f[0]: getattr(c, f[0]) for f in _ServerCounters._fields_ if f[0] != "pad"}
+
+    def close(self) -> None:
+        if self._h is not None:
+            lib().ent_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -38,7 +38,7 @@ SOURCES = [
     "serve.cpp",
     "tune.cpp",
 ]
-HEADERS = ["gen_common.h", "ent_internal.h", "dev_graph.h", "dev_common.cuh"]
+HEADERS = ["gen_common.h", "ent_internal.h", "dev_graph.h", "dev_common.cuh", "batch_internal.h"]
 
 
 def nvcc() -> str:

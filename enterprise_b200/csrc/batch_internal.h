@@ -1,0 +1,18 @@
+// Internal interface of the batched traversal used by the serving loop.
+#pragma once
+#include <cuda_runtime.h>
+#include "dev_graph.h"
+
+namespace ent {
+// Traversal state for one batched run of up to words_for(n_src)*64 sources.
+int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out);
+// Adds one independent branch (memsets, seed, while{expand, commit, flush,
+// recycle}, final flush) for workspace w to `graph`.
+int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream_t cap_stream);
+// Uploads sources and output location for the next launch of w's branch.
+// With row_map_dev (device, n_src entries) source s writes depth row row_map[s].
+int stage_request(ent_graph* g, BatchWorkspace* w, const int32_t* src, int32_t n_src, int32_t* depth_dev,
+                  cudaStream_t s, const int32_t* row_map_dev);
+int batch_source_stats(BatchWorkspace* w, int32_t n_src, cudaStream_t s, ent_stats* stats);
+int batch_max_sources(const BatchWorkspace* w);
+}  // namespace ent

@@ -53,6 +53,7 @@ struct BatchCtl {
   int32_t n_src;
   int32_t pad;
   int32_t* depth;    // [n_src][V] output of this run
+  const int32_t* row_map;  // optional: source s writes row row_map[s] of depth
   unsigned long long acc_m, acc_mdone;
   int64_t m_f, m_done;
   uint32_t finished;
@@ -599,8 +600,8 @@ __device__ __forceinline__ void load_cols(const unsigned long long* p, unsigned 
 
 template <int CG>
 __device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, int last, int base, int windows,
-                           int nsrc, int32_t* depth, bool vec_ok, unsigned char* tile, const int* s_deg,
-                           unsigned* s_cnt, int* s_maxd, unsigned long long* s_edg) {
+                           int nsrc, int32_t* depth, const int32_t* row_map, bool vec_ok, unsigned char* tile,
+                           const int* s_deg, unsigned* s_cnt, int* s_maxd, unsigned long long* s_edg) {
   constexpr int VS = TILE_BYTES / (64 * CG);  // vertices per pass
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int64_t sub = 0; sub < nv; sub += VS) {
@@ -634,7 +635,7 @@ __device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, in
         const int s = cg * 64 + r;
         if (s >= nsrc) break;
         const uint32_t* row = reinterpret_cast<const uint32_t*>(tile + r * VS);
-        int32_t* out = depth + (size_t)s * a.V + v0 + sub;
+        int32_t* out = depth + (size_t)(row_map ? row_map[s] : s) * a.V + v0 + sub;
         const int* dg = s_deg + sub;
         unsigned cnt = 0;
         unsigned long long edg = 0;
@@ -705,9 +706,10 @@ __global__ void __launch_bounds__(BB) k_b_flush(BatchArgs a, int final_flush) {
     __syncthreads();
     for (int i = threadIdx.x; i < 1024; i += BB) s_deg[i] = i < nv ? a.deg[v0 + i] : 0;
     __syncthreads();
-    if (a.W == 1) flush_span<1>(a, v0, nv, first, last, base, windows, nsrc, depth, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
-    else if (a.W == 2) flush_span<2>(a, v0, nv, first, last, base, windows, nsrc, depth, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
-    else flush_span<4>(a, v0, nv, first, last, base, windows, nsrc, depth, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
+    const int32_t* row_map = c->row_map;
+    if (a.W == 1) flush_span<1>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
+    else if (a.W == 2) flush_span<2>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
+    else flush_span<4>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
   }
   __syncthreads();
   for (int s = threadIdx.x; s < nsrc; s += BB) {
@@ -823,7 +825,7 @@ constexpr int MAX_BATCH = WMAX * 64;
 
 // Appends this graph's whole batched traversal to `graph` as an independent
 // branch: memsets -> seed -> while { expand, commit, flush } -> final flush.
-static int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream_t cap_stream) {
+int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream_t cap_stream) {
   cudaGraphNode_t prev = nullptr;
   auto add_memset = [&](void* p, size_t bytes) -> int {
     cudaMemsetParams mp = {};
@@ -896,7 +898,7 @@ static int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cud
   return ENT_OK;
 }
 
-static int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
+int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
   BatchWorkspace* w = new BatchWorkspace();
   const int64_t V = g->V;
   const int W = words_for(n_src);
@@ -1013,8 +1015,8 @@ static int ensure_batch(ent_graph* g, int n_src) {
 
 // Uploads sources, mask and the output pointer (the kernels read them from
 // device memory, so one instantiated graph serves every batch).
-static int stage_request(ent_graph*, BatchWorkspace* w, const int32_t* src, int32_t n_src, int32_t* depth_dev,
-                         cudaStream_t s) {
+int stage_request(ent_graph*, BatchWorkspace* w, const int32_t* src, int32_t n_src, int32_t* depth_dev,
+                  cudaStream_t s, const int32_t* row_map_dev) {
   std::vector<unsigned long long> mask(w->W, 0);
   for (int i = 0; i < n_src; ++i) mask[i >> 6] |= 1ull << (i & 63);
   ENT_CUDA(cudaMemcpyAsync((void*)w->args.mask, mask.data(), sizeof(unsigned long long) * w->W, cudaMemcpyHostToDevice, s));
@@ -1022,6 +1024,7 @@ static int stage_request(ent_graph*, BatchWorkspace* w, const int32_t* src, int3
   BatchCtl init = {};
   init.n_src = n_src;
   init.depth = depth_dev;
+  init.row_map = row_map_dev;
   ENT_CUDA(cudaMemcpyAsync(w->ctl, &init, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
   return ENT_OK;
 }
@@ -1048,6 +1051,29 @@ static int read_batch_stats(ent_graph* g, BatchWorkspace* w, int32_t n_src, cuda
   return ENT_OK;
 }
 
+// Per-source statistics of a finished run of workspace w (the caller has
+// waited for the run; copies on stream s and synchronises it).
+int batch_source_stats(BatchWorkspace* w, int32_t n_src, cudaStream_t s, ent_stats* stats) {
+  ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+  ENT_CUDA(cudaMemcpyAsync(w->h_edges.data(), w->args.st_edges, sizeof(unsigned long long) * n_src, cudaMemcpyDeviceToHost, s));
+  ENT_CUDA(cudaMemcpyAsync(w->h_verts.data(), w->args.st_verts, sizeof(unsigned long long) * n_src, cudaMemcpyDeviceToHost, s));
+  ENT_CUDA(cudaMemcpyAsync(w->h_maxd.data(), w->args.st_maxd, sizeof(int32_t) * n_src, cudaMemcpyDeviceToHost, s));
+  ENT_CUDA(cudaStreamSynchronize(s));
+  for (int i = 0; i < n_src; ++i) {
+    stats[i].reached_vertices = (int64_t)w->h_verts[i];
+    stats[i].traversed_edges = (int64_t)w->h_edges[i];
+    stats[i].levels = w->h_maxd[i] + 1;
+    stats[i].td_levels = w->ctl_h->td_levels;
+    stats[i].bu_levels = w->ctl_h->bu_levels;
+    stats[i].status = w->ctl_h->err;
+    stats[i].device_ms = 0;
+  }
+  g_kernel_launches += 3 + 4 * (int64_t)w->ctl_h->level;
+  return w->ctl_h->err ? fail(ENT_ERR_TIMEOUT, "batched traversal error flags 0x%x", w->ctl_h->err) : ENT_OK;
+}
+
+int batch_max_sources(const BatchWorkspace* w) { return w->cap_src; }
+
 int run_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, cudaStream_t stream,
                   ent_stats* stats) {
   for (int i = 0; i < n_src; ++i)
@@ -1056,7 +1082,7 @@ int run_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* dept
   if (rc != ENT_OK) return rc;
   BatchWorkspace* w = g->bws;
   cudaStream_t s = stream ? stream : g->stream;
-  rc = stage_request(g, w, src, n_src, depth_dev, s);
+  rc = stage_request(g, w, src, n_src, depth_dev, s, nullptr);
   if (rc != ENT_OK) return rc;
   ENT_CUDA(cudaEventRecord(w->ev0, s));
   ENT_CUDA(cudaGraphLaunch(w->exec, s));
@@ -1123,7 +1149,7 @@ int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t
   if (rc != ENT_OK) return rc;
   BatchWorkspace* w = g->bws;
   cudaStream_t s = g->stream;
-  rc = stage_request(g, w, src, n_src, depth_dev, s);
+  rc = stage_request(g, w, src, n_src, depth_dev, s, nullptr);
   if (rc != ENT_OK) return rc;
   ENT_CUDA(cudaMemsetAsync(w->x_ptr, 0, w->x_bytes, s));
   ENT_CUDA(cudaMemsetAsync(w->small_ptr, 0, w->small_bytes, s));
@@ -1279,7 +1305,7 @@ int ent_multi_run(ent_multi* m, double* device_ms) {
   std::vector<std::unique_lock<std::mutex>> locks;
   for (ent_graph* g : order) locks.emplace_back(g->mu);
   for (size_t k = 0; k < m->graphs.size(); ++k) {
-    int rc = stage_request(m->graphs[k], m->ws[k], m->src[k].data(), m->n_src[k], m->depth[k], m->stream);
+    int rc = stage_request(m->graphs[k], m->ws[k], m->src[k].data(), m->n_src[k], m->depth[k], m->stream, nullptr);
     if (rc != ENT_OK) return rc;
   }
   ENT_CUDA(cudaEventRecord(m->ev0, m->stream));

@@ -243,6 +243,54 @@ int ent_multi_run(ent_multi* plan, double* device_ms);
 int ent_multi_depths(ent_multi* plan, int32_t k, int32_t* depth_out);
 int ent_multi_destroy(ent_multi* plan);
 
+/* ------------------------------------------------------- serving -------- */
+/* A request loop over device-resident graphs with continuous batching. No
+ * reference counterpart (the reference runs a fixed 64-source list per
+ * process). Each graph has slots_per_graph concurrent batched launches; a
+ * scheduler thread forms each batch from the queries waiting at the moment a
+ * slot frees up (at most max_batch, and only queries that get a depth row).
+ * Per-query state is one depth row (V int32) in a per-graph HBM pool sized by
+ * rows_per_graph or, when 0, by hbm_budget_bytes (0 = a quarter of free HBM):
+ * a query holds its row from launch until ent_server_release, so unreleased
+ * results throttle admission. submit fails with ENT_ERR_ADMISSION once
+ * max_pending queries wait. Results are the same depths as ent_bfs. */
+typedef struct ent_server ent_server;
+typedef struct ent_server_opts {
+  int32_t max_batch;        /* sources per batched launch, 1..2048 (default 64) */
+  int32_t slots_per_graph;  /* concurrent batches per graph, 1..16 (default 2)  */
+  int32_t rows_per_graph;   /* depth rows per graph, 0 = from the budget         */
+  int32_t max_pending;      /* waiting queries before submit refuses             */
+  int64_t hbm_budget_bytes; /* depth-row budget across graphs, 0 = free HBM / 4  */
+} ent_server_opts;
+typedef struct ent_query_result {
+  int64_t query_id;
+  int32_t graph;
+  int32_t src;
+  int64_t reached_vertices;
+  int64_t traversed_edges;
+  int32_t levels;
+  int32_t status;           /* 0 ok, else an ent_status */
+  double latency_ms;        /* submit -> result on the device */
+  double queue_ms;          /* submit -> launch */
+} ent_query_result;
+typedef struct ent_server_counters {
+  int64_t submitted, rejected, completed, released, batches, launched, pending, rows_total, rows_free;
+  int32_t max_batch_seen;
+  int32_t pad;
+} ent_server_counters;
+void ent_server_opts_default(ent_server_opts* opts);
+int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_server_opts* opts,
+                      ent_server** out);
+int ent_server_submit(ent_server* s, int32_t graph, int32_t src, int64_t* query_id);
+/* Completed queries (up to max_results); waits up to wait_us if none is ready. */
+int ent_server_poll(ent_server* s, ent_query_result* out, int32_t max_results, int32_t* n_out,
+                    int32_t wait_us);
+int ent_server_depth(ent_server* s, int64_t query_id, int32_t* depth_out);
+int ent_server_depth_device(ent_server* s, int64_t query_id, const int32_t** depth_dev);
+int ent_server_release(ent_server* s, int64_t query_id);
+int ent_server_get_counters(ent_server* s, ent_server_counters* out);
+int ent_server_destroy(ent_server* s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,124 @@
+"""GPU tests of the serving loop: every query's depths are identical to the
+same BFS run alone (ent_bfs), whatever else shares its batch, its slot or the
+device; admission by memory throttles and resumes; the queue refuses when full."""
+import threading
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _drain(srv, want, timeout_polls=20000):
+    done = []
+    polls = 0
+    while len(done) < want and polls < timeout_polls:
+        done += srv.poll(wait_us=2000)
+        polls += 1
+    assert len(done) == want, f"only {len(done)} of {want} queries completed"
+    return done
+
+
+def test_results_same_alone_and_in_the_mix(eb, orc):
+    csrs = [eb.Csr.rmat(12, 16, seed=61), eb.Csr.grid(60, 50, 0.1, seed=62), eb.Csr.er(5000, 12, seed=63),
+            eb.Csr.rmat(10, 8, seed=64)]
+    graphs = [eb.Graph.from_csr(c) for c in csrs]
+    rng = np.random.default_rng(7)
+    alone = {}
+    with eb.Server(graphs, max_batch=16, slots_per_graph=2) as srv:
+        qs = {}
+        for _ in range(300):
+            gi = int(rng.integers(len(graphs)))
+            src = int(eb.pick_sources(csrs[gi].beg_pos, int(rng.integers(1 << 30)), 1)[0])
+            qs[srv.submit(gi, src)] = (gi, src)
+        res = _drain(srv, len(qs))
+        assert srv.counters()["batches"] >= 2
+        for r in res:
+            gi, src = qs[r["query_id"]]
+            assert (r["graph"], r["src"], r["status"]) == (gi, src, 0)
+            got = srv.depth(r["query_id"])
+            key = (gi, src)
+            if key not in alone:
+                alone[key] = graphs[gi].bfs(src)[0]
+            np.testing.assert_array_equal(got, alone[key])
+            e, v = orc.report(csrs[gi].beg_pos, got)
+            assert (r["traversed_edges"], r["reached_vertices"]) == (e, v)
+            assert r["latency_ms"] >= r["queue_ms"] >= 0
+            srv.release(r["query_id"])
+        c = srv.counters()
+        assert c["completed"] == c["released"] == 300 and c["rows_free"] == c["rows_total"]
+    for g in graphs:
+        g.close()
+
+
+def test_admission_by_memory_throttles_and_resumes(eb):
+    """5 depth rows: 5 queries run, the rest wait until results are released."""
+    csr = eb.Csr.rmat(11, 8, seed=71)
+    g = eb.Graph.from_csr(csr)
+    srcs = eb.pick_sources(csr.beg_pos, 3, 40)
+    with eb.Server([g], max_batch=8, slots_per_graph=2, rows_per_graph=5) as srv:
+        ids = [srv.submit(0, int(s)) for s in srcs]
+        done = []
+        for _ in range(500):
+            done += srv.poll(wait_us=2000)
+            if len(done) >= 5:
+                break
+        done += srv.poll(wait_us=50000)  # nothing else can run: every row is held
+        assert len(done) == 5
+        c = srv.counters()
+        assert c["rows_free"] == 0 and c["pending"] == len(ids) - 5
+        released = 0
+        for _ in range(5000):
+            while released < len(done):
+                srv.release(done[released]["query_id"])
+                released += 1
+            if released == len(ids):
+                break
+            done += srv.poll(wait_us=2000)
+        assert released == len(ids)
+        assert srv.counters()["completed"] == len(ids)
+    g.close()
+
+
+def test_queue_limit_refuses(eb):
+    csr = eb.Csr.rmat(10, 8, seed=81)
+    g = eb.Graph.from_csr(csr)
+    with eb.Server([g], max_batch=4, slots_per_graph=1, rows_per_graph=1, max_pending=3) as srv:
+        src = int(eb.pick_sources(csr.beg_pos, 1, 1)[0])
+        accepted, refused = 0, 0
+        for _ in range(20):
+            try:
+                srv.submit(0, src)
+                accepted += 1
+            except eb.EntError as e:
+                assert e.code == 9
+                refused += 1
+        assert refused > 0 and accepted >= 3
+        assert srv.counters()["rejected"] == refused
+    g.close()
+
+
+def test_submissions_from_threads(eb):
+    csr = eb.Csr.rmat(12, 8, seed=91)
+    g = eb.Graph.from_csr(csr)
+    srcs = eb.pick_sources(csr.beg_pos, 5, 64)
+    ref = {int(s): g.bfs(int(s))[0] for s in srcs}
+    with eb.Server([g], max_batch=32, slots_per_graph=3) as srv:
+        ids = {}
+        lock = threading.Lock()
+
+        def worker(part):
+            for s in part:
+                q = srv.submit(0, int(s))
+                with lock:
+                    ids[q] = int(s)
+
+        ts = [threading.Thread(target=worker, args=(srcs[i::4],)) for i in range(4)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        for r in _drain(srv, len(srcs)):
+            np.testing.assert_array_equal(srv.depth(r["query_id"]), ref[ids[r["query_id"]]])
+            srv.release(r["query_id"])
+    g.close()
