@@ -142,6 +142,13 @@ def run_ours(args, rank, world, dist):
     else:
         beg = g.download().beg_pos
     srcs = eb.pick_sources(beg, source_seed(args.scale, rank), args.sources)
+    tuned = None
+    if not args.no_tune:
+        from enterprise_b200 import tune
+        t0 = time.time()
+        opts, ms, hit = tune.autotune(g, srcs[:8], "single", reps=1, label="rmat", device=local)
+        tuned = {"opts": {k: v for k, v in vars(opts).items() if k != "pad"}, "cached": hit,
+                 "search_s": round(time.time() - t0, 2)}
 
     stream = torch.cuda.Stream(device=local)
     sptr = stream.cuda_stream
@@ -230,7 +237,7 @@ def run_ours(args, rank, world, dist):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(beg, csr_h, srcs, args, g, depth)
 
-    launches = int(args.steps * np.sum(1 + 2 * levels)) * world
+    launches = int(args.steps * np.sum(2 + 2 * levels)) * world
     line = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -275,7 +282,172 @@ def run_ours(args, rank, world, dist):
     }
     if cpu:
         line["cpu_baseline"] = cpu
+    if tuned:
+        line["config"]["autotuned"] = tuned
+    if world == 1 and not args.no_extras:
+        g.close()
+        del depth, flush
+        torch.cuda.empty_cache()
+        line["batched"] = run_batched(args)
+        line["serving"] = run_serving(args)
     return line
+
+
+def run_batched(args):
+    """Bitwise multi-source BFS on R-MAT s22 ef16: batches of 64/256/1024
+    sources against 256 sequential single-source runs of the same sources,
+    plus 48 R-MAT graphs of scales 12-20, edge factors 8-32, in one launch."""
+    import torch
+    import enterprise_b200 as eb
+    scale = args.batch_scale
+    g = eb.Graph.rmat(scale, 16, seed=graph_seed(scale), **RMAT)
+    beg = g.download().beg_pos
+    srcs = eb.pick_sources(beg, source_seed(scale), 1024)
+    V = g.vert_count
+    d1 = torch.empty(V, dtype=torch.int32, device="cuda")
+    st = [g.bfs_device(int(s), d1.data_ptr()) for s in srcs[:256]]
+    m = np.array([x.traversed_edges for x in st], dtype=np.float64)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    strm = torch.cuda.Stream()
+    seq = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        s0.record(strm)
+        for s in srcs[:256]:
+            g.bfs_device(int(s), d1.data_ptr(), 0, strm.cuda_stream, stats=False)
+        s1.record(strm)
+        torch.cuda.synchronize()
+        seq.append(s0.elapsed_time(s1))
+    seq_ms = min(seq)
+    out = {"graph": f"rmat s{scale} ef16", "vertices": V, "directed_entries": g.edge_count,
+           "sequential_256": {"ms": round(seq_ms, 3), "gteps": round(m.sum() / seq_ms / 1e6, 2),
+                              "kind": "256 direction-optimizing single-source runs, back to back"}}
+    tuned = None
+    if not args.no_tune:
+        from enterprise_b200 import tune
+        opts, _, hit = tune.autotune(g, srcs[:256], "batch", reps=1, label="rmat")
+        tuned = {"batch_alpha": opts.batch_alpha, "batch_small_max": opts.batch_small_max,
+                 "batch_large_min": opts.batch_large_min, "batch_heavy": opts.batch_heavy, "cached": hit}
+        out["autotuned"] = tuned
+    for n in (64, 256, 1024):
+        dd = torch.empty((n, V), dtype=torch.int32, device="cuda")
+        times, edges = [], 0
+        for rep in range(4):
+            stb = g.bfs_batch_device(srcs[:n], dd.data_ptr())
+            if rep:
+                times.append(stb[0].device_ms)
+            edges = sum(x.traversed_edges for x in stb)
+        ms = min(times)
+        ok = all(np.array_equal(dd[i].cpu().numpy(), g.bfs(int(srcs[i]))[0]) for i in (0, n // 2, n - 1))
+        out[f"batch_{n}"] = {"ms": round(ms, 3), "gteps": round(edges / ms / 1e6, 2), "rows_checked_exact": ok,
+                            "levels": stb[0].td_levels + stb[0].bu_levels}
+        del dd
+        torch.cuda.empty_cache()
+    out["batch_256_vs_sequential_256"] = round(out["sequential_256"]["ms"] / out["batch_256"]["ms"], 3)
+    g.close()
+    # 48 graphs of uneven sizes, 64 sources each, one launch
+    rng = np.random.default_rng(0x48)
+    graphs, sources, total_v = [], [], 0
+    for k in range(48):
+        sc = int(rng.integers(12, 21))
+        ef = int(rng.choice([8, 16, 32]))
+        gk = eb.Graph.rmat(sc, ef, seed=0xC4000 + k, **RMAT)
+        bk = gk.download().beg_pos
+        graphs.append(gk)
+        sources.append(eb.pick_sources(bk, 0xC4100 + k, 64))
+        total_v += gk.vert_count
+    plan = eb.MultiPlan(graphs, sources)
+    mts = [plan.run() for _ in range(4)][1:]
+    ms = min(mts)
+    edges = 0
+    for gk, sk in zip(graphs, sources):
+        # per-source edges (report() convention) from a separate batched run
+        dd = torch.empty((len(sk), gk.vert_count), dtype=torch.int32, device="cuda")
+        edges += sum(x.traversed_edges for x in gk.bfs_batch_device(sk, dd.data_ptr()))
+        del dd
+    d_last = plan.depths(47)
+    ok = np.array_equal(d_last[0], graphs[47].bfs(int(sources[47][0]))[0])
+    out["multi_graph_48"] = {"ms": round(ms, 3), "graphs": 48, "sources_per_graph": 64, "vertices_total": total_v,
+                             "gteps": round(edges / ms / 1e6, 2), "row_checked_exact": ok,
+                             "launches": "one CUDA graph launch, one branch per graph"}
+    plan.close()
+    for gk in graphs:
+        gk.close()
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_serving(args):
+    """Poisson stream of BFS queries against 16 device-resident graphs (12
+    R-MAT s14-22 ef16, 4 grids 1024^2..2048^2 with 10% of edges dropped):
+    continuous batching, admission by HBM depth rows, latency percentiles."""
+    import torch
+    import enterprise_b200 as eb
+    rmat_scales = [14, 15, 16, 17, 18, 18, 19, 19, 20, 20, 21, 22]
+    graphs, begs = [], []
+    for k, sc in enumerate(rmat_scales):
+        graphs.append(eb.Graph.rmat(sc, 16, seed=0xC5000 + k, **RMAT))
+    for k, w in enumerate([1024, 1448, 1774, 2048]):
+        graphs.append(eb.Graph.grid(w, w, 0.1, seed=0xC5100 + k))
+    for gk in graphs:
+        begs.append(gk.download().beg_pos)
+    pools = [eb.pick_sources(b, 0xC5200 + k, 512) for k, b in enumerate(begs)]
+    rng = np.random.default_rng(0xC5)
+    duration, rate = args.serve_seconds, args.serve_rate
+    n_q = int(rng.poisson(rate * duration))
+    arrivals = np.sort(rng.uniform(0, duration, n_q))
+    which = rng.integers(0, len(graphs), n_q)
+    pick = rng.integers(0, 512, n_q)
+    lat, qwait, edges, done = [], [], 0, 0
+    sample_every = max(1, n_q // 40)
+    checks, bad_status, mismatches = 0, 0, []
+    graph_of = {}
+    with eb.Server(graphs, max_batch=args.serve_batch, slots_per_graph=args.serve_slots) as srv:
+        t0 = time.perf_counter()
+        i = 0
+        while done < n_q:
+            now = time.perf_counter() - t0
+            while i < n_q and arrivals[i] <= now:
+                q = srv.submit(int(which[i]), int(pools[which[i]][pick[i]]))
+                graph_of[q] = (int(which[i]), int(pools[which[i]][pick[i]]), i % sample_every == 0)
+                i += 1
+            for r in srv.poll(wait_us=200):
+                done += 1
+                lat.append(r["latency_ms"])
+                qwait.append(r["queue_ms"])
+                edges += r["traversed_edges"]
+                gi, src, sample = graph_of.pop(r["query_id"])
+                if r["status"] != 0:
+                    bad_status += 1
+                if sample and r["status"] == 0:
+                    d = srv.depth(r["query_id"])
+                    ref = graphs[gi].bfs(src)[0]
+                    if not np.array_equal(d, ref):
+                        diff = np.flatnonzero(d != ref)
+                        mismatches.append({"graph": gi, "src": src, "n_diff": int(len(diff)), "at": int(diff[0]),
+                                           "got": int(d[diff[0]]), "want": int(ref[diff[0]])})
+                    checks += 1
+                srv.release(r["query_id"])
+            if time.perf_counter() - t0 > duration * 3 + 60:
+                break
+        wall = time.perf_counter() - t0
+        c = srv.counters()
+    for gk in graphs:
+        gk.close()
+    torch.cuda.empty_cache()
+    lat = np.array(lat)
+    return {"graphs": "12 R-MAT s14-22 ef16 + 4 grids 1024^2,1448^2,1774^2,2048^2 (10% edges dropped)",
+            "arrival": f"Poisson {rate}/s for {duration} s ({n_q} queries, seeded)",
+            "completed": int(done), "wall_s": round(wall, 2), "throughput_qps": round(done / wall, 1),
+            "gteps": round(edges / wall / 1e9, 2),
+            "p50_ms": round(float(np.percentile(lat, 50)), 3) if len(lat) else None,
+            "p99_ms": round(float(np.percentile(lat, 99)), 3) if len(lat) else None,
+            "p999_ms": round(float(np.percentile(lat, 99.9)), 3) if len(lat) else None,
+            "queue_p50_ms": round(float(np.percentile(qwait, 50)), 3) if len(qwait) else None,
+            "batches": c["batches"], "mean_batch": round(c["launched"] / max(1, c["batches"]), 2),
+            "max_batch_seen": c["max_batch_seen"], "samples_checked": checks,
+            "sampled_exact": not mismatches and bad_status == 0, "bad_status": bad_status,
+            "mismatches": mismatches[:5], "max_batch": args.serve_batch, "slots_per_graph": args.serve_slots}
 
 
 def cpu_baseline(beg, csr, srcs, args, g, depth):
@@ -373,6 +545,15 @@ def main():
     ap.add_argument("--sources", type=int, default=64)
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner")
+    ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
+    ap.add_argument("--batch-scale", type=int, default=22)
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="serving run length (config: 60)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-batch", type=int, default=64)
+    ap.add_argument("--serve-slots", type=int, default=1)
+    ap.add_argument("--only", choices=["batch", "serve"], default=None,
+                    help="run only one of the extra measurements and print it")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -388,7 +569,9 @@ def main():
                                  timeout=datetime.timedelta(seconds=600))
         dist = tdist
     try:
-        if args.impl == "reference":
+        if args.only:
+            line = run_batched(args) if args.only == "batch" else run_serving(args)
+        elif args.impl == "reference":
             line = run_reference(args, rank, world)
         else:
             line = run_ours(args, rank, world, dist)

@@ -49,6 +49,8 @@ class _Opts(C.Structure):
         ("policy", C.c_int32), ("loop", C.c_int32), ("alpha", C.c_double), ("beta", C.c_double),
         ("ref_ratio", C.c_double), ("small_max", C.c_int32), ("large_min", C.c_int32),
         ("hub_slots", C.c_int32), ("chunk_edges", C.c_int32), ("blocks_per_sm", C.c_int32),
+        ("batch_alpha", C.c_double), ("batch_small_max", C.c_int32), ("batch_large_min", C.c_int32),
+        ("batch_heavy", C.c_int32), ("pad", C.c_int32),
     ]
 
 
@@ -98,6 +100,11 @@ class BfsOpts:
     hub_slots: int = 0
     chunk_edges: int = 2048
     blocks_per_sm: int = 0
+    batch_alpha: float = 4.0
+    batch_small_max: int = 32
+    batch_large_min: int = 1024
+    batch_heavy: int = 4096
+    pad: int = 0
 
     def _c(self) -> _Opts:
         return _Opts(**{f.name: getattr(self, f.name) for f in fields(self)})
@@ -189,6 +196,8 @@ def lib() -> C.CDLL:
         "ent_multi_run": (C.c_int, [_P, C.POINTER(C.c_double)]),
         "ent_multi_depths": (C.c_int, [_P, C.c_int32, _I32P]),
         "ent_multi_destroy": (C.c_int, [_P]),
+        "ent_autotune": (C.c_int, [_P, _I32P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(_Opts),
+                                   C.POINTER(C.c_double)]),
         "ent_server_opts_default": (None, [C.POINTER(_ServerOpts)]),
         "ent_server_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_ServerOpts), C.POINTER(_P)]),
         "ent_server_submit": (C.c_int, [_P, C.c_int32, C.c_int32, _I64P]),

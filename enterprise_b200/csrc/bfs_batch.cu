@@ -11,7 +11,7 @@
 //   X    uint64[V][W]      visited bits
 //   log  uint64[K][V][W]   ring of K levels: log[L-base][v] = bits found at level L
 //   jf   int32[2][V]       joint frontier (vertices with any new bit), ping-pong
-//   heavy int32[2][V]      joint-frontier vertices of degree >= HEAVY
+//   heavy int32[2][V]      joint-frontier vertices of degree >= opts.batch_heavy
 //   done bit per vertex    every source has visited it (bottom-up skips it)
 //   jfb  bit per vertex    [2] joint-frontier membership of levels L and L+1:
 //                          dedups top-down claims and lets bottom-up skip the
@@ -32,10 +32,7 @@
 namespace ent {
 
 constexpr int BB = 256;        // threads per CTA
-constexpr int HEAVY = 4096;    // top-down: degree at which all CTAs share a vertex
 constexpr int KMAX = 16;       // log slots (levels per flush window)
-constexpr int SMALLB = 32;     // bottom-up: below this degree a lane group owns a vertex
-constexpr int LARGEB = 1024;   // bottom-up: from this degree a CTA owns a vertex
 constexpr int WMAX = 32;       // words per vertex per launch (2048 sources)
 
 struct BatchCtl {
@@ -74,9 +71,9 @@ struct BatchArgs {
   const unsigned long long* mask;  // [W] valid source bits
   uint32_t* donebits;
   uint32_t* jfb[2];
-  const uint32_t* lightbits;  // degree in [1, SMALLB): bottom-up light tier
-  const int32_t* mid;         // vertices with SMALLB <= degree < LARGEB
-  const int32_t* large;       // vertices with degree >= LARGEB
+  const uint32_t* lightbits;  // degree in [1, batch_small_max): bottom-up light tier
+  const int32_t* mid;         // batch_small_max <= degree < batch_large_min
+  const int32_t* large;       // degree >= batch_large_min
   int32_t n_mid, n_large;
   int32_t* jf[2];
   int32_t* heavy[2];
@@ -84,7 +81,8 @@ struct BatchArgs {
   unsigned long long* st_edges;  // per source: sum of degrees of reached vertices
   unsigned long long* st_verts;  // per source: reached vertices
   int32_t* st_maxd;              // per source: max depth
-  double alpha;
+  double alpha;      // bottom-up when frontier edges * alpha > unfinished edges
+  int32_t heavy_deg; // top-down: from this degree every CTA takes a slice of a vertex
   cudaGraphConditionalHandle cond;
   int32_t use_cond;
   int32_t max_levels;
@@ -137,7 +135,7 @@ __global__ void k_b_seed(BatchArgs a) {
       a.jf[0][atomicAdd(&s_n, 1)] = v;
       const int d = a.deg[v];
       atomicAdd(&s_m, (unsigned long long)d);
-      if (d >= HEAVY) a.heavy[0][atomicAdd(&s_h, 1)] = v;
+      if (d >= a.heavy_deg) a.heavy[0][atomicAdd(&s_h, 1)] = v;
     }
   }
   __syncthreads();
@@ -218,7 +216,7 @@ __device__ void b_td_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
   for (int i = gw; i < n; i += nw) {
     const int u = a.jf[cur][i];
     const int64_t beg = a.off[u], end = a.off[u + 1];
-    if (end - beg >= HEAVY) continue;
+    if (end - beg >= a.heavy_deg) continue;
     __syncwarp();
     for (int w = lane; w < a.W; w += 32) fw[w] = F[(size_t)u * a.W + w];
     __syncwarp();
@@ -255,7 +253,7 @@ __device__ __forceinline__ void bu_finish_vertex(const BatchArgs& a, BatchCtl* c
     my_m += (unsigned long long)d;
     atomicOr(&a.jfb[nxt][v >> 5], 1u << (v & 31));
     a.jf[nxt][atomicAdd(&c->n_jf[nxt], 1)] = v;
-    if (d >= HEAVY) a.heavy[nxt][atomicAdd(&c->n_heavy[nxt], 1)] = v;
+    if (d >= a.heavy_deg) a.heavy[nxt][atomicAdd(&c->n_heavy[nxt], 1)] = v;
   }
   if (gfull) {
     atomicOr(&a.donebits[v >> 5], 1u << (v & 31));
@@ -263,7 +261,7 @@ __device__ __forceinline__ void bu_finish_vertex(const BatchArgs& a, BatchCtl* c
   }
 }
 
-// Mid tier (SMALLB <= degree < LARGEB): one warp per vertex. Lane = (word w,
+// Mid tier (batch_small_max <= degree < batch_large_min): one warp per vertex. Lane = (word w,
 // neighbour slot k): lanes w, w+W, w+2W, ... OR word w of different
 // neighbours, so a lane keeps one accumulator and the W consecutive words of
 // a neighbour are read by W consecutive lanes.
@@ -307,7 +305,7 @@ __device__ void b_bu_mid(const BatchArgs& a, BatchCtl* c, const unsigned long lo
   }
 }
 
-// Large tier (degree >= LARGEB): one CTA per vertex, reduced through shared
+// Large tier (degree >= batch_large_min): one CTA per vertex, reduced through shared
 // memory, early exit by block vote.
 __device__ void b_bu_large(const BatchArgs& a, BatchCtl* c, const unsigned long long* F, unsigned long long* NB,
                            unsigned long long& my_m, unsigned long long& my_md) {
@@ -361,7 +359,7 @@ __device__ void b_bu_large(const BatchArgs& a, BatchCtl* c, const unsigned long 
   }
 }
 
-// Light tier (degree < SMALLB): a group of G = W / WPL lanes handles one
+// Light tier (degree < batch_small_max): a group of G = W / WPL lanes handles one
 // vertex; each lane owns WPL words.
 template <int WPL>
 __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long* s_red) {
@@ -446,7 +444,7 @@ __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
           full_bits |= 1u << vl;
           if (gany) my_md += (unsigned long long)(e1 - e0);
         }
-        if (gl == 0 && gany && e1 - e0 >= HEAVY) {
+        if (gl == 0 && gany && e1 - e0 >= a.heavy_deg) {
           const int at = atomicAdd(&c->n_heavy[nxt], 1);
           a.heavy[nxt][at] = (int)v;
         }
@@ -497,7 +495,10 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
   __shared__ unsigned long long s_red[BB / 32];
   __shared__ int s_last;
   BatchCtl* c = a.ctl;
-  if (c->done) return;
+  if (c->done) {  // never leave the while node spinning on a finished traversal
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
+    return;
+  }
   const int cur = c->cur, nxt = cur ^ 1;
   const int dir = c->dir;
   {
@@ -526,7 +527,7 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
         atomicOr(&a.donebits[v >> 5], 1u << (v & 31));
         my_md += d;
       }
-      if (d >= HEAVY) a.heavy[nxt][atomicAdd(&c->n_heavy[nxt], 1)] = v;
+      if (d >= a.heavy_deg) a.heavy[nxt][atomicAdd(&c->n_heavy[nxt], 1)] = v;
     }
     if (__syncthreads_or(my_m != 0 || my_md != 0)) {
       unsigned long long r = bsum(my_m, s_red);
@@ -766,17 +767,18 @@ __global__ void __launch_bounds__(BB) k_b_recycle(BatchArgs a, int final_flush) 
 }
 
 // Static degree tiers of a graph for the bottom-up pass (degrees never change).
-__global__ void k_b_tiers(const int32_t* __restrict__ deg, int64_t V, uint32_t* __restrict__ lightbits,
-                          int32_t* __restrict__ mid, int32_t* __restrict__ large, int32_t* __restrict__ counts) {
+__global__ void k_b_tiers(const int32_t* __restrict__ deg, int64_t V, int small_max, int large_min,
+                          uint32_t* __restrict__ lightbits, int32_t* __restrict__ mid, int32_t* __restrict__ large,
+                          int32_t* __restrict__ counts) {
   const int lane = threadIdx.x & 31;
   const int64_t nth = (int64_t)gridDim.x * blockDim.x;
   for (int64_t base = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) & ~31ll; base < V; base += nth) {
     const int64_t v = base + lane;
     const int d = v < V ? deg[v] : 0;
-    const unsigned lb = __ballot_sync(FULL, d >= 1 && d < SMALLB);
+    const unsigned lb = __ballot_sync(FULL, d >= 1 && d < small_max);
     if (lane == 0) lightbits[base >> 5] = lb;
-    wappend(d >= SMALLB && d < LARGEB, (int)v, mid, &counts[0]);
-    wappend(d >= LARGEB, (int)v, large, &counts[1]);
+    wappend(d >= small_max && d < large_min, (int)v, mid, &counts[0]);
+    wappend(d >= large_min, (int)v, large, &counts[1]);
   }
 }
 
@@ -918,9 +920,12 @@ int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
   const size_t total = sz_x + sz_log + 4 * sz_bits + 6 * sz_q + sz_mask + sz_src + sz_st + 256;
   cudaError_t e = cudaMalloc(&w->slab, total);
   if (e != cudaSuccess) { destroy_batch_workspace(w); return fail(ENT_ERR_OOM, "batch workspace (%zu bytes) failed", total); }
-  e = cudaMemset(w->slab, 0, total);
+  // Initialise on the graph's stream and wait (see create_workspace in
+  // bfs_single.cu): the runs use other, non-blocking streams.
+  e = cudaMemsetAsync(w->slab, 0, total, g->stream);
   if (e == cudaSuccess) e = cudaMalloc(&w->ctl, sizeof(BatchCtl));
-  if (e == cudaSuccess) e = cudaMemset(w->ctl, 0, sizeof(BatchCtl));
+  if (e == cudaSuccess) e = cudaMemsetAsync(w->ctl, 0, sizeof(BatchCtl), g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
   if (e == cudaSuccess) e = cudaMallocHost(&w->ctl_h, sizeof(BatchCtl));
   if (e == cudaSuccess) e = cudaEventCreate(&w->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&w->ev1);
@@ -961,12 +966,14 @@ int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
   a.st_edges = (unsigned long long*)p; p += al(sizeof(unsigned long long) * w->cap_src);
   a.st_verts = (unsigned long long*)p; p += al(sizeof(unsigned long long) * w->cap_src);
   a.st_maxd = (int32_t*)p; p += al(sizeof(int32_t) * w->cap_src);
-  a.alpha = 4.0;
+  a.alpha = g->opts.batch_alpha;
+  a.heavy_deg = g->opts.batch_heavy;
   a.max_levels = (int32_t)std::min<int64_t>(V + 2, 0x7ffffff0);
   w->smem = sizeof(unsigned long long) * std::max(W * (BB / 32), W);
   {
     const int blocks = (int)std::min<int64_t>((V + BB - 1) / BB, (int64_t)g->num_sms * 8);
-    k_b_tiers<<<blocks, BB, 0, g->stream>>>(g->deg, V, lightbits, mid, large, counts);
+    k_b_tiers<<<blocks, BB, 0, g->stream>>>(g->deg, V, g->opts.batch_small_max, g->opts.batch_large_min, lightbits,
+                                             mid, large, counts);
     g_kernel_launches++;
     int32_t hc[2] = {0, 0};
     e = cudaMemcpyAsync(hc, counts, sizeof(hc), cudaMemcpyDeviceToHost, g->stream);

@@ -143,7 +143,6 @@ __device__ void fill_neg1(int32_t* p, int64_t n, int64_t tid, int64_t nth) {
 }
 
 __global__ void __launch_bounds__(BT) k_reset(LevelArgs a, int32_t src, int32_t* depth, int32_t* parent) {
-  BfsCtl* c = a.ctl;
   const int64_t tid = blockIdx.x * (int64_t)BT + threadIdx.x, nth = (int64_t)gridDim.x * BT;
   fill_neg1(depth, a.V, tid, nth);
   if (parent) fill_neg1(parent, a.V, tid, nth);
@@ -157,15 +156,14 @@ __global__ void __launch_bounds__(BT) k_reset(LevelArgs a, int32_t src, int32_t*
     a.hub[0][i] = 0;
     a.hub[1][i] = 0;
   }
-  __shared__ int s_last;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    s_last = atomicAdd(&c->finished, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!s_last || threadIdx.x != 0) return;
-  __threadfence();
+}
+
+// Initialises the loop state for one traversal (one thread; runs after
+// k_reset, so it needs no completion counter and also resets the counters
+// the level kernels use).
+__global__ void k_init(LevelArgs a, int32_t src, int32_t* depth, int32_t* parent) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  BfsCtl* c = a.ctl;
   const int d = a.deg[src];
   const int cl = cls_of(d, a);
   depth[src] = 0;
@@ -457,7 +455,10 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   __shared__ int s_last;
   __shared__ unsigned long long s_red[BT / 32];
   BfsCtl* c = a.ctl;
-  if (c->done) return;
+  if (c->done) {  // never leave the while node spinning on a finished traversal
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
+    return;
+  }
   const int L = c->level, dir = c->dir;
   const uint32_t epoch = c->epoch;
   const int qcur = c->qcur;
@@ -636,6 +637,7 @@ struct BfsWorkspace {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaGraphNode_t reset_node = nullptr;
+  cudaGraphNode_t init_node = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -670,6 +672,10 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
   kp.sharedMemBytes = 0;
   kp.kernelParams = rargs;
   ENT_CUDA(cudaGraphAddKernelNode(&w->reset_node, graph, nullptr, 0, &kp));
+  kp.func = (void*)k_init;
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(32);
+  ENT_CUDA(cudaGraphAddKernelNode(&w->init_node, graph, &w->reset_node, 1, &kp));
   cudaGraphConditionalHandle handle;
   ENT_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
   cudaGraphNodeParams cp = {};
@@ -678,7 +684,7 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
   cp.conditional.type = cudaGraphCondTypeWhile;
   cp.conditional.size = 1;
   cudaGraphNode_t cond_node;
-  ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &w->reset_node, 1, &cp));
+  ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &w->init_node, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   LevelArgs la = w->args;
   la.cond = handle;
@@ -712,9 +718,13 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out) {
   size_t total = 3 * sz_bits + 9 * sz_q + 2 * sz_hub + sz_tiles;
   cudaError_t e = cudaMalloc(&w->slab, total);
   if (e != cudaSuccess) { destroy_bfs_workspace(w); return fail(ENT_ERR_OOM, "workspace allocation (%zu bytes) failed", total); }
-  e = cudaMemset(w->slab, 0, total);
+  // Initialise on the graph's stream and wait: the traversal runs on
+  // non-blocking streams, which a plain cudaMemset (legacy stream, async to
+  // the host) would not be ordered against.
+  e = cudaMemsetAsync(w->slab, 0, total, g->stream);
   if (e == cudaSuccess) e = cudaMalloc(&w->ctl, sizeof(BfsCtl));
-  if (e == cudaSuccess) e = cudaMemset(w->ctl, 0, sizeof(BfsCtl));
+  if (e == cudaSuccess) e = cudaMemsetAsync(w->ctl, 0, sizeof(BfsCtl), g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
   if (e == cudaSuccess) e = cudaMallocHost(&w->ctl_h, sizeof(BfsCtl));
   if (e == cudaSuccess) e = cudaMalloc(&w->depth, sizeof(int32_t) * V);
   if (e == cudaSuccess) e = cudaMalloc(&w->parent, sizeof(int32_t) * V);
@@ -801,12 +811,17 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, c
     kp.sharedMemBytes = 0;
     kp.kernelParams = rargs;
     ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec, w->reset_node, &kp));
+    kp.func = (void*)k_init;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec, w->init_node, &kp));
     ENT_CUDA(cudaGraphLaunch(w->exec, s));
   } else {
     LevelArgs la = w->args;
     la.use_cond = 0;
     k_reset<<<w->grid_reset, BT, 0, s>>>(la, src, depth, parent);
-    g_kernel_launches++;
+    k_init<<<1, 32, 0, s>>>(la, src, depth, parent);
+    g_kernel_launches += 2;
     ENT_CUDA(cudaGetLastError());
     int32_t* done_h = &w->ctl_h->done;
     for (int64_t it = 0;; ++it) {
@@ -827,10 +842,10 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, c
     float ms = 0.f;
     cudaEventElapsedTime(&ms, w->ev0, w->ev1);
     fill_stats(*w->ctl_h, ms, stats);
-    if (g->opts.loop == ENT_LOOP_GRAPH) g_kernel_launches += 1 + 2 * (int64_t)w->ctl_h->level;
+    if (g->opts.loop == ENT_LOOP_GRAPH) g_kernel_launches += 2 + 2 * (int64_t)w->ctl_h->level;
     if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "device traversal reported error flags 0x%x", w->ctl_h->err);
   } else if (g->opts.loop == ENT_LOOP_GRAPH) {
-    g_kernel_launches += 1;  // level kernels are counted when stats are read
+    g_kernel_launches += 2;  // reset + init; level kernels are counted when stats are read
   }
   return ENT_OK;
 }
@@ -869,7 +884,8 @@ int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_l
   la.use_cond = 0;
   ENT_CUDA(cudaEventRecord(w->ev0, s));
   k_reset<<<w->grid_reset, BT, 0, s>>>(la, src, w->depth, nullptr);
-  g_kernel_launches++;
+  k_init<<<1, 32, 0, s>>>(la, src, w->depth, nullptr);
+  g_kernel_launches += 2;
   int n = 0;
   for (;;) {
     ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));

@@ -310,6 +310,11 @@ void ent_bfs_opts_default(ent_bfs_opts* o) {
   o->hub_slots = 0;
   o->chunk_edges = 2048;
   o->blocks_per_sm = 0;
+  o->batch_alpha = 4.0;
+  o->batch_small_max = 32;
+  o->batch_large_min = 1024;
+  o->batch_heavy = 4096;
+  o->pad = 0;
 }
 
 int ent_graph_create(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E, int32_t gpu, ent_graph** out) {
@@ -335,8 +340,16 @@ int ent_graph_create(const int64_t* beg, const int32_t* csr, int64_t V, int64_t 
   g->device = gpu;
   int rc = graph_alloc(g, V, E);
   if (rc != ENT_OK) { graph_free(g); return rc; }
-  cudaError_t e1 = cudaMemcpy(g->off, beg, sizeof(int64_t) * (V + 1), cudaMemcpyHostToDevice);
-  cudaError_t e2 = E > 0 ? cudaMemcpy(g->adj, csr, sizeof(int32_t) * E, cudaMemcpyHostToDevice) : cudaSuccess;
+  // Upload on the graph's stream and wait for it: a cudaMemcpy from pageable
+  // memory may return before its DMA lands, and the kernels that read the
+  // CSR next run on this non-blocking stream.
+  cudaError_t e1 = cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking);
+  if (e1 == cudaSuccess)
+    e1 = cudaMemcpyAsync(g->off, beg, sizeof(int64_t) * (V + 1), cudaMemcpyHostToDevice, g->stream);
+  cudaError_t e2 = (E > 0 && e1 == cudaSuccess)
+                       ? cudaMemcpyAsync(g->adj, csr, sizeof(int32_t) * E, cudaMemcpyHostToDevice, g->stream)
+                       : cudaSuccess;
+  if (e1 == cudaSuccess && e2 == cudaSuccess) e1 = cudaStreamSynchronize(g->stream);
   if (e1 != cudaSuccess || e2 != cudaSuccess) {
     graph_free(g);
     return fail(ENT_ERR_CUDA, "CSR upload failed");
@@ -419,13 +432,19 @@ int ent_graph_set_opts(ent_graph* g, const ent_bfs_opts* o) {
   if (o->chunk_edges < 32) return fail(ENT_ERR_INVALID_ARG, "chunk_edges must be >= 32");
   if (o->alpha <= 0 || o->beta <= 0 || o->ref_ratio < 0) return fail(ENT_ERR_INVALID_ARG, "alpha/beta must be > 0");
   if (o->blocks_per_sm < 0 || o->blocks_per_sm > 32) return fail(ENT_ERR_INVALID_ARG, "blocks_per_sm out of range");
+  if (o->batch_alpha <= 0) return fail(ENT_ERR_INVALID_ARG, "batch_alpha must be > 0");
+  if (o->batch_small_max < 1 || o->batch_large_min < o->batch_small_max)
+    return fail(ENT_ERR_INVALID_ARG, "need 1 <= batch_small_max <= batch_large_min");
+  if (o->batch_heavy < 32) return fail(ENT_ERR_INVALID_ARG, "batch_heavy must be >= 32");
   std::lock_guard<std::mutex> lk(g->mu);
   g->opts = *o;
-  if (g->ws) {  // workspace graphs were captured with the old options
+  if (g->ws || g->bws) {  // workspaces were built and captured with the old options
     DeviceGuard dg(g->device);
     cudaStreamSynchronize(g->stream);
     destroy_bfs_workspace(g->ws);
     g->ws = nullptr;
+    destroy_batch_workspace(g->bws);
+    g->bws = nullptr;
   }
   return ENT_OK;
 }

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define ENT_ABI_VERSION 1
+#define ENT_ABI_VERSION 2
 
 enum ent_status {
   ENT_OK = 0,
@@ -79,6 +79,12 @@ typedef struct ent_bfs_opts {
   int32_t chunk_edges;   /* edges per CTA chunk of a large TD vertex       */
   int32_t blocks_per_sm; /* resident CTAs per SM for the level kernels,
                             0 = occupancy maximum                          */
+  /* batched (bitwise multi-source) traversal */
+  double batch_alpha;      /* bottom-up when frontier edges*alpha > unfinished edges */
+  int32_t batch_small_max; /* bottom-up: degree < this -> lane group per vertex     */
+  int32_t batch_large_min; /* bottom-up: degree >= this -> CTA per vertex           */
+  int32_t batch_heavy;     /* top-down: degree >= this -> all CTAs share the vertex */
+  int32_t pad;
 } ent_bfs_opts;
 
 typedef struct ent_stats {
@@ -242,6 +248,17 @@ int ent_multi_create(ent_graph* const* graphs, int32_t n_graphs, const int32_t* 
 int ent_multi_run(ent_multi* plan, double* device_ms);
 int ent_multi_depths(ent_multi* plan, int32_t k, int32_t* depth_out);
 int ent_multi_destroy(ent_multi* plan);
+
+/* ------------------------------------------------------ autotuning ------ */
+/* Coordinate-descent search of the traversal thresholds on this graph and
+ * GPU (the reference fixes them at compile time: bfs_gpu_opt.cuh:323-324,
+ * comm.h:155, comm.h:176-177, inspector.cuh:497). mode 0 tunes the
+ * single-source knobs (tiers, chunk size, hub cache, alpha/beta, CTAs per SM)
+ * timing ent_bfs over `src`; mode 1 tunes the batched knobs timing one
+ * ent_bfs_batch of all of `src`. Every candidate gives the same depths. The
+ * best options are applied to g and returned with their device time. */
+int ent_autotune(ent_graph* g, const int32_t* src, int32_t n_src, int32_t mode, int32_t reps,
+                 ent_bfs_opts* best, double* best_ms);
 
 /* ------------------------------------------------------- serving -------- */
 /* A request loop over device-resident graphs with continuous batching. No

@@ -122,3 +122,25 @@ def test_submissions_from_threads(eb):
             np.testing.assert_array_equal(srv.depth(r["query_id"]), ref[ids[r["query_id"]]])
             srv.release(r["query_id"])
     g.close()
+
+
+def test_fresh_graph_traversals_while_serving(eb, orc):
+    """First traversals of new graphs (workspace set-up included) run while the
+    server keeps other streams busy; their results must not depend on timing."""
+    load = [eb.Graph.grid(400, 400, 0.1, seed=101), eb.Graph.rmat(16, 16, seed=102)]
+    pools = [eb.pick_sources(g.download().beg_pos, 9, 64) for g in load]
+    with eb.Server(load, max_batch=64, slots_per_graph=2) as srv:
+        ids = [srv.submit(k % 2, int(pools[k % 2][k % 64])) for k in range(400)]
+        for seed in range(4):
+            csr = eb.Csr.rmat(14, 16, seed=200 + seed)
+            with eb.Graph.from_csr(csr) as g:
+                for src in eb.pick_sources(csr.beg_pos, seed, 3):
+                    d, _, st = g.bfs(int(src))
+                    exp, _ = orc.bfs(csr.beg_pos, csr.csr, int(src))
+                    np.testing.assert_array_equal(d, exp)
+                    db, _ = g.bfs_batch([int(src)])
+                    np.testing.assert_array_equal(db[0], exp)
+        for r in _drain(srv, len(ids)):
+            srv.release(r["query_id"])
+    for g in load:
+        g.close()
