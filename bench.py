@@ -150,6 +150,11 @@ def run_ours(args, rank, world, dist):
         tuned = {"opts": {k: v for k, v in vars(opts).items() if k != "pad"}, "cached": hit,
                  "search_s": round(time.time() - t0, 2)}
 
+    if args.loop != "graph":
+        o = g.opts
+        o.loop = eb.LOOP[args.loop]
+        g.opts = o
+
     stream = torch.cuda.Stream(device=local)
     sptr = stream.cuda_stream
     depth = torch.empty(V, dtype=torch.int32, device=f"cuda:{local}")
@@ -206,7 +211,7 @@ def run_ours(args, rank, world, dist):
     amean = float(np.mean(gteps_src))
     peak, peak_kind = measured_peak()
     achieved = float(b_alg.mean() / (mean_per_src.mean() * 1e-3) / 1e9)
-    traffic = profiled_traffic("bfs_s24_rmat_traffic.txt")
+    traffic = profiled_traffic("bfs_rmat_s24_traffic.txt") if args.scale == 24 else None
 
     # ------------------------------------------------ e2e through the C ABI
     host_depth = np.empty(V, dtype=np.int32)
@@ -546,6 +551,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner")
+    ap.add_argument("--loop", choices=["graph", "host"], default="graph",
+                    help="level loop driver; host launches each kernel (profilers can see them)")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
     ap.add_argument("--batch-scale", type=int, default=22)
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="serving run length (config: 60)")
