@@ -41,7 +41,8 @@ def graph_seed(scale):
 
 
 def source_seed(scale, rank=0):
-    return 0x50C0000 + scale + 1000 * rank
+    from enterprise_b200.replicas import source_seed as seed
+    return seed(scale, rank)
 
 
 # ----------------------------------------------------------------- clocks --
@@ -197,13 +198,12 @@ def run_ours(args, rank, world, dist):
     clocks = clk.stop()
     if dist:
         dist.barrier()
-    total_ms = float(sum(step_ms))
-    if dist:
-        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    from enterprise_b200 import replicas
+    dev = f"cuda:{local}"
     edges_per_step = float(m_c.sum())
-    value = world * edges_per_step * args.steps / (total_ms * 1e-3) / 1e9
+    job_edges, job_s, rate = replicas.job_rate(edges_per_step * args.steps, float(sum(step_ms)) * 1e-3, dist, dev)
+    total_ms = job_s * 1e3
+    value = rate / 1e9
     per = np.array(per_bfs)  # steps x sources (ms)
     mean_per_src = per.mean(axis=0)
     gteps_src = m_c / (mean_per_src * 1e-3) / 1e9
@@ -229,11 +229,8 @@ def run_ours(args, rank, world, dist):
         for s in srcs:
             g.bfs(int(s), depth_out=host_depth)
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * edges_per_step * e2e_steps / e2e_s / 1e9
+    _, _, e2e_rate = replicas.job_rate(edges_per_step * e2e_steps, e2e_s, dist, dev)
+    e2e_value = e2e_rate / 1e9
     if pinned:
         eb.host_unregister(host_depth)
 
