@@ -50,7 +50,8 @@ class _Opts(C.Structure):
         ("ref_ratio", C.c_double), ("small_max", C.c_int32), ("large_min", C.c_int32),
         ("hub_slots", C.c_int32), ("chunk_edges", C.c_int32), ("blocks_per_sm", C.c_int32),
         ("batch_alpha", C.c_double), ("batch_small_max", C.c_int32), ("batch_large_min", C.c_int32),
-        ("batch_heavy", C.c_int32), ("pad", C.c_int32),
+        ("batch_heavy", C.c_int32), ("narrow_max_frontier", C.c_int32), ("narrow_max_edges", C.c_int32),
+        ("narrow_max_degree", C.c_int32), ("narrow_cluster", C.c_int32), ("pad", C.c_int32),
     ]
 
 
@@ -58,7 +59,7 @@ class _Stats(C.Structure):
     _fields_ = [
         ("reached_vertices", C.c_int64), ("traversed_edges", C.c_int64), ("levels", C.c_int32),
         ("td_levels", C.c_int32), ("bu_levels", C.c_int32), ("status", C.c_int32),
-        ("device_ms", C.c_double),
+        ("device_ms", C.c_double), ("narrow_levels", C.c_int32), ("launches", C.c_int32),
     ]
 
 
@@ -104,6 +105,10 @@ class BfsOpts:
     batch_small_max: int = 32
     batch_large_min: int = 1024
     batch_heavy: int = 4096
+    narrow_max_frontier: int = 8192
+    narrow_max_edges: int = 131072
+    narrow_max_degree: int = 256
+    narrow_cluster: int = 0
     pad: int = 0
 
     def _c(self) -> _Opts:
@@ -125,11 +130,13 @@ class Stats:
     bu_levels: int
     status: int
     device_ms: float
+    narrow_levels: int = 0
+    launches: int = 0
 
     @staticmethod
     def _from_c(s: _Stats) -> "Stats":
         return Stats(s.reached_vertices, s.traversed_edges, s.levels, s.td_levels, s.bu_levels, s.status,
-                     s.device_ms)
+                     s.device_ms, s.narrow_levels, s.launches)
 
     @property
     def gteps(self) -> float:

@@ -1052,6 +1052,8 @@ static int read_batch_stats(ent_graph* g, BatchWorkspace* w, int32_t n_src, cuda
     stats[i].bu_levels = w->ctl_h->bu_levels;
     stats[i].status = w->ctl_h->err;
     stats[i].device_ms = ms;
+    stats[i].narrow_levels = 0;
+    stats[i].launches = 3 + 4 * w->ctl_h->level;  // shared by the batch
   }
   g_kernel_launches += 3 + 4 * (int64_t)w->ctl_h->level;
   if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "batched traversal reported error flags 0x%x", w->ctl_h->err);
@@ -1074,6 +1076,8 @@ int batch_source_stats(BatchWorkspace* w, int32_t n_src, cudaStream_t s, ent_sta
     stats[i].bu_levels = w->ctl_h->bu_levels;
     stats[i].status = w->ctl_h->err;
     stats[i].device_ms = 0;
+    stats[i].narrow_levels = 0;
+    stats[i].launches = 3 + 4 * w->ctl_h->level;  // shared by the batch
   }
   g_kernel_launches += 3 + 4 * (int64_t)w->ctl_h->level;
   return w->ctl_h->err ? fail(ENT_ERR_TIMEOUT, "batched traversal error flags 0x%x", w->ctl_h->err) : ENT_OK;

@@ -30,10 +30,22 @@
 //  * The direction policy runs on the device in the inspector's last CTA
 //    (reference rule inspector.cuh:486-521 is one option; Beamer alpha/beta
 //    with switch-back is the default).
+//  * Small frontiers (high-diameter graphs such as grids, and the first and
+//    last levels of any traversal) would pay two grid-wide launches per level.
+//    While the TD frontier stays small, one thread-block cluster runs level
+//    after level inside a single launch instead (k_narrow): the frontier lives
+//    in the CTAs' shared memory (read across the cluster through distributed
+//    shared memory), levels are separated by the hardware cluster barrier, and
+//    each queue entry carries the vertex's row start and degree, read while
+//    its visit was being claimed, so a level costs one adjacency read, one
+//    status probe and one claim on its critical path.
 //  * The whole traversal is one CUDA graph: a reset kernel, then a while node
-//    whose body is [expand, inspect]; the inspector sets the loop condition.
+//    whose body is [expand, inspect, if(narrow){narrow}]; the inspector sets
+//    both conditions.
 #include <algorithm>
 #include <string.h>
+
+#include <cooperative_groups.h>
 
 #include "dev_common.cuh"
 #include "dev_graph.h"
@@ -45,6 +57,11 @@ constexpr int IPT = 4;           // items per thread in an inspector tile
 constexpr int TILE = BT * IPT;   // items per inspector tile
 constexpr int KS = 4;            // look-back status words per tile
 constexpr int TD = 0, BU = 1;
+constexpr int NT = 1024;         // threads per CTA of the small-frontier kernel
+constexpr int NWARP = NT / 32;
+constexpr int NC_MAX = 16;       // CTAs per cluster, at most
+constexpr int NQCAP = 4096;      // small-frontier entries per CTA and buffer
+constexpr uint32_t NF_HEAVY = 1, NF_SPILL = 2;
 
 // Device-resident loop state. Written only by the reset kernel's and the
 // inspector's last CTA (plus atomics on the acc_* counters and n_raw); read
@@ -61,9 +78,16 @@ struct BfsCtl {
   int32_t n_chunks;   // chunks of the large TD queue
   int32_t n_raw;      // TD raw next-frontier count (atomic append)
   int32_t done;
+  int32_t narrow;     // next level runs in the small-frontier kernel (next to `done`: read together)
   int32_t err;        // bit 1: look-back wait timed out, 2: level overflow, 3: count overflow
   int32_t td_levels;
   int32_t bu_levels;
+  int32_t skip;       // the small-frontier kernel already expanded this level
+  int32_t narrow_levels;
+  int32_t iters;      // inspector launches (level-loop iterations)
+  int32_t narrow_runs;
+  uint32_t n_spill;   // small-frontier entries that did not fit in shared memory
+  uint32_t acc_maxd;  // maximum degree in the next frontier being classified
   int64_t n_f, m_f;   // frontier size and degree sum
   int64_t n_vis, m_vis;
   unsigned long long acc_n, acc_m;  // next frontier size / degree sum being accumulated
@@ -92,8 +116,13 @@ struct LevelArgs {
   int32_t policy;
   double alpha, beta, ref_ratio;
   cudaGraphConditionalHandle cond;
+  cudaGraphConditionalHandle cond_narrow;
   int32_t use_cond;
   int32_t max_levels;
+  // small-frontier mode: enter at <= narrow_f vertices, <= narrow_m edges and
+  // no degree above narrow_deg; leave above exit_f vertices or exit_m edges.
+  int32_t narrow_f, exit_f, narrow_deg;
+  int64_t narrow_m, exit_m;
 };
 
 __device__ __forceinline__ int cls_of(int d, const LevelArgs& a) {
@@ -126,6 +155,18 @@ __device__ __forceinline__ T block_sum(T x, T* s_red) {
   T r = 0;
   if (threadIdx.x == 0)
     for (int w = 0; w < BT / 32; ++w) r += s_red[w];
+  return r;  // valid in thread 0
+}
+
+__device__ __forceinline__ uint32_t block_max(uint32_t x, uint32_t* s_red) {
+  x = __reduce_max_sync(FULL, x);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) s_red[warp] = x;
+  __syncthreads();
+  uint32_t r = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < BT / 32; ++w) r = max(r, s_red[w]);
   return r;  // valid in thread 0
 }
 
@@ -187,9 +228,16 @@ __global__ void k_init(LevelArgs a, int32_t src, int32_t* depth, int32_t* parent
   }
   c->n_raw = 0;
   c->done = 0;
+  c->narrow = 0;
   c->err = 0;
   c->td_levels = 0;
   c->bu_levels = 0;
+  c->skip = 0;
+  c->narrow_levels = 0;
+  c->iters = 0;
+  c->narrow_runs = 0;
+  c->n_spill = 0;
+  c->acc_maxd = 0;
   c->n_f = 1;
   c->m_f = d;
   c->n_vis = 1;
@@ -407,7 +455,7 @@ __global__ void __launch_bounds__(BT) k_expand(LevelArgs a) {
   extern __shared__ int32_t s_hub[];
   __shared__ unsigned long long s_red[BT / 32];
   BfsCtl* c = a.ctl;
-  if (c->done) return;
+  if (c->done || c->skip) return;
   const int L = c->level;
   if (c->dir == TD) td_expand(a, c, L, c->depth, c->parent);
   else bu_expand(a, c, L, c->depth, c->parent, s_hub, s_red);
@@ -454,9 +502,16 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   __shared__ uint32_t s_tile;
   __shared__ int s_last;
   __shared__ unsigned long long s_red[BT / 32];
+  __shared__ uint32_t s_redu[BT / 32];
   BfsCtl* c = a.ctl;
   if (c->done) {  // never leave the while node spinning on a finished traversal
-    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      c->iters = c->iters + 1;
+      if (a.use_cond) {
+        cudaGraphSetConditional(a.cond, 0u);
+        if (a.narrow_f > 0) cudaGraphSetConditional(a.cond_narrow, 0u);
+      }
+    }
     return;
   }
   const int L = c->level, dir = c->dir;
@@ -473,6 +528,7 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   uint32_t* fbo = a.fb[L & 1];
   const uint32_t* fbn = a.fb[(L + 1) & 1];
   unsigned long long my_m = 0;
+  uint32_t my_maxd = 0;
   bool to_td = false;
 
   if (dir == TD) {
@@ -499,6 +555,7 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
         if (cl[j] >= 0) {
           cnt[cl[j]]++;
           my_m += dg[j];
+          my_maxd = max(my_maxd, (uint32_t)dg[j]);
           hub_insert(a, hub_next, v[j], dg[j]);
           if (cl[j] == 2) cnt[3] += n_chunks_of(dg[j], a);
         }
@@ -538,6 +595,7 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
           const int v = (int)(wi * 32 + __ffs(m) - 1);
           const int d = a.deg[v];
           const int cl = cls_of(d, a);
+          my_maxd = max(my_maxd, (uint32_t)d);
           cnt[cl]++;
           if (cl == 2) cnt[3] += n_chunks_of(d, a);
         }
@@ -564,6 +622,10 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   if (dir == TD && __syncthreads_or(my_m != 0)) {
     const unsigned long long r = block_sum(my_m, s_red);
     if (threadIdx.x == 0) atomicAdd(&c->acc_m, r);
+  }
+  if (a.narrow_f > 0 && __syncthreads_or(my_maxd != 0)) {
+    const uint32_t r = block_max(my_maxd, s_redu);
+    if (threadIdx.x == 0 && r > ld_cg(&c->acc_maxd)) atomicMax(&c->acc_maxd, r);
   }
   if (threadIdx.x == 0) {
     __threadfence();
@@ -610,7 +672,14 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
     vc->err = vc->err | 8;
     done = 1;
   }
+  // Small-frontier mode for the next level (top-down only).
+  const int narrow = !done && next_dir == TD && a.narrow_f > 0 && n_next <= a.narrow_f &&
+                     m_next <= a.narrow_m && (int64_t)vc->acc_maxd <= a.narrow_deg;
   vc->done = done;
+  vc->narrow = narrow;
+  vc->skip = 0;
+  vc->acc_maxd = 0;
+  vc->iters = vc->iters + 1;
   vc->n_raw = 0;
   vc->acc_n = 0;
   vc->acc_m = 0;
@@ -619,7 +688,263 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   vc->finished = 0;
   vc->epoch = epoch + 1;
   __threadfence();
-  if (a.use_cond) cudaGraphSetConditional(a.cond, done ? 0u : 1u);
+  if (a.use_cond) {
+    cudaGraphSetConditional(a.cond, done ? 0u : 1u);
+    if (a.narrow_f > 0) cudaGraphSetConditional(a.cond_narrow, narrow ? 1u : 0u);
+  }
+}
+
+// ------------------------------------------------------ small frontier ----
+namespace cg = cooperative_groups;
+
+// A small-frontier queue entry: vertex, degree, row start (16 bytes).
+__device__ __forceinline__ int4 nentry(int v, int d, int64_t st) {
+  return make_int4(v, d, (int)(uint32_t)st, (int)(uint32_t)((uint64_t)st >> 32));
+}
+
+struct NarrowOut {
+  int4* q;                   // this CTA's next-frontier buffer
+  uint32_t* cnt;             // its append counter (may pass NQCAP: the rest spills)
+  unsigned long long* msum;  // degree sum of the appended vertices
+  uint32_t* flag;            // NF_HEAVY | NF_SPILL
+  int32_t* spill;            // global overflow list
+};
+
+// Claims v for depth ln. The row of a claimed vertex is read in the shadow of
+// the claim (the offsets load is issued before the atomic's result is needed).
+__device__ __forceinline__ void narrow_visit(const LevelArgs& a, BfsCtl* c, int v, int u, bool valid, int ln,
+                                             int32_t* depth, int32_t* parent, const NarrowOut& o) {
+  bool mine = false;
+  int vd = 0;
+  int64_t vst = 0;
+  if (valid) {
+    const uint32_t w = (uint32_t)v >> 5, b = 1u << (v & 31);
+    if (!(ld_cg(a.vis + w) & b)) {
+      const int64_t o0 = __ldg(a.off + v), o1 = __ldg(a.off + v + 1);
+      const uint32_t old = atomicOr(a.vis + w, b);
+      if (!(old & b)) {
+        mine = true;
+        vst = o0;
+        vd = (int)(o1 - o0);
+        depth[v] = ln;
+        if (parent) parent[v] = u;
+      }
+    }
+  }
+  const unsigned m = __ballot_sync(FULL, mine);
+  if (!m) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(o.cnt, (uint32_t)__popc(m));
+  base = __shfl_sync(FULL, base, leader);
+  const unsigned wsum = __reduce_add_sync(FULL, mine ? (unsigned)vd : 0u);
+  const bool heavy = __any_sync(FULL, mine && vd > a.narrow_deg);
+  if (lane == leader) {
+    atomicAdd(o.msum, (unsigned long long)wsum);
+    if (heavy) atomicOr(o.flag, NF_HEAVY);
+  }
+  if (mine) {
+    const uint32_t pos = base + __popc(m & lanemask_lt());
+    if (pos < (uint32_t)NQCAP) {
+      o.q[pos] = nentry(v, vd, vst);
+    } else {
+      o.spill[atomicAdd(&c->n_spill, 1u)] = v;
+      atomicOr(o.flag, NF_SPILL);
+    }
+  }
+}
+
+// Runs top-down levels of a small frontier inside one launch of one cluster
+// (grid = one cluster of nc CTAs). Entered with frontier L0 classified in
+// q[qcur] (the state the inspector leaves). Leaves either
+//  * done (frontier empty or level limit), or
+//  * the state the top-down expander leaves after level Lx-1: frontier Lx in
+//    raw[0, n_raw) with its bits in fb[Lx & 1], and `skip` set so that the
+//    expander of the next loop iteration does nothing and the inspector
+//    classifies raw as usual.
+// Every CTA takes the same decisions from the same cluster-wide counts, so all
+// reach the same cluster barriers; there are no spin waits.
+__global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
+  extern __shared__ int4 s_q[];  // [2][NQCAP]
+  __shared__ uint32_t s_cnt[2], s_flag[2];
+  __shared__ unsigned long long s_m[2];
+  __shared__ uint32_t r_cnt[NC_MAX], r_flag[NC_MAX];
+  __shared__ unsigned long long r_m[NC_MAX];
+  cg::cluster_group cl = cg::this_cluster();
+  BfsCtl* c = a.ctl;
+  if (c->done || !c->narrow) return;  // same value in every CTA
+  const int nc = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int gw = rank * NWARP + (tid >> 5), nwt = nc * NWARP;
+  int32_t* depth = c->depth;
+  int32_t* parent = c->parent;
+  const int L0 = c->level;
+  const int qcur = c->qcur;
+  int32_t* spill = a.q[qcur ^ 1][0];
+
+  // Entry: each CTA loads a slice of frontier L0 (with its rows) into buffer 0
+  // and clears the frontier's bits (nothing reads them during the run).
+  {
+    const int n0 = c->n_q[0], n1 = c->n_q[1], n2 = c->n_q[2];
+    const int N0 = n0 + n1 + n2;
+    const int lo = (int)((int64_t)N0 * rank / nc), hi = (int)((int64_t)N0 * (rank + 1) / nc);
+    uint32_t* fbo = a.fb[L0 & 1];
+    for (int i = lo + tid; i < hi; i += NT) {
+      const int u = i < n0 ? a.q[qcur][0][i] : (i < n0 + n1 ? a.q[qcur][1][i - n0] : a.q[qcur][2][i - n0 - n1]);
+      const int64_t st = a.off[u];
+      s_q[i - lo] = nentry(u, (int)(a.off[u + 1] - st), st);
+      fbo[(uint32_t)u >> 5] = 0;
+    }
+    // the hub table of frontier L0 would be stale for a later bottom-up level
+    if (a.hub_slots)
+      for (int i = rank * NT + tid; i < a.hub_slots; i += nc * NT) a.hub[L0 & 1][i] = 0;
+    if (tid == 0) {
+      s_cnt[0] = (uint32_t)(hi - lo);
+      s_m[0] = 0;
+      s_flag[0] = 0;
+    }
+  }
+  cl.sync();
+
+  unsigned long long n_vis = (unsigned long long)c->n_vis, m_vis = (unsigned long long)c->m_vis;
+  int64_t nf_last = c->n_f, mf_last = c->m_f;
+  int L = L0;
+  int outcome = 0;  // 1 frontier empty, 2 hand over, 3 level limit
+  uint32_t n_all = 0;
+  for (int it = 0;; ++it) {
+    const int cur = it & 1, nxt = cur ^ 1;
+    // Counts of frontier L from every CTA of the cluster.
+    if (tid < nc) {
+      r_cnt[tid] = *cl.map_shared_rank(&s_cnt[cur], tid);
+      r_m[tid] = *cl.map_shared_rank(&s_m[cur], tid);
+      r_flag[tid] = *cl.map_shared_rank(&s_flag[cur], tid);
+    }
+    if (tid == 0) {  // buffer nxt was last read before the previous cluster barrier
+      s_cnt[nxt] = 0;
+      s_m[nxt] = 0;
+      s_flag[nxt] = 0;
+    }
+    __syncthreads();
+    n_all = 0;
+    uint32_t flags = 0;
+    unsigned long long m_all = 0;
+    for (int r = 0; r < nc; ++r) {
+      n_all += r_cnt[r];
+      m_all += r_m[r];
+      flags |= r_flag[r];
+    }
+    if (n_all == 0) outcome = 1;
+    else if (it > 0 && (flags || n_all > (uint32_t)a.exit_f || (int64_t)m_all > a.exit_m)) outcome = 2;
+    else if (L + 1 >= a.max_levels) outcome = 3;
+    if (outcome) break;
+    if (it > 0) {
+      n_vis += n_all;
+      m_vis += m_all;
+      nf_last = n_all;
+      mf_last = (int64_t)m_all;
+    }
+
+    // Expand level L: warp gw takes k consecutive entries of the cluster-wide
+    // frontier (entries of CTA r follow those of CTAs < r) and walks their
+    // concatenated rows 32 edges at a time.
+    const NarrowOut o{s_q + nxt * NQCAP, &s_cnt[nxt], &s_m[nxt], &s_flag[nxt], spill};
+    const int ln = L + 1;
+    int k = (int)((n_all + nwt - 1) / nwt);
+    if (k > 32) k = 32;
+    for (int first = gw * k; first < (int)n_all; first += nwt * k) {
+      const int i = first + lane;
+      int u = -1, d = 0;
+      int64_t st = 0;
+      if (lane < k && i < (int)n_all) {
+        int r = 0, base = 0;
+        while (r < nc - 1 && i >= base + (int)r_cnt[r]) {
+          base += (int)r_cnt[r];
+          ++r;
+        }
+        const int4 e = *(cl.map_shared_rank(s_q + cur * NQCAP, r) + (i - base));
+        u = e.x;
+        d = e.y;
+        st = (int64_t)(((uint64_t)(uint32_t)e.w << 32) | (uint32_t)e.z);
+      }
+      int incl = d;
+#pragma unroll
+      for (int ofs = 1; ofs < 32; ofs <<= 1) {
+        const int y = __shfl_up_sync(FULL, incl, ofs);
+        if (lane >= ofs) incl += y;
+      }
+      const int total = __shfl_sync(FULL, incl, 31);
+      const int excl = incl - d;
+      for (int rr = 0; rr < total; rr += 32) {
+        const int kk = rr + lane;
+        const bool valid = kk < total;
+        int j = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int cand = j + step;
+          const int ev = __shfl_sync(FULL, excl, cand & 31);
+          if (cand < 32 && ev <= kk) j = cand;
+        }
+        const int64_t sj = __shfl_sync(FULL, st, j);
+        const int ej = __shfl_sync(FULL, excl, j);
+        const int uj = __shfl_sync(FULL, u, j);
+        const int v = valid ? __ldg(a.adj + sj + (kk - ej)) : 0;
+        narrow_visit(a, c, v, uj, valid, ln, depth, parent, o);
+      }
+    }
+    cl.sync();
+    ++L;
+  }
+  cl.sync();  // no CTA leaves while another may still read its counters
+
+  const int cur = (L - L0) & 1;
+  if (outcome == 2) {
+    // Hand over frontier L: this CTA's stored entries to raw[base, ...),
+    // spilled ones after all stored entries; set their frontier bits.
+    uint32_t base = 0, n_stored = 0;
+    for (int r = 0; r < nc; ++r) {
+      const uint32_t sr = min(r_cnt[r], (uint32_t)NQCAP);
+      if (r < rank) base += sr;
+      n_stored += sr;
+    }
+    uint32_t* fbn = a.fb[L & 1];
+    const uint32_t mine = min(r_cnt[rank], (uint32_t)NQCAP);
+    for (uint32_t j = tid; j < mine; j += NT) {
+      const int v = s_q[cur * NQCAP + j].x;
+      a.raw[base + j] = v;
+      red_or(fbn + ((uint32_t)v >> 5), 1u << (v & 31));
+    }
+    for (uint32_t j = rank * NT + tid; j < n_all - n_stored; j += nc * NT) {
+      const int v = __ldcg(spill + j);
+      a.raw[n_stored + j] = v;
+      red_or(fbn + ((uint32_t)v >> 5), 1u << (v & 31));
+    }
+  }
+  if (rank != 0 || tid != 0) return;
+  c->narrow_levels += L - L0;
+  c->narrow_runs += 1;
+  c->narrow = 0;
+  c->n_spill = 0;
+  c->n_vis = (int64_t)n_vis;
+  c->m_vis = (int64_t)m_vis;
+  if (outcome == 2) {
+    c->level = L - 1;  // as if the expander had just run level L-1
+    c->td_levels += L - 1 - L0;
+    c->n_raw = (int32_t)n_all;
+    for (int q = 0; q < 3; ++q) c->n_q[q] = 0;
+    c->n_chunks = 0;
+    c->n_f = nf_last;
+    c->m_f = mf_last;
+    c->acc_m = 0;
+    c->skip = 1;
+  } else {
+    c->level = L;
+    c->td_levels += L - L0;
+    c->n_f = 0;
+    c->m_f = 0;
+    if (outcome == 3) c->err |= 4;
+    c->done = 1;
+  }
+  __threadfence();
 }
 
 // ------------------------------------------------------------- host -------
@@ -634,6 +959,8 @@ struct BfsWorkspace {
   LevelArgs args;
   int grid_reset = 0, grid_expand = 0, grid_inspect = 0;
   size_t smem_expand = 0;
+  int narrow_nc = 0;        // CTAs of the small-frontier cluster (0: mode off)
+  size_t smem_narrow = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaGraphNode_t reset_node = nullptr;
@@ -686,17 +1013,90 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
   cudaGraphNode_t cond_node;
   ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &w->init_node, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
+  // Loop body: expand -> inspect -> if (narrow) { small-frontier cluster }.
   LevelArgs la = w->args;
   la.cond = handle;
   la.use_cond = 1;
-  ENT_CUDA(cudaStreamBeginCaptureToGraph(g->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  k_expand<<<w->grid_expand, BT, w->smem_expand, g->stream>>>(la);
-  k_inspect<<<w->grid_inspect, BT, 0, g->stream>>>(la);
-  cudaGraph_t captured;
-  cudaError_t e = cudaStreamEndCapture(g->stream, &captured);
-  if (e != cudaSuccess) return fail(ENT_ERR_CUDA, "level-loop capture failed: %s", cudaGetErrorString(e));
+  if (w->narrow_nc > 0)
+    ENT_CUDA(cudaGraphConditionalHandleCreate(&la.cond_narrow, body, 0, cudaGraphCondAssignDefault));
+  void* largs[1] = {&la};
+  cudaKernelNodeParams bp = {};
+  bp.func = (void*)k_expand;
+  bp.gridDim = dim3(w->grid_expand);
+  bp.blockDim = dim3(BT);
+  bp.sharedMemBytes = (unsigned)w->smem_expand;
+  bp.kernelParams = largs;
+  cudaGraphNode_t n_expand, n_inspect;
+  ENT_CUDA(cudaGraphAddKernelNode(&n_expand, body, nullptr, 0, &bp));
+  bp.func = (void*)k_inspect;
+  bp.gridDim = dim3(w->grid_inspect);
+  bp.sharedMemBytes = 0;
+  ENT_CUDA(cudaGraphAddKernelNode(&n_inspect, body, &n_expand, 1, &bp));
+  if (w->narrow_nc > 0) {
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = la.cond_narrow;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t n_if, n_narrow;
+    ENT_CUDA(cudaGraphAddNode(&n_if, body, &n_inspect, 1, &ip));
+    bp.func = (void*)k_narrow;
+    bp.gridDim = dim3(w->narrow_nc);
+    bp.blockDim = dim3(NT);
+    bp.sharedMemBytes = (unsigned)w->smem_narrow;
+    ENT_CUDA(cudaGraphAddKernelNode(&n_narrow, ip.conditional.phGraph_out[0], nullptr, 0, &bp));
+    cudaLaunchAttributeValue cv = {};
+    cv.clusterDim.x = (unsigned)w->narrow_nc;
+    cv.clusterDim.y = 1;
+    cv.clusterDim.z = 1;
+    ENT_CUDA(cudaGraphKernelNodeSetAttribute(n_narrow, cudaLaunchAttributeClusterDimension, &cv));
+  }
   ENT_CUDA(cudaGraphInstantiate(&w->exec, graph, 0));
   return ENT_OK;
+}
+
+static cudaError_t launch_narrow(const BfsWorkspace* w, const LevelArgs& la, cudaStream_t s) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(w->narrow_nc);
+  cfg.blockDim = dim3(NT);
+  cfg.dynamicSmemBytes = w->smem_narrow;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)w->narrow_nc;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_narrow, la);
+}
+
+// Largest cluster (<= limit CTAs, 0 = no limit) of the small-frontier kernel
+// that can be resident on this GPU; 0 if none.
+static int pick_narrow_cluster(int limit, size_t smem) {
+  if (cudaFuncSetAttribute(k_narrow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_narrow, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  for (int nc = NC_MAX; nc >= 1; nc >>= 1) {
+    if (limit > 0 && nc > limit) continue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nc);
+    cfg.blockDim = dim3(NT);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)nc;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, k_narrow, &cfg) == cudaSuccess && n >= 1) return nc;
+    cudaGetLastError();
+  }
+  return 0;
 }
 
 static int create_workspace(ent_graph* g, BfsWorkspace** out) {
@@ -774,6 +1174,15 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out) {
   w->grid_expand = g->num_sms * occ_e;
   w->grid_inspect = g->num_sms * std::min(occ_i, 4);
   w->grid_reset = g->num_sms * 4;
+  w->smem_narrow = 2 * NQCAP * sizeof(int4);
+  w->narrow_nc = o.narrow_max_frontier > 0 ? pick_narrow_cluster(o.narrow_cluster, w->smem_narrow) : 0;
+  if (w->narrow_nc > 0) {
+    a.narrow_f = std::min(o.narrow_max_frontier, w->narrow_nc * NQCAP / 2);
+    a.exit_f = 2 * a.narrow_f;
+    a.narrow_m = o.narrow_max_edges;
+    a.exit_m = 2 * (int64_t)o.narrow_max_edges;
+    a.narrow_deg = o.narrow_max_degree;
+  }
   if (o.loop == ENT_LOOP_GRAPH) {
     int rc = build_graph(g, w);
     if (rc != ENT_OK) { destroy_bfs_workspace(w); return rc; }
@@ -790,6 +1199,8 @@ static void fill_stats(const BfsCtl& h, float ms, ent_stats* stats) {
   stats->bu_levels = h.bu_levels;
   stats->status = h.err;
   stats->device_ms = ms;
+  stats->narrow_levels = h.narrow_levels;
+  stats->launches = 2 + 2 * h.iters + h.narrow_runs;
 }
 
 int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, cudaStream_t stream, ent_stats* stats) {
@@ -823,15 +1234,19 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, c
     k_init<<<1, 32, 0, s>>>(la, src, depth, parent);
     g_kernel_launches += 2;
     ENT_CUDA(cudaGetLastError());
-    int32_t* done_h = &w->ctl_h->done;
+    int32_t* flags_h = &w->ctl_h->done;  // done, narrow
     for (int64_t it = 0;; ++it) {
       k_expand<<<w->grid_expand, BT, w->smem_expand, s>>>(la);
       k_inspect<<<w->grid_inspect, BT, 0, s>>>(la);
       g_kernel_launches += 2;
       ENT_CUDA(cudaGetLastError());
-      ENT_CUDA(cudaMemcpyAsync(done_h, &w->ctl->done, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+      ENT_CUDA(cudaMemcpyAsync(flags_h, &w->ctl->done, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
       ENT_CUDA(cudaStreamSynchronize(s));
-      if (*done_h) break;
+      if (flags_h[0]) break;
+      if (flags_h[1]) {
+        ENT_CUDA(launch_narrow(w, la, s));
+        g_kernel_launches += 1;
+      }
       if (it > w->V + 2) return fail(ENT_ERR_INTERNAL, "level loop did not terminate");
     }
   }
@@ -842,7 +1257,7 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, c
     float ms = 0.f;
     cudaEventElapsedTime(&ms, w->ev0, w->ev1);
     fill_stats(*w->ctl_h, ms, stats);
-    if (g->opts.loop == ENT_LOOP_GRAPH) g_kernel_launches += 2 + 2 * (int64_t)w->ctl_h->level;
+    if (g->opts.loop == ENT_LOOP_GRAPH) g_kernel_launches += stats->launches;
     if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "device traversal reported error flags 0x%x", w->ctl_h->err);
   } else if (g->opts.loop == ENT_LOOP_GRAPH) {
     g_kernel_launches += 2;  // reset + init; level kernels are counted when stats are read
@@ -893,6 +1308,26 @@ int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_l
     const BfsCtl h = *w->ctl_h;
     if (h.done || n >= max_levels) break;
     ent_level_trace& t = out[n];
+    if (h.narrow) {  // one row for a run of the small-frontier kernel (direction 2)
+      t.level = h.level;
+      t.direction = 2;
+      t.bu_sweep = 0;
+      t.pad = 0;
+      t.frontier_vertices = h.n_f;
+      t.frontier_edges = h.m_f;
+      t.unvisited_queued = 0;
+      ENT_CUDA(cudaEventRecord(e[0], s));
+      ENT_CUDA(launch_narrow(w, la, s));
+      ENT_CUDA(cudaEventRecord(e[1], s));
+      g_kernel_launches += 1;
+      ENT_CUDA(cudaEventSynchronize(e[1]));
+      float ta = 0;
+      cudaEventElapsedTime(&ta, e[0], e[1]);
+      t.expand_ms = ta;
+      t.inspect_ms = 0;
+      ++n;
+      continue;
+    }
     t.level = h.level;
     t.direction = h.dir;
     t.bu_sweep = h.dir == BU;

@@ -314,6 +314,10 @@ void ent_bfs_opts_default(ent_bfs_opts* o) {
   o->batch_small_max = 32;
   o->batch_large_min = 1024;
   o->batch_heavy = 4096;
+  o->narrow_max_frontier = 8192;
+  o->narrow_max_edges = 131072;
+  o->narrow_max_degree = 256;
+  o->narrow_cluster = 0;
   o->pad = 0;
 }
 
@@ -436,6 +440,11 @@ int ent_graph_set_opts(ent_graph* g, const ent_bfs_opts* o) {
   if (o->batch_small_max < 1 || o->batch_large_min < o->batch_small_max)
     return fail(ENT_ERR_INVALID_ARG, "need 1 <= batch_small_max <= batch_large_min");
   if (o->batch_heavy < 32) return fail(ENT_ERR_INVALID_ARG, "batch_heavy must be >= 32");
+  if (o->narrow_max_frontier < 0 || o->narrow_max_frontier > 16384)
+    return fail(ENT_ERR_INVALID_ARG, "narrow_max_frontier must be in [0, 16384]");
+  if (o->narrow_max_edges < 0 || o->narrow_max_degree < 1 || o->narrow_max_degree > (1 << 20))
+    return fail(ENT_ERR_INVALID_ARG, "need narrow_max_edges >= 0 and 1 <= narrow_max_degree <= 2^20");
+  if (o->narrow_cluster < 0 || o->narrow_cluster > 16) return fail(ENT_ERR_INVALID_ARG, "narrow_cluster must be in [0, 16]");
   std::lock_guard<std::mutex> lk(g->mu);
   g->opts = *o;
   if (g->ws || g->bws) {  // workspaces were built and captured with the old options

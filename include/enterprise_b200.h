@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define ENT_ABI_VERSION 2
+#define ENT_ABI_VERSION 3
 
 enum ent_status {
   ENT_OK = 0,
@@ -84,6 +84,16 @@ typedef struct ent_bfs_opts {
   int32_t batch_small_max; /* bottom-up: degree < this -> lane group per vertex     */
   int32_t batch_large_min; /* bottom-up: degree >= this -> CTA per vertex           */
   int32_t batch_heavy;     /* top-down: degree >= this -> all CTAs share the vertex */
+  /* small-frontier ("narrow") mode of the single-source traversal: while the
+     top-down frontier stays small, one thread-block cluster runs level after
+     level inside a single launch. Entered when the frontier has at most
+     narrow_max_frontier vertices, narrow_max_edges edges and no vertex of
+     degree > narrow_max_degree; left when it grows past twice the first two
+     or meets such a vertex. narrow_max_frontier = 0 disables the mode. */
+  int32_t narrow_max_frontier;
+  int32_t narrow_max_edges;
+  int32_t narrow_max_degree;
+  int32_t narrow_cluster;  /* CTAs in the cluster (1..16), 0 = largest that fits */
   int32_t pad;
 } ent_bfs_opts;
 
@@ -96,6 +106,9 @@ typedef struct ent_stats {
   int32_t bu_levels;        /* levels expanded bottom-up                          */
   int32_t status;           /* device status word (0 ok)                          */
   double device_ms;         /* CUDA-event time of the traversal on the device     */
+  int32_t narrow_levels;    /* of td_levels, those run inside the small-frontier
+                               cluster kernel                                     */
+  int32_t launches;         /* kernels launched by this traversal                 */
 } ent_stats;
 
 typedef struct ent_graph ent_graph; /* device-resident CSR + traversal state */

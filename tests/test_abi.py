@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol(eb):
 
 
 def test_abi_version_and_defaults(eb):
-    assert eb.lib().ent_abi_version() == 2
+    assert eb.lib().ent_abi_version() == 3
     o = eb.BfsOpts()
     import ctypes
     c = eb._Opts()
@@ -39,8 +39,8 @@ def test_abi_version_and_defaults(eb):
 
 def test_struct_layout_matches_header(eb):
     import ctypes
-    assert ctypes.sizeof(eb._Opts) == 4 + 4 + 8 * 3 + 4 * 5 + 4 + 8 + 4 * 4
-    assert ctypes.sizeof(eb._Stats) == 8 + 8 + 4 * 4 + 8
+    assert ctypes.sizeof(eb._Opts) == 4 + 4 + 8 * 3 + 4 * 5 + 4 + 8 + 4 * 8
+    assert ctypes.sizeof(eb._Stats) == 8 + 8 + 4 * 4 + 8 + 4 * 2
 
 
 def test_invalid_arguments_return_status(eb):

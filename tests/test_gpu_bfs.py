@@ -35,22 +35,26 @@ def _check(eb, orc, csr, g, src, parents=True):
     return st
 
 
+# narrow: the small-frontier cluster kernel on (default) or off (every level
+# through the grid-wide expander and inspector)
+@pytest.mark.parametrize("narrow", [8192, 0])
 @pytest.mark.parametrize("policy", POLICIES)
 @pytest.mark.parametrize("loop", ["graph", "host"])
-def test_hand_graphs_all_sources(eb, orc, policy, loop):
+def test_hand_graphs_all_sources(eb, orc, policy, loop, narrow):
     for name, V, edges in hand_graphs():
         e = np.array(edges, dtype=np.int64)
         csr = eb.Csr.from_edges(e[:, 0], e[:, 1], V)
-        with _graph(eb, csr, policy=policy, loop=loop) as g:
+        with _graph(eb, csr, policy=policy, loop=loop, narrow_max_frontier=narrow) as g:
             for s in range(V):
                 _check(eb, orc, csr, g, s)
 
 
+@pytest.mark.parametrize("narrow", [8192, 0])
 @pytest.mark.parametrize("policy", POLICIES)
-def test_tier_graph_every_tier_and_many_levels(eb, orc, policy):
+def test_tier_graph_every_tier_and_many_levels(eb, orc, policy, narrow):
     V, s, d = tier_graph()
     csr = eb.Csr.from_edges(s, d, V)
-    with _graph(eb, csr, policy=policy) as g:
+    with _graph(eb, csr, policy=policy, narrow_max_frontier=narrow) as g:
         for src in [0, 1, 3000, 3041, 4999, 5999, 5500]:
             _check(eb, orc, csr, g, src)
 
@@ -67,7 +71,7 @@ def test_tier_graph_every_tier_and_many_levels(eb, orc, policy):
 ])
 def test_option_variants(eb, orc, opts):
     csr = eb.Csr.rmat(13, 16, seed=21)
-    with _graph(eb, csr, **opts) as g:
+    with _graph(eb, csr, narrow_max_frontier=0, **opts) as g:
         for src in eb.pick_sources(csr.beg_pos, 4, 6):
             _check(eb, orc, csr, g, src)
 
