@@ -57,8 +57,9 @@ constexpr int IPT = 4;           // items per thread in an inspector tile
 constexpr int TILE = BT * IPT;   // items per inspector tile
 constexpr int KS = 4;            // look-back status words per tile
 constexpr int TD = 0, BU = 1;
-constexpr int NT = 1024;         // threads per CTA of the small-frontier kernel
-constexpr int NWARP = NT / 32;
+constexpr int NWE = 16;          // expansion warps per CTA of the small-frontier kernel
+constexpr int NT = 32 * (NWE + 1);  // ... plus one coordinator warp
+constexpr int NROUND = 4;        // rounds of 32 edges a warp keeps in flight together
 constexpr int NC_MAX = 16;       // CTAs per cluster, at most
 constexpr int NQCAP = 4096;      // small-frontier entries per CTA and buffer
 constexpr uint32_t NF_HEAVY = 1, NF_SPILL = 2;
@@ -702,6 +703,15 @@ __device__ __forceinline__ int4 nentry(int v, int d, int64_t st) {
   return make_int4(v, d, (int)(uint32_t)st, (int)(uint32_t)((uint64_t)st >> 32));
 }
 
+__device__ __forceinline__ void cluster_arrive_relaxed() {
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.aligned;" ::: "memory"); }
+__device__ __forceinline__ void fence_cluster() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
+// Named CTA barrier 1 between the expansion warps (arrive) and the coordinator (sync).
+__device__ __forceinline__ void bar1_arrive() { asm volatile("bar.arrive 1, %0;" ::"r"(NT) : "memory"); }
+__device__ __forceinline__ void bar1_sync() { asm volatile("bar.sync 1, %0;" ::"r"(NT) : "memory"); }
+
 struct NarrowOut {
   int4* q;                   // this CTA's next-frontier buffer
   uint32_t* cnt;             // its append counter (may pass NQCAP: the rest spills)
@@ -710,27 +720,9 @@ struct NarrowOut {
   int32_t* spill;            // global overflow list
 };
 
-// Claims v for depth ln. The row of a claimed vertex is read in the shadow of
-// the claim (the offsets load is issued before the atomic's result is needed).
-__device__ __forceinline__ void narrow_visit(const LevelArgs& a, BfsCtl* c, int v, int u, bool valid, int ln,
-                                             int32_t* depth, int32_t* parent, const NarrowOut& o) {
-  bool mine = false;
-  int vd = 0;
-  int64_t vst = 0;
-  if (valid) {
-    const uint32_t w = (uint32_t)v >> 5, b = 1u << (v & 31);
-    if (!(ld_cg(a.vis + w) & b)) {
-      const int64_t o0 = __ldg(a.off + v), o1 = __ldg(a.off + v + 1);
-      const uint32_t old = atomicOr(a.vis + w, b);
-      if (!(old & b)) {
-        mine = true;
-        vst = o0;
-        vd = (int)(o1 - o0);
-        depth[v] = ln;
-        if (parent) parent[v] = u;
-      }
-    }
-  }
+// Appends the vertices this warp claimed (mine) to the CTA's next frontier.
+__device__ __forceinline__ void narrow_append(const LevelArgs& a, BfsCtl* c, bool mine, int v, int vd, int64_t vst,
+                                              const NarrowOut& o) {
   const unsigned m = __ballot_sync(FULL, mine);
   if (!m) return;
   const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
@@ -749,6 +741,7 @@ __device__ __forceinline__ void narrow_visit(const LevelArgs& a, BfsCtl* c, int 
       o.q[pos] = nentry(v, vd, vst);
     } else {
       o.spill[atomicAdd(&c->n_spill, 1u)] = v;
+      __threadfence();  // read by other CTAs after the (relaxed) cluster barrier
       atomicOr(o.flag, NF_SPILL);
     }
   }
@@ -762,20 +755,40 @@ __device__ __forceinline__ void narrow_visit(const LevelArgs& a, BfsCtl* c, int 
 //    raw[0, n_raw) with its bits in fb[Lx & 1], and `skip` set so that the
 //    expander of the next loop iteration does nothing and the inspector
 //    classifies raw as usual.
-// Every CTA takes the same decisions from the same cluster-wide counts, so all
-// reach the same cluster barriers; there are no spin waits.
+//
+// A CTA is NWE expansion warps plus one coordinator warp. Per level:
+//  * every warp reads the cluster-wide counts of the frontier from its own
+//    shared memory (lane r: CTA r's count) and takes the same exit decision;
+//  * expansion warp gw takes k consecutive entries of the cluster-wide
+//    frontier (CTA r's entries follow those of CTAs < r; read through
+//    distributed shared memory) and walks their concatenated rows, up to
+//    NROUND rounds of 32 edges with all loads and claims in flight together.
+//    The claim is an atomicOr on the visited bitmap without a probe first,
+//    with the claimed vertex's row read beside it, so a level costs one
+//    adjacency read and one claim on its critical path;
+//  * expansion warps signal the coordinator (named barrier, no wait) and
+//    arrive at the cluster barrier relaxed: their global stores (depths) are
+//    only read after the kernel, so they never wait for them to drain;
+//  * the coordinator pushes its CTA's counts into every CTA's r_* arrays
+//    (double-buffered by level parity: a slow CTA may still use the previous
+//    level's while a fast one pushes the next), fences at cluster scope
+//    (releasing those and, through the named barrier, the expansion warps'
+//    shared-memory entries) and arrives.
+// Every CTA takes the same decisions from the same counts, so all reach the
+// same barriers; there are no spin waits.
 __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
   extern __shared__ int4 s_q[];  // [2][NQCAP]
   __shared__ uint32_t s_cnt[2], s_flag[2];
   __shared__ unsigned long long s_m[2];
-  __shared__ uint32_t r_cnt[NC_MAX], r_flag[NC_MAX];
-  __shared__ unsigned long long r_m[NC_MAX];
+  __shared__ uint32_t r_cnt[2][NC_MAX], r_flag[2][NC_MAX];
+  __shared__ unsigned long long r_m[2][NC_MAX];
   cg::cluster_group cl = cg::this_cluster();
   BfsCtl* c = a.ctl;
   if (c->done || !c->narrow) return;  // same value in every CTA
   const int nc = (int)cl.num_blocks(), rank = (int)cl.block_rank();
-  const int tid = threadIdx.x, lane = tid & 31;
-  const int gw = rank * NWARP + (tid >> 5), nwt = nc * NWARP;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool coord = warp == NWE;
+  const int gw = rank * NWE + warp, nwt = nc * NWE;
   int32_t* depth = c->depth;
   int32_t* parent = c->parent;
   const int L0 = c->level;
@@ -798,10 +811,16 @@ __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
     // the hub table of frontier L0 would be stale for a later bottom-up level
     if (a.hub_slots)
       for (int i = rank * NT + tid; i < a.hub_slots; i += nc * NT) a.hub[L0 & 1][i] = 0;
+    // every CTA knows every slice size: no push needed for frontier L0
+    if (tid < nc) {
+      r_cnt[0][tid] = (uint32_t)((int64_t)N0 * (tid + 1) / nc - (int64_t)N0 * tid / nc);
+      r_m[0][tid] = 0;
+      r_flag[0][tid] = 0;
+    }
     if (tid == 0) {
-      s_cnt[0] = (uint32_t)(hi - lo);
-      s_m[0] = 0;
-      s_flag[0] = 0;
+      s_cnt[1] = 0;
+      s_m[1] = 0;
+      s_flag[1] = 0;
     }
   }
   cl.sync();
@@ -813,26 +832,18 @@ __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
   uint32_t n_all = 0;
   for (int it = 0;; ++it) {
     const int cur = it & 1, nxt = cur ^ 1;
-    // Counts of frontier L from every CTA of the cluster.
-    if (tid < nc) {
-      r_cnt[tid] = *cl.map_shared_rank(&s_cnt[cur], tid);
-      r_m[tid] = *cl.map_shared_rank(&s_m[cur], tid);
-      r_flag[tid] = *cl.map_shared_rank(&s_flag[cur], tid);
+    // Counts of frontier L: lane r holds CTA r's; `incl` is their inclusive
+    // prefix, i.e. the end of CTA r's entries in the cluster-wide order.
+    uint32_t incl = lane < nc ? r_cnt[cur][lane] : 0u;
+    unsigned long long m_all = lane < nc ? r_m[cur][lane] : 0ull;
+    const uint32_t flags = __reduce_or_sync(FULL, lane < nc ? r_flag[cur][lane] : 0u);
+#pragma unroll
+    for (int ofs = 1; ofs < 32; ofs <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, incl, ofs);
+      if (lane >= ofs) incl += y;
+      m_all += __shfl_xor_sync(FULL, m_all, ofs);
     }
-    if (tid == 0) {  // buffer nxt was last read before the previous cluster barrier
-      s_cnt[nxt] = 0;
-      s_m[nxt] = 0;
-      s_flag[nxt] = 0;
-    }
-    __syncthreads();
-    n_all = 0;
-    uint32_t flags = 0;
-    unsigned long long m_all = 0;
-    for (int r = 0; r < nc; ++r) {
-      n_all += r_cnt[r];
-      m_all += r_m[r];
-      flags |= r_flag[r];
-    }
+    n_all = __shfl_sync(FULL, incl, 31);
     if (n_all == 0) outcome = 1;
     else if (it > 0 && (flags || n_all > (uint32_t)a.exit_f || (int64_t)m_all > a.exit_m)) outcome = 2;
     else if (L + 1 >= a.max_levels) outcome = 3;
@@ -844,57 +855,109 @@ __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
       mf_last = (int64_t)m_all;
     }
 
-    // Expand level L: warp gw takes k consecutive entries of the cluster-wide
-    // frontier (entries of CTA r follow those of CTAs < r) and walks their
-    // concatenated rows 32 edges at a time.
-    const NarrowOut o{s_q + nxt * NQCAP, &s_cnt[nxt], &s_m[nxt], &s_flag[nxt], spill};
-    const int ln = L + 1;
-    int k = (int)((n_all + nwt - 1) / nwt);
-    if (k > 32) k = 32;
-    for (int first = gw * k; first < (int)n_all; first += nwt * k) {
-      const int i = first + lane;
-      int u = -1, d = 0;
-      int64_t st = 0;
-      if (lane < k && i < (int)n_all) {
-        int r = 0, base = 0;
-        while (r < nc - 1 && i >= base + (int)r_cnt[r]) {
-          base += (int)r_cnt[r];
-          ++r;
-        }
-        const int4 e = *(cl.map_shared_rank(s_q + cur * NQCAP, r) + (i - base));
-        u = e.x;
-        d = e.y;
-        st = (int64_t)(((uint64_t)(uint32_t)e.w << 32) | (uint32_t)e.z);
-      }
-      int incl = d;
+    if (!coord) {
+      const NarrowOut o{s_q + nxt * NQCAP, &s_cnt[nxt], &s_m[nxt], &s_flag[nxt], spill};
+      const int ln = L + 1;
+      int k = (int)((n_all + nwt - 1) / nwt);
+      if (k > 32) k = 32;
+      for (int first = gw * k; first < (int)n_all; first += nwt * k) {
+        const int i = first + lane;
+        // owner CTA of entry i: the number of CTAs whose entries end at or before i
+        int r = 0;
 #pragma unroll
-      for (int ofs = 1; ofs < 32; ofs <<= 1) {
-        const int y = __shfl_up_sync(FULL, incl, ofs);
-        if (lane >= ofs) incl += y;
-      }
-      const int total = __shfl_sync(FULL, incl, 31);
-      const int excl = incl - d;
-      for (int rr = 0; rr < total; rr += 32) {
-        const int kk = rr + lane;
-        const bool valid = kk < total;
-        int j = 0;
-#pragma unroll
-        for (int step = 16; step > 0; step >>= 1) {
-          const int cand = j + step;
-          const int ev = __shfl_sync(FULL, excl, cand & 31);
-          if (cand < 32 && ev <= kk) j = cand;
+        for (int step = NC_MAX / 2; step > 0; step >>= 1) {
+          const uint32_t e_end = __shfl_sync(FULL, incl, r + step - 1);
+          if (r + step <= nc - 1 && (uint32_t)i >= e_end) r += step;
         }
-        const int64_t sj = __shfl_sync(FULL, st, j);
-        const int ej = __shfl_sync(FULL, excl, j);
-        const int uj = __shfl_sync(FULL, u, j);
-        const int v = valid ? __ldg(a.adj + sj + (kk - ej)) : 0;
-        narrow_visit(a, c, v, uj, valid, ln, depth, parent, o);
+        const uint32_t base = __shfl_sync(FULL, incl, (r + 31) & 31);  // end of CTA r-1 (unused for r = 0)
+        int u = -1, d = 0;
+        int64_t st = 0;
+        if (lane < k && i < (int)n_all) {
+          const int4 e = *(cl.map_shared_rank(s_q + cur * NQCAP, r) + (i - (r ? (int)base : 0)));
+          u = e.x;
+          d = e.y;
+          st = (int64_t)(((uint64_t)(uint32_t)e.w << 32) | (uint32_t)e.z);
+        }
+        int dincl = d;
+#pragma unroll
+        for (int ofs = 1; ofs < 32; ofs <<= 1) {
+          const int y = __shfl_up_sync(FULL, dincl, ofs);
+          if (lane >= ofs) dincl += y;
+        }
+        const int total = __shfl_sync(FULL, dincl, 31);
+        const int excl = dincl - d;
+        for (int r0 = 0; r0 < total; r0 += 32 * NROUND) {
+          int v[NROUND], uj[NROUND], vd[NROUND];
+          int64_t vst[NROUND];
+          bool mine[NROUND];
+          // adjacency reads of up to NROUND rounds
+#pragma unroll
+          for (int q = 0; q < NROUND; ++q) {
+            v[q] = -1;
+            uj[q] = 0;
+            if (r0 + 32 * q < total) {  // warp-uniform
+              const int kk = r0 + 32 * q + lane;
+              int j = 0;
+#pragma unroll
+              for (int step = 16; step > 0; step >>= 1) {
+                const int cand = j + step;
+                const int ev = __shfl_sync(FULL, excl, cand & 31);
+                if (cand < 32 && ev <= kk) j = cand;
+              }
+              const int64_t sj = __shfl_sync(FULL, st, j);
+              const int ej = __shfl_sync(FULL, excl, j);
+              uj[q] = __shfl_sync(FULL, u, j);
+              if (kk < total) v[q] = __ldg(a.adj + sj + (kk - ej));
+            }
+          }
+          // claims, with each candidate's row read beside its claim
+#pragma unroll
+          for (int q = 0; q < NROUND; ++q) {
+            mine[q] = false;
+            vd[q] = 0;
+            vst[q] = 0;
+            if (v[q] >= 0) {
+              const int x = v[q];
+              const int64_t o0 = __ldg(a.off + x), o1 = __ldg(a.off + x + 1);
+              const uint32_t b = 1u << (x & 31);
+              const uint32_t old = atomicOr(a.vis + ((uint32_t)x >> 5), b);
+              if (!(old & b)) {
+                mine[q] = true;
+                vst[q] = o0;
+                vd[q] = (int)(o1 - o0);
+                depth[x] = ln;
+                if (parent) parent[x] = uj[q];
+              }
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < NROUND; ++q)
+            if (r0 + 32 * q < total) narrow_append(a, c, mine[q], v[q], vd[q], vst[q], o);
+        }
       }
+      bar1_arrive();  // this warp's appends are complete
+      cluster_arrive_relaxed();
+      cluster_wait();
+    } else {
+      bar1_sync();  // all expansion warps' appends to buffer nxt are complete
+      if (lane < nc) {
+        *cl.map_shared_rank(&r_cnt[nxt][rank], lane) = s_cnt[nxt];
+        *cl.map_shared_rank(&r_m[nxt][rank], lane) = s_m[nxt];
+        *cl.map_shared_rank(&r_flag[nxt][rank], lane) = s_flag[nxt];
+      }
+      __syncwarp();
+      if (lane == 0) {  // buffer cur takes the appends of the next level
+        s_cnt[cur] = 0;
+        s_m[cur] = 0;
+        s_flag[cur] = 0;
+      }
+      fence_cluster();
+      cluster_arrive_relaxed();
+      cluster_wait();
     }
-    cl.sync();
     ++L;
   }
-  cl.sync();  // no CTA leaves while another may still read its counters
+  cl.sync();  // no CTA leaves while another may still read its entries
 
   const int cur = (L - L0) & 1;
   if (outcome == 2) {
@@ -902,12 +965,12 @@ __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
     // spilled ones after all stored entries; set their frontier bits.
     uint32_t base = 0, n_stored = 0;
     for (int r = 0; r < nc; ++r) {
-      const uint32_t sr = min(r_cnt[r], (uint32_t)NQCAP);
+      const uint32_t sr = min(r_cnt[cur][r], (uint32_t)NQCAP);
       if (r < rank) base += sr;
       n_stored += sr;
     }
     uint32_t* fbn = a.fb[L & 1];
-    const uint32_t mine = min(r_cnt[rank], (uint32_t)NQCAP);
+    const uint32_t mine = min(r_cnt[cur][rank], (uint32_t)NQCAP);
     for (uint32_t j = tid; j < mine; j += NT) {
       const int v = s_q[cur * NQCAP + j].x;
       a.raw[base + j] = v;
