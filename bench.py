@@ -401,6 +401,7 @@ def run_serving(args):
     which = rng.integers(0, len(graphs), n_q)
     pick = rng.integers(0, 512, n_q)
     lat, qwait, edges, done = [], [], 0, 0
+    lat_cls = {"rmat": [], "grid": []}
     sample_every = max(1, n_q // 40)
     checks, bad_status, mismatches = 0, 0, []
     graph_of = {}
@@ -419,6 +420,7 @@ def run_serving(args):
                 qwait.append(r["queue_ms"])
                 edges += r["traversed_edges"]
                 gi, src, sample = graph_of.pop(r["query_id"])
+                lat_cls["grid" if gi >= len(rmat_scales) else "rmat"].append(r["latency_ms"])
                 if r["status"] != 0:
                     bad_status += 1
                 if sample and r["status"] == 0:
@@ -449,7 +451,12 @@ def run_serving(args):
             "batches": c["batches"], "mean_batch": round(c["launched"] / max(1, c["batches"]), 2),
             "max_batch_seen": c["max_batch_seen"], "samples_checked": checks,
             "sampled_exact": not mismatches and bad_status == 0, "bad_status": bad_status,
-            "mismatches": mismatches[:5], "max_batch": args.serve_batch, "slots_per_graph": args.serve_slots}
+            "mismatches": mismatches[:5], "max_batch": args.serve_batch, "slots_per_graph": args.serve_slots,
+            "single_source_graphs": c["single_graphs"],
+            "by_class": {k: {"queries": len(v),
+                             "p50_ms": round(float(np.percentile(v, 50)), 3) if v else None,
+                             "p99_ms": round(float(np.percentile(v, 99)), 3) if v else None}
+                         for k, v in lat_cls.items()}}
 
 
 def cpu_baseline(beg, csr, srcs, args, g, depth):

@@ -1,4 +1,4 @@
-// Internal interface of the batched traversal used by the serving loop.
+// Internal interface of the traversals used by the serving loop.
 #pragma once
 #include <cuda_runtime.h>
 #include "dev_graph.h"
@@ -15,4 +15,12 @@ int stage_request(ent_graph* g, BatchWorkspace* w, const int32_t* src, int32_t n
                   cudaStream_t s, const int32_t* row_map_dev);
 int batch_source_stats(BatchWorkspace* w, int32_t n_src, cudaStream_t s, ent_stats* stats);
 int batch_max_sources(const BatchWorkspace* w);
+
+// Single-source traversal state with its own instantiated CUDA graph
+// (independent of the graph's own workspace, so several run concurrently).
+int create_bfs_workspace(ent_graph* g, BfsWorkspace** out);
+// Launches one traversal from src writing depth_dev (V int32) on stream s; async.
+int launch_bfs_single(BfsWorkspace* w, int32_t src, int32_t* depth_dev, cudaStream_t s);
+// Statistics of w's last traversal once it finished (copies on s, synchronises).
+int bfs_single_stats(BfsWorkspace* w, cudaStream_t s, ent_stats* stats);
 }  // namespace ent

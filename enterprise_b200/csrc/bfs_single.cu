@@ -1162,7 +1162,7 @@ static int pick_narrow_cluster(int limit, size_t smem) {
   return 0;
 }
 
-static int create_workspace(ent_graph* g, BfsWorkspace** out) {
+static int create_workspace(ent_graph* g, BfsWorkspace** out, bool force_graph = false) {
   BfsWorkspace* w = new BfsWorkspace();
   w->device = g->device;
   w->V = g->V;
@@ -1246,13 +1246,15 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out) {
     a.exit_m = 2 * (int64_t)o.narrow_max_edges;
     a.narrow_deg = o.narrow_max_degree;
   }
-  if (o.loop == ENT_LOOP_GRAPH) {
+  if (o.loop == ENT_LOOP_GRAPH || force_graph) {
     int rc = build_graph(g, w);
     if (rc != ENT_OK) { destroy_bfs_workspace(w); return rc; }
   }
   *out = w;
   return ENT_OK;
 }
+
+int create_bfs_workspace(ent_graph* g, BfsWorkspace** out) { return create_workspace(g, out, true); }
 
 static void fill_stats(const BfsCtl& h, float ms, ent_stats* stats) {
   stats->reached_vertices = h.n_vis;
@@ -1266,6 +1268,40 @@ static void fill_stats(const BfsCtl& h, float ms, ent_stats* stats) {
   stats->launches = 2 + 2 * h.iters + h.narrow_runs;
 }
 
+// One launch of the workspace's instantiated traversal graph on stream s.
+static int launch_graph(BfsWorkspace* w, int32_t src, int32_t* depth, int32_t* parent, cudaStream_t s) {
+  LevelArgs ra = w->args;
+  ra.use_cond = 0;
+  void* rargs[4] = {&ra, &src, &depth, &parent};
+  cudaKernelNodeParams kp = {};
+  kp.func = (void*)k_reset;
+  kp.gridDim = dim3(w->grid_reset);
+  kp.blockDim = dim3(BT);
+  kp.sharedMemBytes = 0;
+  kp.kernelParams = rargs;
+  ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec, w->reset_node, &kp));
+  kp.func = (void*)k_init;
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(32);
+  ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec, w->init_node, &kp));
+  ENT_CUDA(cudaGraphLaunch(w->exec, s));
+  return ENT_OK;
+}
+
+int launch_bfs_single(BfsWorkspace* w, int32_t src, int32_t* depth_dev, cudaStream_t s) {
+  g_kernel_launches += 2;  // reset + init; the level kernels are counted by bfs_single_stats
+  return launch_graph(w, src, depth_dev, nullptr, s);
+}
+
+int bfs_single_stats(BfsWorkspace* w, cudaStream_t s, ent_stats* stats) {
+  ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));
+  ENT_CUDA(cudaStreamSynchronize(s));
+  fill_stats(*w->ctl_h, 0.f, stats);
+  g_kernel_launches += stats->launches - 2;
+  if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "device traversal reported error flags 0x%x", w->ctl_h->err);
+  return ENT_OK;
+}
+
 int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, cudaStream_t stream, ent_stats* stats) {
   if (!g->ws) {
     int rc = create_workspace(g, &g->ws);
@@ -1275,21 +1311,8 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, c
   cudaStream_t s = stream ? stream : g->stream;
   if (stats) ENT_CUDA(cudaEventRecord(w->ev0, s));
   if (g->opts.loop == ENT_LOOP_GRAPH) {
-    LevelArgs ra = w->args;
-    ra.use_cond = 0;
-    void* rargs[4] = {&ra, &src, &depth, &parent};
-    cudaKernelNodeParams kp = {};
-    kp.func = (void*)k_reset;
-    kp.gridDim = dim3(w->grid_reset);
-    kp.blockDim = dim3(BT);
-    kp.sharedMemBytes = 0;
-    kp.kernelParams = rargs;
-    ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec, w->reset_node, &kp));
-    kp.func = (void*)k_init;
-    kp.gridDim = dim3(1);
-    kp.blockDim = dim3(32);
-    ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec, w->init_node, &kp));
-    ENT_CUDA(cudaGraphLaunch(w->exec, s));
+    int rc = launch_graph(w, src, depth, parent, s);
+    if (rc != ENT_OK) return rc;
   } else {
     LevelArgs la = w->args;
     la.use_cond = 0;

@@ -16,6 +16,15 @@
 //    launches the slot's graph on its stream. Queries that arrive while other
 //    batches run join the next batch as soon as a slot and rows free up, and
 //    batches of different graphs and slots overlap on the device.
+//  * High-diameter graphs are served one source per launch: a probe
+//    traversal at creation measures the graph's depth, and a graph at least
+//    single_source_levels deep gets single_slots single-source slots instead
+//    (each a single-source workspace with its own instantiated CUDA graph,
+//    stream and event). A bitwise batch on such a graph would hold every one
+//    of its queries for thousands of levels of grid-wide launches; a
+//    single-source traversal runs its small frontiers inside one
+//    thread-block cluster, so several queries proceed side by side on
+//    different SMs and each finishes as soon as its own traversal does.
 //  * Latency = submit to the scheduler observing completion (poll granularity
 //    tens of microseconds); queue time = submit to launch.
 #include <algorithm>
@@ -45,7 +54,8 @@ struct Query {
 };
 
 struct Slot {
-  ent::BatchWorkspace* ws = nullptr;
+  ent::BatchWorkspace* ws = nullptr;   // batched slot
+  ent::BfsWorkspace* sws = nullptr;    // single-source slot
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t stream = nullptr;
@@ -63,6 +73,8 @@ struct GraphState {
   std::vector<int32_t> free_rows;
   std::deque<int64_t> pending;
   std::vector<Slot> slots;
+  bool single = false;       // served one source per launch
+  int32_t probe_levels = 0;  // depth of the probe traversal
 };
 
 }  // namespace
@@ -97,6 +109,7 @@ void free_server(ent_server* s) {
       if (sl.exec) cudaGraphExecDestroy(sl.exec);
       if (sl.graph) cudaGraphDestroy(sl.graph);
       if (sl.ws) destroy_batch_workspace(sl.ws);
+      if (sl.sws) destroy_bfs_workspace(sl.sws);
       if (sl.row_map_dev) cudaFree(sl.row_map_dev);
       if (sl.done) cudaEventDestroy(sl.done);
       if (sl.stream) cudaStreamDestroy(sl.stream);
@@ -116,8 +129,9 @@ bool retire(ent_server* s) {
       if (q == cudaErrorNotReady) continue;
       const Clock::time_point now = Clock::now();
       std::vector<ent_stats> st(sl.qids.size());
-      int rc = q == cudaSuccess ? batch_source_stats(sl.ws, (int32_t)sl.qids.size(), sl.stream, st.data())
-                                : fail(ENT_ERR_CUDA, "batch failed: %s", cudaGetErrorString(q));
+      int rc = q != cudaSuccess ? fail(ENT_ERR_CUDA, "batch failed: %s", cudaGetErrorString(q))
+               : sl.sws         ? bfs_single_stats(sl.sws, sl.stream, st.data())
+                                : batch_source_stats(sl.ws, (int32_t)sl.qids.size(), sl.stream, st.data());
       std::lock_guard<std::mutex> lk(s->mu);
       for (size_t i = 0; i < sl.qids.size(); ++i) {
         auto it = s->queries.find(sl.qids[i]);
@@ -153,7 +167,7 @@ bool launch(ent_server* s) {
       {
         std::lock_guard<std::mutex> lk(s->mu);
         if (g.pending.empty() || g.free_rows.empty()) break;
-        const int cap = batch_max_sources(sl.ws);
+        const int cap = sl.sws ? 1 : batch_max_sources(sl.ws);
         const int take = (int)std::min<size_t>({(size_t)s->opts.max_batch, (size_t)cap, g.pending.size(),
                                                 g.free_rows.size()});
         const Clock::time_point now = Clock::now();
@@ -174,11 +188,16 @@ bool launch(ent_server* s) {
         if (take > s->ctr.max_batch_seen) s->ctr.max_batch_seen = take;
       }
       const int n = (int)src.size();
-      cudaError_t e = cudaMemcpyAsync(sl.row_map_dev, rows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice,
-                                      sl.stream);
-      int rc = e == cudaSuccess ? stage_request(g.g, sl.ws, src.data(), n, g.pool, sl.stream, sl.row_map_dev)
-                                : fail(ENT_ERR_CUDA, "row map upload failed");
-      if (rc == ENT_OK) e = cudaGraphLaunch(sl.exec, sl.stream);
+      cudaError_t e = cudaSuccess;
+      int rc = ENT_OK;
+      if (sl.sws) {
+        rc = launch_bfs_single(sl.sws, src[0], g.pool + (size_t)rows[0] * g.V, sl.stream);
+      } else {
+        e = cudaMemcpyAsync(sl.row_map_dev, rows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, sl.stream);
+        rc = e == cudaSuccess ? stage_request(g.g, sl.ws, src.data(), n, g.pool, sl.stream, sl.row_map_dev)
+                              : fail(ENT_ERR_CUDA, "row map upload failed");
+        if (rc == ENT_OK) e = cudaGraphLaunch(sl.exec, sl.stream);
+      }
       if (rc == ENT_OK && e == cudaSuccess) e = cudaEventRecord(sl.done, sl.stream);
       if (rc != ENT_OK || e != cudaSuccess) {
         // the batch never ran: complete its queries with the error status
@@ -228,6 +247,27 @@ void ent_server_opts_default(ent_server_opts* o) {
   o->rows_per_graph = 0;
   o->max_pending = 1 << 20;
   o->hbm_budget_bytes = 0;
+  o->single_source_levels = 64;
+  o->single_slots = 8;
+}
+
+// Depth of one traversal of g from its first non-isolated vertex (0 if the
+// first 4096 vertices are all isolated); scratch is a depth row of the pool.
+static int probe_depth(ent_graph* g, int32_t* scratch, int32_t* levels) {
+  *levels = 0;
+  const int64_t n = std::min<int64_t>(g->V, 4096);
+  std::vector<int64_t> off(n + 1);
+  std::lock_guard<std::mutex> lk(g->mu);
+  ENT_CUDA(cudaMemcpyAsync(off.data(), g->off, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost, g->stream));
+  ENT_CUDA(cudaStreamSynchronize(g->stream));
+  int32_t src = -1;
+  for (int64_t v = 0; v < n && src < 0; ++v)
+    if (off[v + 1] > off[v]) src = (int32_t)v;
+  if (src < 0) return ENT_OK;
+  ent_stats st{};
+  int rc = run_bfs_single(g, src, scratch, nullptr, g->stream, &st);
+  if (rc == ENT_OK) *levels = st.levels;
+  return rc;
 }
 
 int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_server_opts* opts, ent_server** out) {
@@ -240,6 +280,8 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
   if (o.max_batch < 1 || o.max_batch > 2048) return fail(ENT_ERR_INVALID_ARG, "max_batch must be 1..2048");
   if (o.slots_per_graph < 1 || o.slots_per_graph > 16) return fail(ENT_ERR_INVALID_ARG, "slots_per_graph must be 1..16");
   if (o.max_pending < 1) return fail(ENT_ERR_INVALID_ARG, "max_pending must be >= 1");
+  if (o.single_source_levels < 0) return fail(ENT_ERR_INVALID_ARG, "single_source_levels must be >= 0");
+  if (o.single_slots < 1 || o.single_slots > 64) return fail(ENT_ERR_INVALID_ARG, "single_slots must be 1..64");
   const int dev = graphs[0]->device;
   for (int k = 0; k < n_graphs; ++k)
     if (!graphs[k] || graphs[k]->device != dev) return fail(ENT_ERR_INVALID_ARG, "all graphs must be on one GPU");
@@ -264,6 +306,35 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
       return fail(ENT_ERR_OOM, "graph %d: depth pool of %d rows does not fit", k, g.rows);
     }
     for (int r = g.rows - 1; r >= 0; --r) g.free_rows.push_back(r);
+    if (o.single_source_levels > 0) {
+      int rc = probe_depth(g.g, g.pool, &g.probe_levels);
+      if (rc != ENT_OK) {
+        free_server(s);
+        return rc;
+      }
+      g.single = g.probe_levels >= o.single_source_levels;
+    }
+    if (g.single) {
+      s->ctr.single_graphs++;
+      g.slots.resize(o.single_slots);
+      for (Slot& sl : g.slots) {
+        int rc;
+        {
+          std::lock_guard<std::mutex> lk(g.g->mu);
+          rc = create_bfs_workspace(g.g, &sl.sws);
+        }
+        if (rc == ENT_OK) {
+          cudaError_t e2 = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
+          if (e2 == cudaSuccess) e2 = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+          if (e2 != cudaSuccess) rc = fail(ENT_ERR_CUDA, "slot setup: %s", cudaGetErrorString(e2));
+        }
+        if (rc != ENT_OK) {
+          free_server(s);
+          return rc;
+        }
+      }
+      continue;
+    }
     g.slots.resize(o.slots_per_graph);
     for (Slot& sl : g.slots) {
       int rc = create_batch_workspace(g.g, o.max_batch, &sl.ws);

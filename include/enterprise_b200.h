@@ -283,7 +283,13 @@ int ent_autotune(ent_graph* g, const int32_t* src, int32_t n_src, int32_t mode, 
  * rows_per_graph or, when 0, by hbm_budget_bytes (0 = a quarter of free HBM):
  * a query holds its row from launch until ent_server_release, so unreleased
  * results throttle admission. submit fails with ENT_ERR_ADMISSION once
- * max_pending queries wait. Results are the same depths as ent_bfs. */
+ * max_pending queries wait. Results are the same depths as ent_bfs.
+ * High-diameter graphs (grids, road-like graphs) would keep a batch on the
+ * device for thousands of levels: a graph whose probe traversal (run once at
+ * creation from its first non-isolated vertex) has at least
+ * single_source_levels levels is served one source per launch instead, by
+ * single_slots concurrent single-source traversals (each runs its small
+ * frontiers inside one thread-block cluster). */
 typedef struct ent_server ent_server;
 typedef struct ent_server_opts {
   int32_t max_batch;        /* sources per batched launch, 1..2048 (default 64) */
@@ -291,6 +297,10 @@ typedef struct ent_server_opts {
   int32_t rows_per_graph;   /* depth rows per graph, 0 = from the budget         */
   int32_t max_pending;      /* waiting queries before submit refuses             */
   int64_t hbm_budget_bytes; /* depth-row budget across graphs, 0 = free HBM / 4  */
+  int32_t single_source_levels; /* probe depth from which a graph is served one
+                                   source per launch (default 64, 0 = never)    */
+  int32_t single_slots;     /* concurrent single-source traversals per such graph,
+                               1..64 (default 8)                                 */
 } ent_server_opts;
 typedef struct ent_query_result {
   int64_t query_id;
@@ -306,7 +316,7 @@ typedef struct ent_query_result {
 typedef struct ent_server_counters {
   int64_t submitted, rejected, completed, released, batches, launched, pending, rows_total, rows_free;
   int32_t max_batch_seen;
-  int32_t pad;
+  int32_t single_graphs;    /* graphs served one source per launch */
 } ent_server_counters;
 void ent_server_opts_default(ent_server_opts* opts);
 int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_server_opts* opts,

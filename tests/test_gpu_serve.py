@@ -144,3 +144,69 @@ def test_fresh_graph_traversals_while_serving(eb, orc):
             srv.release(r["query_id"])
     for g in load:
         g.close()
+
+
+def test_deep_graphs_served_one_source_per_launch(eb, orc):
+    """A grid (hundreds of levels) gets single-source slots, an R-MAT graph
+    keeps bitwise batches; every result equals the traversal run alone."""
+    csrs = [eb.Csr.grid(150, 120, 0.1, seed=81), eb.Csr.rmat(12, 16, seed=82)]
+    graphs = [eb.Graph.from_csr(c) for c in csrs]
+    rng = np.random.default_rng(8)
+    with eb.Server(graphs, max_batch=32, slots_per_graph=2, single_slots=4) as srv:
+        assert srv.counters()["single_graphs"] == 1
+        qs = {}
+        for _ in range(120):
+            gi = int(rng.integers(2))
+            src = int(eb.pick_sources(csrs[gi].beg_pos, int(rng.integers(1 << 30)), 1)[0])
+            qs[srv.submit(gi, src)] = (gi, src)
+        for r in _drain(srv, len(qs)):
+            gi, src = qs[r["query_id"]]
+            assert (r["graph"], r["src"], r["status"]) == (gi, src, 0)
+            exp, _ = orc.bfs(csrs[gi].beg_pos, csrs[gi].csr, src)
+            np.testing.assert_array_equal(srv.depth(r["query_id"]), exp)
+            e, v = orc.report(csrs[gi].beg_pos, exp)
+            assert (r["traversed_edges"], r["reached_vertices"], r["levels"]) == (e, v, int(exp.max()) + 1)
+            srv.release(r["query_id"])
+        c = srv.counters()
+        assert c["completed"] == c["released"] == 120 and c["max_batch_seen"] > 1
+    for g in graphs:
+        g.close()
+
+
+def test_single_source_mode_off_keeps_batches(eb, orc):
+    csr = eb.Csr.grid(80, 60, 0.1, seed=83)
+    g = eb.Graph.from_csr(csr)
+    srcs = eb.pick_sources(csr.beg_pos, 5, 20)
+    with eb.Server([g], max_batch=16, slots_per_graph=1, single_source_levels=0) as srv:
+        assert srv.counters()["single_graphs"] == 0
+        ids = {srv.submit(0, int(s)): int(s) for s in srcs}
+        for r in _drain(srv, len(ids)):
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, ids[r["query_id"]])
+            np.testing.assert_array_equal(srv.depth(r["query_id"]), exp)
+            srv.release(r["query_id"])
+        assert srv.counters()["max_batch_seen"] > 1
+    g.close()
+
+
+def test_single_source_slots_admission_by_memory(eb, orc):
+    """3 depth rows on a deep graph: at most 3 queries hold rows; the rest
+    wait for releases, then complete with the same depths."""
+    csr = eb.Csr.grid(100, 100, 0.1, seed=84)
+    g = eb.Graph.from_csr(csr)
+    srcs = eb.pick_sources(csr.beg_pos, 6, 12)
+    with eb.Server([g], rows_per_graph=3, single_slots=8) as srv:
+        assert srv.counters()["single_graphs"] == 1
+        ids = {srv.submit(0, int(s)): int(s) for s in srcs}
+        got = 0
+        for _ in range(200):
+            res = srv.poll(wait_us=20000)
+            assert srv.counters()["rows_free"] >= 0
+            for r in res:
+                exp, _ = orc.bfs(csr.beg_pos, csr.csr, ids[r["query_id"]])
+                np.testing.assert_array_equal(srv.depth(r["query_id"]), exp)
+                srv.release(r["query_id"])
+                got += 1
+            if got == len(ids):
+                break
+        assert got == len(ids)
+    g.close()
