@@ -166,6 +166,7 @@ def run_ours(args, rank, world, dist):
     m_c = np.array([st.traversed_edges for st in stats], dtype=np.float64)
     n_c = np.array([st.reached_vertices for st in stats], dtype=np.float64)
     levels = np.array([st.levels for st in stats])
+    launches_per_step = int(sum(st.launches for st in stats))  # reset, init, level kernels, cluster runs
     b_alg = 4 * m_c + 8 * n_c + 4 * V  # algorithmic bytes per BFS
 
     n = len(srcs)
@@ -239,7 +240,7 @@ def run_ours(args, rank, world, dist):
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(beg, csr_h, srcs, args, g, depth)
 
-    launches = int(args.steps * np.sum(2 + 2 * levels)) * world
+    launches = args.steps * launches_per_step * world
     line = {
         "metric": METRIC,
         "value": round(value, 3),
@@ -291,6 +292,7 @@ def run_ours(args, rank, world, dist):
         del depth, flush
         torch.cuda.empty_cache()
         line["batched"] = run_batched(args)
+        line["high_diameter_and_uniform"] = run_deep(args)
         line["serving"] = run_serving(args)
     return line
 
@@ -376,6 +378,60 @@ def run_batched(args):
     for gk in graphs:
         gk.close()
     torch.cuda.empty_cache()
+    return out
+
+
+def run_deep(args):
+    """High-diameter and low-skew graphs, 32 seeded sources each: a 4096^2
+    4-neighbour grid with 10% of edges dropped (thousands of levels, tiny
+    frontiers: the small-frontier cluster kernel) and an Erdos-Renyi graph
+    with 2^24 vertices and mean degree 32. Each source's depths are compared
+    with the same traversal on the grid-wide path alone (mode off)."""
+    import torch
+    import enterprise_b200 as eb
+    out = {}
+    specs = [("grid_4096x4096", lambda: eb.Graph.grid(4096, 4096, 0.1, seed=0x6E1D4096)),
+             ("er_2^24_d32", lambda: eb.Graph.er(1 << 24, 32.0, seed=0xE12424))]
+    specs = [sp for sp in specs if sp[0].split("_")[0] in args.deep_graphs.split(",")]
+    for name, make in specs:
+        g = make()
+        if args.loop != "graph":
+            o = g.opts
+            o.loop = eb.LOOP[args.loop]
+            g.opts = o
+        srcs = eb.pick_sources(g.download().beg_pos, 0x50C0C3 + len(name), args.deep_sources)
+        V = g.vert_count
+        depth = torch.empty(V, dtype=torch.int32, device="cuda")
+        strm = torch.cuda.Stream()
+        sp = strm.cuda_stream
+        st = [g.bfs_device(int(s), depth.data_ptr(), 0, sp) for s in srcs]
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in srcs]
+        with torch.cuda.stream(strm):
+            for i, s in enumerate(srcs):
+                ev[i][0].record(strm)
+                g.bfs_device(int(s), depth.data_ptr(), 0, sp, stats=False)
+                ev[i][1].record(strm)
+        strm.synchronize()
+        ms = np.array([a.elapsed_time(b) for a, b in ev])
+        m = np.array([x.traversed_edges for x in st], dtype=np.float64)
+        lv = np.array([x.levels for x in st])
+        nl = np.array([x.narrow_levels for x in st])
+        # cross-check one source against the grid-wide path
+        on = g.bfs(int(srcs[0]))[0]
+        o = g.opts
+        o.narrow_max_frontier = 0
+        g.opts = o
+        off = g.bfs(int(srcs[0]))[0]
+        g.close()
+        out[name] = {"vertices": V, "sources": len(srcs), "ms_per_bfs_mean": round(float(ms.mean()), 3),
+                     "gteps_harmonic": round(len(m) / float(np.sum(ms * 1e-3 / m)) / 1e9, 3),
+                     "gteps_total": round(float(m.sum() / ms.sum() / 1e6), 3),
+                     "levels_mean": round(float(lv.mean()), 1),
+                     "small_frontier_levels_mean": round(float(nl.mean()), 1),
+                     "us_per_level": round(float((ms / lv).mean() * 1e3), 3),
+                     "same_depths_with_small_frontier_mode_off": bool(np.array_equal(on, off))}
+        del depth
+        torch.cuda.empty_cache()
     return out
 
 
@@ -563,7 +619,9 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--serve-slots", type=int, default=1)
-    ap.add_argument("--only", choices=["batch", "serve"], default=None,
+    ap.add_argument("--deep-graphs", default="grid,er", help="graphs of the high-diameter/uniform leg")
+    ap.add_argument("--deep-sources", type=int, default=32)
+    ap.add_argument("--only", choices=["batch", "serve", "deep"], default=None,
                     help="run only one of the extra measurements and print it")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -581,7 +639,7 @@ def main():
         dist = tdist
     try:
         if args.only:
-            line = run_batched(args) if args.only == "batch" else run_serving(args)
+            line = {"batch": run_batched, "serve": run_serving, "deep": run_deep}[args.only](args)
         elif args.impl == "reference":
             line = run_reference(args, rank, world)
         else:
