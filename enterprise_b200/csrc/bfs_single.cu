@@ -63,6 +63,7 @@ constexpr int NROUND = 4;        // rounds of 32 edges a warp keeps in flight to
 constexpr int NC_MAX = 16;       // CTAs per cluster, at most
 constexpr int NQCAP = 4096;      // small-frontier entries per CTA and buffer
 constexpr uint32_t NF_HEAVY = 1, NF_SPILL = 2;
+constexpr int BU_ILP = 4;        // bottom-up light path: neighbours checked per step
 
 // Device-resident loop state. Written only by the reset kernel's and the
 // inspector's last CTA (plus atomics on the acc_* counters and n_raw); read
@@ -103,6 +104,7 @@ struct LevelArgs {
   BfsCtl* ctl;
   const int64_t* off;
   const int32_t* adj;      // traversal order (descending neighbour degree)
+  const int32_t* lead;     // adj[off[v]] per vertex (-1: isolated)
   const int32_t* deg;
   const uint32_t* active;
   int64_t V, E;
@@ -402,19 +404,34 @@ __device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, 
     const bool todo = (todo_mask >> lane) & 1u;
     int64_t e0 = 0;
     int d = 0;
-    if (todo) {
-      e0 = a.off[v];
-      d = (int)(a.off[v + 1] - e0);
-    }
     bool found = false;
     int pu = -1;
-    if (todo && d < a.small_max) {
-      for (int k = 0; k < d; ++k) {
-        const int u = __ldg(a.adj + e0 + k);
-        if (is_front(u)) { found = true; pu = u; break; }
+    if (todo) {
+      // The lead neighbour (the highest-degree one) is the parent of most
+      // vertices found: it is read coalesced, beside the row offsets, and
+      // probed before anything else, whatever the vertex's degree.
+      const int u0 = __ldg(a.lead + v);
+      e0 = a.off[v];
+      d = (int)(a.off[v + 1] - e0);
+      if (is_front(u0)) { found = true; pu = u0; }
+    }
+    if (todo && !found && d < a.small_max) {
+      // A light vertex that keeps scanning is usually not adjacent to the
+      // frontier at all: it checks BU_ILP neighbours per step, their reads
+      // and then their frontier probes in flight together.
+      for (int k = 1; k < d && !found; k += BU_ILP) {
+        int u[BU_ILP];
+        bool f[BU_ILP];
+#pragma unroll
+        for (int i = 0; i < BU_ILP; ++i) u[i] = k + i < d ? __ldg(a.adj + e0 + k + i) : -1;
+#pragma unroll
+        for (int i = 0; i < BU_ILP; ++i) f[i] = u[i] >= 0 && is_front(u[i]);
+#pragma unroll
+        for (int i = 0; i < BU_ILP; ++i)
+          if (!found && f[i]) { found = true; pu = u[i]; }
       }
     }
-    unsigned heavy = __ballot_sync(FULL, todo && d >= a.small_max);
+    unsigned heavy = __ballot_sync(FULL, todo && !found && d >= a.small_max);
     while (heavy) {
       const int j = __ffs(heavy) - 1;
       heavy &= heavy - 1;
@@ -452,7 +469,7 @@ __device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, 
   }
 }
 
-__global__ void __launch_bounds__(BT) k_expand(LevelArgs a) {
+__global__ void __launch_bounds__(BT, 8) k_expand(LevelArgs a) {
   extern __shared__ int32_t s_hub[];
   __shared__ unsigned long long s_red[BT / 32];
   BfsCtl* c = a.ctl;
@@ -1200,6 +1217,7 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out, bool force_graph =
   a.ctl = w->ctl;
   a.off = g->off;
   a.adj = g->trav;
+  a.lead = g->lead;
   a.deg = g->deg;
   a.active = g->active;
   a.V = V;

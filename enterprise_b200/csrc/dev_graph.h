@@ -21,6 +21,9 @@ void destroy_batch_workspace(BatchWorkspace* w);
 //                     (ties by id): the traversal's adjacency. A bottom-up check
 //                     then meets the likeliest parent, a hub, first. Equal to
 //                     adj when E >= 2^31 (no re-ordering).
+//   lead int32[V]     first entry of each trav row (the highest-degree
+//                     neighbour), -1 if isolated: a bottom-up sweep reads it
+//                     coalesced instead of one random row sector per vertex.
 struct ent_graph {
   int device = 0;
   int num_sms = 0;
@@ -30,6 +33,7 @@ struct ent_graph {
   int32_t* deg = nullptr;
   uint32_t* active = nullptr;
   int32_t* trav = nullptr;
+  int32_t* lead = nullptr;
   cudaStream_t stream = nullptr;
   ent_bfs_opts opts;
   std::mutex mu;

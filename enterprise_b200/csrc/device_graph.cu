@@ -59,6 +59,14 @@ __global__ void k_keys_to_ids(const unsigned long long* __restrict__ keys, int64
     out[e] = (int32_t)(uint32_t)keys[e];
 }
 
+// lead[v] = first neighbour of v in the traversal adjacency (its
+// highest-degree neighbour), -1 for isolated vertices.
+__global__ void k_lead(const int64_t* __restrict__ off, const int32_t* __restrict__ trav, int64_t V,
+                       int32_t* __restrict__ lead) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x)
+    lead[v] = off[v + 1] > off[v] ? trav[off[v]] : -1;
+}
+
 // Builds the traversal adjacency (rows by descending neighbour degree).
 static int build_traversal_order(ent_graph* g) {
   const int64_t E = g->E, V = g->V;
@@ -111,6 +119,10 @@ int graph_finish(ent_graph* g) {
   ENT_CUDA(cudaGetLastError());
   int rc = build_traversal_order(g);
   if (rc != ENT_OK) return rc;
+  ENT_CUDA(cudaMalloc(&g->lead, sizeof(int32_t) * (g->V > 0 ? g->V : 1)));
+  k_lead<<<blocks, 256, 0, g->stream>>>(g->off, g->trav, g->V, g->lead);
+  g_kernel_launches++;
+  ENT_CUDA(cudaGetLastError());
   ENT_CUDA(cudaStreamSynchronize(g->stream));
   ent_bfs_opts_default(&g->opts);
   return ENT_OK;
@@ -123,6 +135,7 @@ static void graph_free(ent_graph* g) {
   if (g->bws) destroy_batch_workspace(g->bws);
   if (g->trav && g->trav != g->adj) cudaFree(g->trav);
   if (g->active) cudaFree(g->active);
+  if (g->lead) cudaFree(g->lead);
   if (g->off) cudaFree(g->off);
   if (g->adj) cudaFree(g->adj);
   if (g->deg) cudaFree(g->deg);
