@@ -104,7 +104,7 @@ struct LevelArgs {
   BfsCtl* ctl;
   const int64_t* off;
   const int32_t* adj;      // traversal order (descending neighbour degree)
-  const int32_t* lead;     // adj[off[v]] per vertex (-1: isolated)
+  const int4* lead;        // adj[off[v] .. off[v]+3] per vertex (-1 past the row)
   const int32_t* deg;
   const uint32_t* active;
   int64_t V, E;
@@ -406,20 +406,29 @@ __device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, 
     int d = 0;
     bool found = false;
     int pu = -1;
+    int4 ld = make_int4(-1, -1, -1, -1);
     if (todo) {
       // The lead neighbour (the highest-degree one) is the parent of most
-      // vertices found: it is read coalesced, beside the row offsets, and
-      // probed before anything else, whatever the vertex's degree.
-      const int u0 = __ldg(a.lead + v);
+      // vertices found: the first 4 neighbours are read coalesced, beside the
+      // row offsets, and the first is probed before anything else, whatever
+      // the vertex's degree.
+      ld = __ldg(a.lead + v);
       e0 = a.off[v];
       d = (int)(a.off[v + 1] - e0);
-      if (is_front(u0)) { found = true; pu = u0; }
+      if (is_front(ld.x)) { found = true; pu = ld.x; }
+    }
+    if (todo && !found && d > 1) {
+      // then the other three together
+      const bool f1 = is_front(ld.y), f2 = ld.z >= 0 && is_front(ld.z), f3 = ld.w >= 0 && is_front(ld.w);
+      if (f1) found = true, pu = ld.y;
+      else if (f2) found = true, pu = ld.z;
+      else if (f3) found = true, pu = ld.w;
     }
     if (todo && !found && d < a.small_max) {
       // A light vertex that keeps scanning is usually not adjacent to the
       // frontier at all: it checks BU_ILP neighbours per step, their reads
       // and then their frontier probes in flight together.
-      for (int k = 1; k < d && !found; k += BU_ILP) {
+      for (int k = 4; k < d && !found; k += BU_ILP) {
         int u[BU_ILP];
         bool f[BU_ILP];
 #pragma unroll

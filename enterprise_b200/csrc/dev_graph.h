@@ -21,9 +21,10 @@ void destroy_batch_workspace(BatchWorkspace* w);
 //                     (ties by id): the traversal's adjacency. A bottom-up check
 //                     then meets the likeliest parent, a hub, first. Equal to
 //                     adj when E >= 2^31 (no re-ordering).
-//   lead int32[V]     first entry of each trav row (the highest-degree
-//                     neighbour), -1 if isolated: a bottom-up sweep reads it
-//                     coalesced instead of one random row sector per vertex.
+//   lead int4[V]      first 4 entries of each trav row (the highest-degree
+//                     neighbours), -1 past the row's end: a bottom-up sweep
+//                     reads them coalesced instead of a random row sector per
+//                     vertex, and most light vertices need nothing else.
 struct ent_graph {
   int device = 0;
   int num_sms = 0;
@@ -33,7 +34,7 @@ struct ent_graph {
   int32_t* deg = nullptr;
   uint32_t* active = nullptr;
   int32_t* trav = nullptr;
-  int32_t* lead = nullptr;
+  int4* lead = nullptr;
   cudaStream_t stream = nullptr;
   ent_bfs_opts opts;
   std::mutex mu;

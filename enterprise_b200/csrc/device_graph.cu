@@ -59,12 +59,15 @@ __global__ void k_keys_to_ids(const unsigned long long* __restrict__ keys, int64
     out[e] = (int32_t)(uint32_t)keys[e];
 }
 
-// lead[v] = first neighbour of v in the traversal adjacency (its
-// highest-degree neighbour), -1 for isolated vertices.
+// lead[v] = the first 4 neighbours of v in the traversal adjacency (its
+// highest-degree ones), -1 where the row is shorter.
 __global__ void k_lead(const int64_t* __restrict__ off, const int32_t* __restrict__ trav, int64_t V,
-                       int32_t* __restrict__ lead) {
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x)
-    lead[v] = off[v + 1] > off[v] ? trav[off[v]] : -1;
+                       int4* __restrict__ lead) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < V; v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = off[v], d = off[v + 1] - b;
+    lead[v] = make_int4(d > 0 ? trav[b] : -1, d > 1 ? trav[b + 1] : -1, d > 2 ? trav[b + 2] : -1,
+                        d > 3 ? trav[b + 3] : -1);
+  }
 }
 
 // Builds the traversal adjacency (rows by descending neighbour degree).
@@ -119,7 +122,7 @@ int graph_finish(ent_graph* g) {
   ENT_CUDA(cudaGetLastError());
   int rc = build_traversal_order(g);
   if (rc != ENT_OK) return rc;
-  ENT_CUDA(cudaMalloc(&g->lead, sizeof(int32_t) * (g->V > 0 ? g->V : 1)));
+  ENT_CUDA(cudaMalloc(&g->lead, sizeof(int4) * (g->V > 0 ? g->V : 1)));
   k_lead<<<blocks, 256, 0, g->stream>>>(g->off, g->trav, g->V, g->lead);
   g_kernel_launches++;
   ENT_CUDA(cudaGetLastError());

@@ -57,7 +57,7 @@ def test_native_search_keeps_results_exact(eb, orc, mode):
     with eb.Graph.from_csr(csr) as g:
         opts, ms = tune.search(g, srcs, mode, reps=1)
         assert ms > 0
-        assert opts.small_max in (32, 64, 128, 256, 512) and opts.batch_small_max in (16, 32, 64)
+        assert opts.small_max in (16, 32, 64, 128, 256) and opts.batch_small_max in (16, 32, 64)
         assert g.opts == opts
         for s in srcs[:3]:
             exp, _ = orc.bfs(csr.beg_pos, csr.csr, int(s))
