@@ -56,6 +56,7 @@ constexpr int BT = 256;          // threads per CTA of the level kernels
 constexpr int IPT = 4;           // items per thread in an inspector tile
 constexpr int TILE = BT * IPT;   // items per inspector tile
 constexpr int KS = 4;            // look-back status words per tile
+constexpr int WPT = 8;           // bitmap words per thread when classifying a frontier bitmap (two uint4)
 constexpr int TD = 0, BU = 1;
 constexpr int NWE = 16;          // expansion warps per CTA of the small-frontier kernel
 constexpr int NT = 32 * (NWE + 1);  // ... plus one coordinator warp
@@ -610,21 +611,35 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
     for (int64_t i = gtid; i < W; i += nth) fbo[i] = 0;
     if (to_td) {
       // Hand over to TD: classify the frontier bitmap (ascending ids) into
-      // q[qcur^1]. A tile is BT words (BT*32 vertices), one word per thread.
-      const uint32_t ntiles = (uint32_t)((W + BT - 1) / BT);
+      // q[qcur^1]. A tile is BT*WPT words, WPT consecutive words per thread
+      // (the frontier is sparse here: few look-back tiles, not few words).
+      const uint32_t ntiles = (uint32_t)((W + BT * WPT - 1) / (BT * WPT));
       while (true) {
         const uint32_t tile = acquire_tile(c, &s_tile);
         if (tile >= ntiles) break;
-        const int64_t wi = (int64_t)tile * BT + threadIdx.x;
-        const uint32_t word = wi < W ? ld_cg(fbn + wi) : 0u;
+        const int64_t w_first = ((int64_t)tile * BT + threadIdx.x) * WPT;
+        uint32_t wd[WPT];
+        if (w_first + WPT <= W) {  // 32-byte aligned: the slab is 256-byte aligned, w_first % 8 == 0
+          const uint4 x = __ldcg(reinterpret_cast<const uint4*>(fbn + w_first));
+          const uint4 y = __ldcg(reinterpret_cast<const uint4*>(fbn + w_first) + 1);
+          wd[0] = x.x; wd[1] = x.y; wd[2] = x.z; wd[3] = x.w;
+          wd[4] = y.x; wd[5] = y.y; wd[6] = y.z; wd[7] = y.w;
+        } else {
+#pragma unroll
+          for (int j = 0; j < WPT; ++j) wd[j] = w_first + j < W ? ld_cg(fbn + w_first + j) : 0u;
+        }
         uint32_t cnt[4] = {0, 0, 0, 0};
-        for (uint32_t m = word; m; m &= m - 1) {
-          const int v = (int)(wi * 32 + __ffs(m) - 1);
-          const int d = a.deg[v];
-          const int cl = cls_of(d, a);
-          my_maxd = max(my_maxd, (uint32_t)d);
-          cnt[cl]++;
-          if (cl == 2) cnt[3] += n_chunks_of(d, a);
+#pragma unroll
+        for (int j = 0; j < WPT; ++j) {
+          const int64_t wi = w_first + j;
+          for (uint32_t m = wd[j]; m; m &= m - 1) {
+            const int v = (int)(wi * 32 + __ffs(m) - 1);
+            const int d = a.deg[v];
+            const int cl = cls_of(d, a);
+            my_maxd = max(my_maxd, (uint32_t)d);
+            cnt[cl]++;
+            if (cl == 2) cnt[3] += n_chunks_of(d, a);
+          }
         }
         uint32_t pre[4] = {cnt[0], cnt[1], cnt[2], cnt[3]}, agg[4], excl[4];
         block_excl_scan<4>(pre, agg, s_scan);
@@ -632,10 +647,14 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
         uint32_t pos[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) pos[k] = excl[k] + pre[k];
-        for (uint32_t m = word; m; m &= m - 1) {
-          const int v = (int)(wi * 32 + __ffs(m) - 1);
-          const int d = a.deg[v];
-          qo.put(a, v, cls_of(d, a), d, pos);
+#pragma unroll
+        for (int j = 0; j < WPT; ++j) {
+          const int64_t wi = w_first + j;
+          for (uint32_t m = wd[j]; m; m &= m - 1) {
+            const int v = (int)(wi * 32 + __ffs(m) - 1);
+            const int d = a.deg[v];
+            qo.put(a, v, cls_of(d, a), d, pos);
+          }
         }
         if (tile == ntiles - 1 && threadIdx.x == 0) {
           for (int k = 0; k < 4; ++k) c->tot[k] = excl[k] + agg[k];
