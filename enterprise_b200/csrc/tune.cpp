@@ -66,7 +66,7 @@ extern "C" int ent_autotune(ent_graph* g, const int32_t* src, int32_t n_src, int
   if (mode == 0) {
     knobs = {{"small_max", {16, 32, 64, 128, 256}, set_small}, {"large_min", {128, 256, 512, 1024, 4096}, set_large},
              {"chunk_edges", {256, 512, 1024, 2048, 8192}, set_chunk}, {"hub_slots", {0, 1024}, set_hub},
-             {"alpha", {4, 14, 32, 64}, set_alpha},    {"beta", {8, 24, 64}, set_beta},
+             {"alpha", {8, 14, 24, 48, 96}, set_alpha}, {"beta", {24, 64, 256, 1024}, set_beta},
              {"blocks_per_sm", {0, 4}, set_bps}};
   } else {
     knobs = {{"batch_alpha", {1, 2, 4, 8, 16}, set_balpha},
