@@ -400,7 +400,16 @@ def run_deep(args):
             o = g.opts
             o.loop = eb.LOOP[args.loop]
             g.opts = o
-        srcs = eb.pick_sources(g.download().beg_pos, 0x50C0C3 + len(name), args.deep_sources)
+        beg = g.download().beg_pos
+        srcs = eb.pick_sources(beg, 0x50C0C3 + len(name), args.deep_sources)
+        tuned = None
+        if name.startswith("er") and not args.no_tune:  # the grid runs in the small-frontier mode throughout
+            from enterprise_b200 import tune
+            t0 = time.time()
+            tsrc = eb.pick_sources(beg, 0x50C0C3 + len(name) + 0x7E57, 8)
+            opts, _, hit = tune.autotune(g, tsrc, "single", reps=1, label="er")
+            tuned = {"opts": {k: v for k, v in vars(opts).items() if k != "pad"}, "cached": hit,
+                     "search_s": round(time.time() - t0, 2)}
         V = g.vert_count
         depth = torch.empty(V, dtype=torch.int32, device="cuda")
         strm = torch.cuda.Stream()
@@ -430,7 +439,8 @@ def run_deep(args):
                      "levels_mean": round(float(lv.mean()), 1),
                      "small_frontier_levels_mean": round(float(nl.mean()), 1),
                      "us_per_level": round(float((ms / lv).mean() * 1e3), 3),
-                     "same_depths_with_small_frontier_mode_off": bool(np.array_equal(on, off))}
+                     "same_depths_with_small_frontier_mode_off": bool(np.array_equal(on, off)),
+                     "autotuned": tuned}
         del depth
         torch.cuda.empty_cache()
     return out

@@ -94,8 +94,8 @@ class BfsOpts:
     """Tuning knobs of one graph's traversals (mirror of ``ent_bfs_opts``)."""
     policy: int = 0
     loop: int = 0
-    alpha: float = 14.0
-    beta: float = 24.0
+    alpha: float = 24.0
+    beta: float = 256.0
     ref_ratio: float = 0.3
     small_max: int = 32
     large_min: int = 1024

@@ -318,8 +318,8 @@ void ent_bfs_opts_default(ent_bfs_opts* o) {
   if (!o) return;
   o->policy = ENT_POLICY_BEAMER;
   o->loop = ENT_LOOP_GRAPH;
-  o->alpha = 14.0;
-  o->beta = 24.0;
+  o->alpha = 24.0;  // measured on B200 (R-MAT s24 and Erdos-Renyi 2^24): Beamer's CPU values 14 / 24
+  o->beta = 256.0;  // switch to bottom-up too early and back too early here
   o->ref_ratio = 0.3;
   o->small_max = 32;
   o->large_min = 1024;

@@ -99,10 +99,11 @@ def test_hand_over_when_the_frontier_grows(eb, orc, grid):
 def test_spill_past_shared_memory(eb, orc):
     """One CTA (4096 entries per buffer) meets a hub with 9000 new neighbours:
     the rest spills to global memory and the run hands over; afterwards the
-    49 remaining paths run in the mode again."""
+    49 remaining paths run in the mode again (top-down policy: the mode only
+    takes top-down levels)."""
     V, s, d, end = broom()
     csr = eb.Csr.from_edges(s, d, V)
-    with _graph(eb, csr, narrow_cluster=1, narrow_max_frontier=2048, narrow_max_degree=1 << 20,
+    with _graph(eb, csr, policy="td", narrow_cluster=1, narrow_max_frontier=2048, narrow_max_degree=1 << 20,
                 narrow_max_edges=1 << 30) as g:
         for src in (end, 1, 0, V - 1):
             st = _check(orc, csr, g, src)
