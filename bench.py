@@ -213,7 +213,7 @@ def run_ours(args, rank, world, dist):
     amean = float(np.mean(gteps_src))
     peak, peak_kind = measured_peak()
     achieved = float(b_alg.mean() / (mean_per_src.mean() * 1e-3) / 1e9)
-    traffic = profiled_traffic("bfs_rmat_s24_traffic.txt") if args.scale == 24 else None
+    traffic = profiled_traffic("bfs_rmat_s24_traffic.txt") if args.scale == 24 else None  # bytes per traversal
 
     # ------------------------------------------------ e2e through the C ABI
     host_depth = np.empty(V, dtype=np.int32)
