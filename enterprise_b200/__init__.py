@@ -188,6 +188,7 @@ def lib() -> C.CDLL:
         "ent_graph_gen_er": (C.c_int, [C.c_int64, C.c_double, C.c_uint64, C.c_int32, C.POINTER(_P)]),
         "ent_graph_vert_count": (C.c_int64, [_P]),
         "ent_graph_edge_count": (C.c_int64, [_P]),
+        "ent_graph_device": (C.c_int32, [_P]),
         "ent_graph_download": (C.c_int, [_P, _I64P, _I32P]),
         "ent_graph_device_csr": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
         "ent_graph_set_opts": (C.c_int, [_P, C.POINTER(_Opts)]),
@@ -196,6 +197,7 @@ def lib() -> C.CDLL:
         "ent_bfs": (C.c_int, [_P, C.c_int32, _I32P, _I32P, C.POINTER(_Stats)]),
         "ent_bfs_device": (C.c_int, [_P, C.c_int32, _P, _P, _P, C.POINTER(_Stats)]),
         "ent_bfs_trace": (C.c_int, [_P, C.c_int32, C.POINTER(_Trace), C.c_int32, _I32P, C.POINTER(_Stats)]),
+        "ent_validate": (C.c_int, [_P, C.c_int32, _P, _P, _I32P, _I64P, _I32P, _I64P]),
         "ent_bfs_batch": (C.c_int, [_P, _I32P, C.c_int32, _I32P, C.POINTER(_Stats)]),
         "ent_bfs_batch_device": (C.c_int, [_P, _I32P, C.c_int32, _P, _P, C.POINTER(_Stats)]),
         "ent_bfs_multi": (C.c_int, [C.POINTER(_P), C.c_int32, _I32P, _I32P, C.POINTER(_I32P)]),
@@ -353,6 +355,7 @@ class Graph:
         L = lib()
         self.vert_count = int(L.ent_graph_vert_count(handle))
         self.edge_count = int(L.ent_graph_edge_count(handle))
+        self.device = int(L.ent_graph_device(handle))
 
     # ---------------------------------------------------------- creation --
     @staticmethod
@@ -437,6 +440,24 @@ class Graph:
         _check(lib().ent_bfs_device(self.handle, int(src), C.c_void_p(depth_ptr), C.c_void_p(parent_ptr or None),
                                     C.c_void_p(stream or None), C.byref(st) if stats else None))
         return Stats._from_c(st) if stats else None
+
+    def validate_device(self, src: int, depth_ptr: int, parent_ptr: int = 0):
+        """Graph500-style certificates of a result on the GPU (``ent_validate``):
+        ((depth rule, vertex), (parent rule, vertex) or None); rule 0 = holds."""
+        dc, pc = C.c_int32(), C.c_int32()
+        db, pb = C.c_int64(), C.c_int64()
+        _check(lib().ent_validate(self.handle, int(src), C.c_void_p(depth_ptr), C.c_void_p(parent_ptr or None),
+                                  C.byref(dc), C.byref(db), C.byref(pc), C.byref(pb)))
+        return (dc.value, db.value), ((pc.value, pb.value) if parent_ptr else None)
+
+    def validate(self, src: int, depth: np.ndarray, parent: Optional[np.ndarray] = None):
+        """validate_device on host arrays (copied to the graph's GPU with torch)."""
+        import torch
+        dev = torch.device("cuda", self.device)
+        d = torch.from_numpy(np.ascontiguousarray(depth, dtype=np.int32)).to(dev)
+        p = torch.from_numpy(np.ascontiguousarray(parent, dtype=np.int32)).to(dev) if parent is not None else None
+        torch.cuda.synchronize(dev)
+        return self.validate_device(src, d.data_ptr(), p.data_ptr() if p is not None else 0)
 
     def trace(self, src: int, max_levels: int = 100000):
         """Per-level trace (direction, frontier size/edges, kernel times) of one BFS."""

@@ -35,6 +35,7 @@ SOURCES = [
     "bfs_single.cu",
     "bfs_batch.cu",
     "bfs_noalloc.cu",
+    "bfs_validate.cu",
     "serve.cpp",
     "tune.cpp",
 ]

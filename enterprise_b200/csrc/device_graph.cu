@@ -424,6 +424,7 @@ int ent_graph_gen_er(int64_t n, double mean_degree, uint64_t seed, int32_t gpu, 
 
 int64_t ent_graph_vert_count(const ent_graph* g) { return g ? g->V : -1; }
 int64_t ent_graph_edge_count(const ent_graph* g) { return g ? g->E : -1; }
+int32_t ent_graph_device(const ent_graph* g) { return g ? g->device : -1; }
 
 int ent_graph_download(const ent_graph* g, int64_t* beg, int32_t* csr) {
   clear_error();

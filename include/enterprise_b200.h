@@ -174,6 +174,7 @@ int ent_graph_gen_er(int64_t vert_count, double mean_degree, uint64_t seed,
                      int32_t gpu_id, ent_graph** out);
 int64_t ent_graph_vert_count(const ent_graph* g);
 int64_t ent_graph_edge_count(const ent_graph* g);
+int32_t ent_graph_device(const ent_graph* g);  /* the graph's GPU */
 /* Copies the device CSR to caller host arrays (V+1 and E entries). */
 int ent_graph_download(const ent_graph* g, int64_t* beg_pos, int32_t* csr);
 /* Device pointers of the resident CSR (for callers that keep work on GPU). */
@@ -229,6 +230,21 @@ int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_l
 #define ENT_NOALLOC_MAX_VERTICES (1 << 20)
 int ent_bfs_noalloc(const int64_t* beg_pos_dev, const int32_t* csr_dev, int64_t vert_count,
                     int32_t src, int32_t* depth_dev, void* stream);
+
+/* Graph500-style validation of one traversal's result on the GPU, every
+ * vertex and edge (the reference's validate() spot-checks one random vertex,
+ * validate.h:34-103). depth_dev / parent_dev: device arrays of V int32 on the
+ * graph's GPU (parent_dev may be NULL). Depth rules, in order: -1 depth[src]
+ * != 0; per vertex v ascending: -2 depth < -1, -3 depth 0 but v != src, at the
+ * first edge of v's row that breaks one: -4 exactly one end reached, -5 both
+ * reached but depths differ by more than 1; -6 v reached at depth > 0 with no
+ * neighbour one level up. Parent rules: -1 parent[src] != src or depth[src]
+ * != 0; per v != src ascending: -2 unreached v with a parent, -3 parent out
+ * of range, -4 depth[parent] != depth[v] - 1, -5 (parent, v) not an edge.
+ * *_code = 0 when all hold, else the rule broken at the smallest offending
+ * vertex *_bad (-1 when none). Synchronous. */
+int ent_validate(ent_graph* g, int32_t src, const int32_t* depth_dev, const int32_t* parent_dev,
+                 int32_t* depth_code, int64_t* depth_bad, int32_t* parent_code, int64_t* parent_bad);
 
 /* Many sources at once with bitwise frontiers (one bit per source per vertex
  * in a shared status word). depth_out: HOST array n_src x V int32, source-major
