@@ -189,6 +189,7 @@ def lib() -> C.CDLL:
         "ent_graph_vert_count": (C.c_int64, [_P]),
         "ent_graph_edge_count": (C.c_int64, [_P]),
         "ent_graph_device": (C.c_int32, [_P]),
+        "ent_graph_from_edges": (C.c_int, [_I64P, _I64P, C.c_int64, C.c_int64, C.c_int32, C.POINTER(_P)]),
         "ent_graph_download": (C.c_int, [_P, _I64P, _I32P]),
         "ent_graph_device_csr": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
         "ent_graph_set_opts": (C.c_int, [_P, C.POINTER(_Opts)]),
@@ -368,6 +369,17 @@ class Graph:
     @staticmethod
     def from_arrays(beg_pos: np.ndarray, csr: np.ndarray, gpu: int = 0) -> "Graph":
         return Graph.from_csr(Csr(beg_pos, csr), gpu)
+
+    @staticmethod
+    def from_edges(src: Sequence[int], dst: Sequence[int], vert_count: int, gpu: int = 0) -> "Graph":
+        """Canonical undirected CSR of an edge list, built on the GPU."""
+        s = np.ascontiguousarray(src, dtype=np.int64)
+        d = np.ascontiguousarray(dst, dtype=np.int64)
+        if len(s) != len(d):
+            raise ValueError("src and dst differ in length")
+        h = _P()
+        _check(lib().ent_graph_from_edges(_i64p(s), _i64p(d), len(s), vert_count, gpu, C.byref(h)))
+        return Graph(h)
 
     @staticmethod
     def load(beg_pos_path: str, csr_path: str, gpu: int = 0) -> "Graph":

@@ -422,6 +422,70 @@ int ent_graph_gen_er(int64_t n, double mean_degree, uint64_t seed, int32_t gpu, 
   return build_on_device(d, d.ep.n_edges, n, gpu, out);
 }
 
+namespace ent {
+// A caller's edge list already on the device (endpoints checked in range).
+struct ListDraw {
+  const int64_t* src;
+  const int64_t* dst;
+  __device__ bool operator()(uint64_t i, uint64_t* u, uint64_t* v) const {
+    *u = (uint64_t)src[i];
+    *v = (uint64_t)dst[i];
+    return true;
+  }
+};
+
+__global__ void k_first_bad_edge(const int64_t* __restrict__ src, const int64_t* __restrict__ dst, int64_t n,
+                                 int64_t V, unsigned long long* first) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (src[i] < 0 || src[i] >= V || dst[i] < 0 || dst[i] >= V) atomicMin(first, (unsigned long long)i);
+}
+}  // namespace ent
+
+int ent_graph_from_edges(const int64_t* src, const int64_t* dst, int64_t n, int64_t V, int32_t gpu,
+                         ent_graph** out) {
+  clear_error();
+  if ((!src || !dst) && n > 0) return fail(ENT_ERR_INVALID_ARG, "null edge arrays");
+  if (!out || V < 1 || n < 0) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
+  if (V >= (1ll << 31) - 1) return fail(ENT_ERR_UNSUPPORTED, "V exceeds int32 ids");
+  int rc = check_gpu(gpu);
+  if (rc) return rc;
+  DeviceGuard dg(gpu);
+  int64_t *d_src = nullptr, *d_dst = nullptr;
+  unsigned long long* d_bad = nullptr;
+  unsigned long long bad = ~0ull;
+  cudaStream_t s = nullptr;
+  cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  const size_t bytes = sizeof(int64_t) * (size_t)std::max<int64_t>(n, 1);
+  if (e == cudaSuccess) e = cudaMalloc(&d_src, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&d_dst, bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&d_bad, sizeof(bad));
+  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(d_src, src, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(d_dst, dst, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_bad, &bad, sizeof(bad), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && n > 0) {
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, gpu);
+    k_first_bad_edge<<<nsm * 8, 256, 0, s>>>(d_src, d_dst, n, V, d_bad);
+    g_kernel_launches++;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    rc = fail(e == cudaErrorMemoryAllocation ? ENT_ERR_OOM : ENT_ERR_CUDA, "edge upload failed: %s",
+              cudaGetErrorString(e));
+  } else if (bad != ~0ull) {
+    rc = fail(ENT_ERR_FORMAT, "edge %lld has an endpoint outside [0,V)", (long long)bad);
+  } else {
+    rc = build_on_device(ListDraw{d_src, d_dst}, (uint64_t)n, V, gpu, out);
+  }
+  if (d_src) cudaFree(d_src);
+  if (d_dst) cudaFree(d_dst);
+  if (d_bad) cudaFree(d_bad);
+  if (s) cudaStreamDestroy(s);
+  return rc;
+}
+
 int64_t ent_graph_vert_count(const ent_graph* g) { return g ? g->V : -1; }
 int64_t ent_graph_edge_count(const ent_graph* g) { return g ? g->E : -1; }
 int32_t ent_graph_device(const ent_graph* g) { return g ? g->device : -1; }

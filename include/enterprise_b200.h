@@ -172,6 +172,14 @@ int ent_graph_gen_grid(int64_t width, int64_t height, double drop_prob, uint64_t
                        int32_t gpu_id, ent_graph** out);
 int ent_graph_gen_er(int64_t vert_count, double mean_degree, uint64_t seed,
                      int32_t gpu_id, ent_graph** out);
+/* Builds the canonical undirected CSR of a caller's edge list on the GPU:
+ * both directions, self loops and duplicates dropped, rows ascending (the
+ * same CSR as ent_csr_from_edges; the reference builds CSR offline with its
+ * text converter, tuple_text_to_binary_csr/). src/dst: HOST arrays of n_edges
+ * ids in [0, vert_count); an endpoint outside returns ENT_ERR_FORMAT naming
+ * the first such edge. */
+int ent_graph_from_edges(const int64_t* src, const int64_t* dst, int64_t n_edges, int64_t vert_count,
+                         int32_t gpu_id, ent_graph** out);
 int64_t ent_graph_vert_count(const ent_graph* g);
 int64_t ent_graph_edge_count(const ent_graph* g);
 int32_t ent_graph_device(const ent_graph* g);  /* the graph's GPU */
