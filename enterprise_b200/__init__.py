@@ -190,6 +190,7 @@ def lib() -> C.CDLL:
         "ent_graph_edge_count": (C.c_int64, [_P]),
         "ent_graph_device": (C.c_int32, [_P]),
         "ent_graph_from_edges": (C.c_int, [_I64P, _I64P, C.c_int64, C.c_int64, C.c_int32, C.POINTER(_P)]),
+        "ent_graph_load": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int32, C.POINTER(_P)]),
         "ent_graph_download": (C.c_int, [_P, _I64P, _I32P]),
         "ent_graph_device_csr": (C.c_int, [_P, C.POINTER(_P), C.POINTER(_P)]),
         "ent_graph_set_opts": (C.c_int, [_P, C.POINTER(_Opts)]),
@@ -383,7 +384,10 @@ class Graph:
 
     @staticmethod
     def load(beg_pos_path: str, csr_path: str, gpu: int = 0) -> "Graph":
-        return Graph.from_csr(Csr.load(beg_pos_path, csr_path), gpu)
+        """Reference-format files streamed straight to the GPU (``ent_graph_load``)."""
+        h = _P()
+        _check(lib().ent_graph_load(os.fsencode(beg_pos_path), os.fsencode(csr_path), gpu, C.byref(h)))
+        return Graph(h)
 
     @staticmethod
     def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,

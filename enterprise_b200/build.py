@@ -36,6 +36,7 @@ SOURCES = [
     "bfs_batch.cu",
     "bfs_noalloc.cu",
     "bfs_validate.cu",
+    "graph_ingest.cu",
     "serve.cpp",
     "tune.cpp",
 ]

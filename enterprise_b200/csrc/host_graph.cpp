@@ -163,7 +163,11 @@ int ent_csr_load(const char* beg_path, const char* csr_path, ent_csr** out) {
   size_t got = fread(g->off.data(), 8, V + 1, f);
   fclose(f);
   if ((int64_t)got != V + 1) { delete g; return fail(ENT_ERR_IO, "short read on %s", beg_path); }
-  if (g->off[0] != 0) { delete g; return fail(ENT_ERR_FORMAT, "beg_pos[0]=%lld, expected 0", (long long)g->off[0]); }
+  if (g->off[0] != 0) {
+    const long long first = (long long)g->off[0];
+    delete g;
+    return fail(ENT_ERR_FORMAT, "beg_pos[0]=%lld, expected 0", first);
+  }
   for (int64_t i = 0; i < V; ++i)
     if (g->off[i + 1] < g->off[i]) {
       int64_t a = g->off[i], b = g->off[i + 1];

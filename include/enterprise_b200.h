@@ -164,6 +164,13 @@ int ent_pick_sources_compat(const int64_t* beg_pos, int64_t vert_count, int32_t 
 int ent_graph_create(const int64_t* beg_pos, const int32_t* csr, int64_t vert_count,
                      int64_t edge_count, int32_t gpu_id, ent_graph** out);
 int ent_graph_from_csr(const ent_csr* g, int32_t gpu_id, ent_graph** out);
+/* Loads <beg_pos.bin> (int64[V+1]) and <csr.bin> (int64[E] or int32[E]) into
+ * a device graph without a host copy of the CSR: chunks of csr.bin are read
+ * by several threads into pinned buffers, copied asynchronously and narrowed
+ * to int32 on the GPU while the next chunk is read (replaces the reference's
+ * graph loader with its serial narrowing loop, graph.hpp:33-118, and its
+ * upload, allocator.cuh:107-120). Format rules and errors as ent_csr_load. */
+int ent_graph_load(const char* beg_pos_path, const char* csr_path, int32_t gpu_id, ent_graph** out);
 /* Generates a graph directly on the GPU (same edges as the host generators,
  * bit-identical CSR). */
 int ent_graph_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c,

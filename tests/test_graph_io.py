@@ -132,3 +132,16 @@ def test_pick_sources_compat_matches_glibc_rand(eb):
             continue
         exp.append(s)
     assert got.tolist() == exp
+
+
+def test_device_load_checks_format_before_any_gpu(eb, tmp_path):
+    """The streamed loader rejects malformed files with the host loader's
+    status and message before it needs a device."""
+    b, c = tmp_path / "x_beg_pos.bin", tmp_path / "x_csr.bin"
+    np.array([1, 2, 3], dtype=np.int64).tofile(b)
+    np.array([1, 0, 0], dtype=np.int64).tofile(c)
+    with pytest.raises(eb.EntError) as host:
+        eb.Csr.load(str(b), str(c))
+    with pytest.raises(eb.EntError) as dev:
+        eb.Graph.load(str(b), str(c))
+    assert (dev.value.code, str(dev.value)) == (host.value.code, str(host.value))
