@@ -61,6 +61,7 @@ struct BatchArgs {
   BatchCtl* ctl;
   const int64_t* off;
   const int32_t* adj;
+  const int4* lead;     // adj[off[v] .. off[v]+3] per vertex (-1 past the row)
   const int32_t* deg;
   const uint32_t* active;
   int64_t V, E;
@@ -393,7 +394,9 @@ __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
       unsigned long long need[WPL], acc[WPL];
       bool any_need = false;
       int64_t e0 = 0, e1 = 0;
+      int4 ld = make_int4(-1, -1, -1, -1);
       if (todo) {
+        ld = __ldg(a.lead + v);  // the row's first four neighbours, read coalesced
         const unsigned long long* xv = a.X + (size_t)v * a.W + gl * WPL;
 #pragma unroll
         for (int j = 0; j < WPL; ++j) {
@@ -407,10 +410,21 @@ __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
       // the whole group scans the row together (same trip count)
       if (todo) {
         bool cover = !(__ballot_sync(gmask, any_need) & gmask);
-        // two neighbours per step: both gathers are in flight together
+        // two neighbours per step: both gathers are in flight together; the
+        // first two steps take their ids from the lead entry instead of the row
         for (int64_t e = e0; e < e1 && !cover; e += 2) {
-          const int u0 = __ldg(a.adj + e);
-          const int u1 = e + 1 < e1 ? __ldg(a.adj + e + 1) : u0;
+          const int k = (int)(e - e0);
+          int u0, u1;
+          if (k == 0) {
+            u0 = ld.x;
+            u1 = e + 1 < e1 ? ld.y : u0;
+          } else if (k == 2) {
+            u0 = ld.z;
+            u1 = e + 1 < e1 ? ld.w : u0;
+          } else {
+            u0 = __ldg(a.adj + e);
+            u1 = e + 1 < e1 ? __ldg(a.adj + e + 1) : u0;
+          }
           unsigned long long f0[WPL], f1[WPL];
 #pragma unroll
           for (int j = 0; j < WPL; ++j) f0[j] = f1[j] = 0;
@@ -936,6 +950,7 @@ int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
   a.ctl = w->ctl;
   a.off = g->off;
   a.adj = g->trav;
+  a.lead = g->lead;
   a.deg = g->deg;
   a.active = g->active;
   a.V = V;
