@@ -680,59 +680,72 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   __syncthreads();
   if (!s_last || threadIdx.x != 0) return;
   __threadfence();
-  volatile BfsCtl* vc = c;
-  const int64_t nf_cur = vc->n_f;
-  const int64_t n_next = dir == TD ? (int64_t)vc->n_raw : (int64_t)vc->acc_n;
-  const int64_t m_next = (int64_t)vc->acc_m;
+  // Every counter the policy needs is loaded at once (independent L2 loads in
+  // flight together), the decision is made in registers, then all is stored:
+  // the finisher is on the critical path of every level.
+  const auto ld64 = [](const void* p) { return (int64_t)__ldcg(reinterpret_cast<const long long*>(p)); };
+  const int32_t n_raw = __ldcg(&c->n_raw), err0 = __ldcg(&c->err), it0 = __ldcg(&c->iters);
+  const int32_t tdl = __ldcg(&c->td_levels), bul = __ldcg(&c->bu_levels);
+  const int64_t acc_n = ld64(&c->acc_n), acc_m = ld64(&c->acc_m);
+  const int64_t n_vis0 = ld64(&c->n_vis), m_vis0 = ld64(&c->m_vis);
+  const uint32_t maxd = __ldcg(&c->acc_maxd);
+  uint32_t tot[KS];
+#pragma unroll
+  for (int k = 0; k < KS; ++k) tot[k] = __ldcg(&c->tot[k]);
+  const int64_t n_next = dir == TD ? (int64_t)n_raw : acc_n;
+  const int64_t m_next = acc_m;
   int next_dir = dir;
+  bool new_queues = false;
   if (dir == TD) {
-    vc->td_levels = vc->td_levels + 1;
-    vc->qcur = qcur ^ 1;
-    for (int k = 0; k < 3; ++k) vc->n_q[k] = (int32_t)vc->tot[k];
-    vc->n_chunks = (int32_t)vc->tot[3];
-    const double m_u = (double)(a.E - (vc->m_vis + m_next));
+    new_queues = true;
+    const double m_u = (double)(a.E - (m_vis0 + m_next));
     if (a.policy == ENT_POLICY_BEAMER && (double)m_next > m_u / a.alpha) next_dir = BU;
     if (a.policy == ENT_POLICY_REFERENCE && (double)m_next >= a.ref_ratio * (double)a.E) next_dir = BU;
     if (a.policy == ENT_POLICY_BU_ONLY) next_dir = BU;
-  } else {
-    vc->bu_levels = vc->bu_levels + 1;
-    if (to_td) {
-      next_dir = TD;
-      vc->qcur = qcur ^ 1;
-      for (int k = 0; k < 3; ++k) vc->n_q[k] = (int32_t)vc->tot[k];
-      vc->n_chunks = (int32_t)vc->tot[3];
-    }
+  } else if (to_td) {
+    next_dir = TD;
+    new_queues = true;
   }
-  vc->n_vis = vc->n_vis + n_next;
-  vc->m_vis = vc->m_vis + m_next;
-  vc->n_f = n_next;
-  vc->m_f = m_next;
-  vc->dir = next_dir;
-  vc->level = L + 1;
+  const int64_t n_vis1 = n_vis0 + n_next;
   int done = n_next == 0;
+  int err1 = err0;
   if (L + 1 >= a.max_levels && !done) {
-    vc->err = vc->err | 4;
+    err1 |= 4;
     done = 1;
   }
-  if (vc->n_vis > a.V) {  // a vertex counted twice: stop instead of looping on
-    vc->err = vc->err | 8;
+  if (n_vis1 > a.V) {  // a vertex counted twice: stop instead of looping on
+    err1 |= 8;
     done = 1;
   }
   // Small-frontier mode for the next level (top-down only).
   const int narrow = !done && next_dir == TD && a.narrow_f > 0 && n_next <= a.narrow_f &&
-                     m_next <= a.narrow_m && (int64_t)vc->acc_maxd <= a.narrow_deg;
-  vc->done = done;
-  vc->narrow = narrow;
-  vc->skip = 0;
-  vc->acc_maxd = 0;
-  vc->iters = vc->iters + 1;
-  vc->n_raw = 0;
-  vc->acc_n = 0;
-  vc->acc_m = 0;
-  for (int k = 0; k < KS; ++k) vc->tot[k] = 0;
-  vc->tile_ticket = 0;
-  vc->finished = 0;
-  vc->epoch = epoch + 1;
+                     m_next <= a.narrow_m && (int64_t)maxd <= a.narrow_deg;
+  if (dir == TD) c->td_levels = tdl + 1;
+  else c->bu_levels = bul + 1;
+  if (new_queues) {
+    c->qcur = qcur ^ 1;
+    for (int k = 0; k < 3; ++k) c->n_q[k] = (int32_t)tot[k];
+    c->n_chunks = (int32_t)tot[3];
+  }
+  c->n_vis = n_vis1;
+  c->m_vis = m_vis0 + m_next;
+  c->n_f = n_next;
+  c->m_f = m_next;
+  c->dir = next_dir;
+  c->level = L + 1;
+  c->err = err1;
+  c->done = done;
+  c->narrow = narrow;
+  c->skip = 0;
+  c->acc_maxd = 0;
+  c->iters = it0 + 1;
+  c->n_raw = 0;
+  c->acc_n = 0;
+  c->acc_m = 0;
+  for (int k = 0; k < KS; ++k) c->tot[k] = 0;
+  c->tile_ticket = 0;
+  c->finished = 0;
+  c->epoch = epoch + 1;
   __threadfence();
   if (a.use_cond) {
     cudaGraphSetConditional(a.cond, done ? 0u : 1u);
