@@ -25,6 +25,9 @@
 //    single-source traversal runs its small frontiers inside one
 //    thread-block cluster, so several queries proceed side by side on
 //    different SMs and each finishes as soon as its own traversal does.
+//  * Batched slots run on the highest stream priority and single-source slots
+//    on the lowest, so that the block scheduler hands freed SMs to batch
+//    kernels before the next cluster of a deep graph's traversal.
 //  * Latency = submit to the scheduler observing completion (poll granularity
 //    tens of microseconds); queue time = submit to launch.
 #include <algorithm>
@@ -292,6 +295,12 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
   const int64_t budget = o.hbm_budget_bytes > 0 ? o.hbm_budget_bytes : (int64_t)(free_b / 4);
+  // Batched slots run on the highest stream priority, single-source slots on
+  // the lowest: a single-source traversal of a deep graph holds a cluster of
+  // SMs for milliseconds, and without priorities the grid-wide kernels of
+  // batches queue behind it for SMs.
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   s->gs.resize(n_graphs);
   for (int k = 0; k < n_graphs; ++k) {
     GraphState& g = s->gs[k];
@@ -324,7 +333,7 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
           rc = create_bfs_workspace(g.g, &sl.sws);
         }
         if (rc == ENT_OK) {
-          cudaError_t e2 = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
+          cudaError_t e2 = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio_low);
           if (e2 == cudaSuccess) e2 = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
           if (e2 != cudaSuccess) rc = fail(ENT_ERR_CUDA, "slot setup: %s", cudaGetErrorString(e2));
         }
@@ -339,7 +348,7 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
     for (Slot& sl : g.slots) {
       int rc = create_batch_workspace(g.g, o.max_batch, &sl.ws);
       if (rc == ENT_OK) {
-        cudaError_t e2 = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
+        cudaError_t e2 = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio_high);
         if (e2 == cudaSuccess) e2 = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
         if (e2 == cudaSuccess) e2 = cudaMalloc(&sl.row_map_dev, sizeof(int32_t) * 2048);
         if (e2 == cudaSuccess) e2 = cudaGraphCreate(&sl.graph, 0);
