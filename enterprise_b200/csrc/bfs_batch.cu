@@ -70,6 +70,10 @@ struct BatchArgs {
   unsigned long long* X;
   unsigned long long* log;
   const unsigned long long* mask;  // [W] valid source bits
+  // [2][W] active sources: act[cur] holds the sources whose level-L frontier
+  // is non-empty, act[nxt] collects those found at level L+1. A source that
+  // is not active can add no bit again, so only its bits are ever needed.
+  unsigned long long* act[2];
   uint32_t* donebits;
   uint32_t* jfb[2];
   const uint32_t* lightbits;  // degree in [1, batch_small_max): bottom-up light tier
@@ -117,6 +121,25 @@ __device__ __forceinline__ void wappend(bool want, int v, int32_t* list, int32_t
   if (want) list[base + __popc(m & lanemask_lt())] = v;
 }
 
+// Adds found source bits to the CTA's active-source word; the atomic is only
+// paid for bits the word does not hold yet (a stale read costs an atomic).
+__device__ __forceinline__ void note_act(unsigned long long* s_word, unsigned long long bits) {
+  if ((*s_word & bits) != bits) atomicOr(s_word, bits);
+}
+
+// ORs the CTA's active-source words (s_act, W words) into dst; a word whose
+// bits are all present already costs a read, not an atomic.
+__device__ __forceinline__ void publish_act(const BatchArgs& a, const unsigned long long* s_act,
+                                            unsigned long long* dst) {
+  __syncthreads();
+  if ((int)threadIdx.x < a.W) {
+    const unsigned long long m = s_act[threadIdx.x];
+    const unsigned long long have =
+        (unsigned long long)__ldcg(reinterpret_cast<const long long*>(dst + threadIdx.x));
+    if ((have & m) != m) atomicOr(dst + threadIdx.x, m);
+  }
+}
+
 // ------------------------------------------------------------ seeding -----
 // Runs after X, donebits and both jfb bitmaps are zeroed (memset nodes). One CTA.
 __global__ void k_b_seed(BatchArgs a) {
@@ -138,6 +161,10 @@ __global__ void k_b_seed(BatchArgs a) {
       atomicAdd(&s_m, (unsigned long long)d);
       if (d >= a.heavy_deg) a.heavy[0][atomicAdd(&s_h, 1)] = v;
     }
+  }
+  for (int w = threadIdx.x; w < a.W; w += blockDim.x) {
+    a.act[0][w] = a.mask[w];
+    a.act[1][w] = 0;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -258,7 +285,7 @@ __device__ __forceinline__ void bu_finish_vertex(const BatchArgs& a, BatchCtl* c
   }
   if (gfull) {
     atomicOr(&a.donebits[v >> 5], 1u << (v & 31));
-    if (gany) my_md += (unsigned long long)d;
+    my_md += (unsigned long long)d;
   }
 }
 
@@ -267,20 +294,23 @@ __device__ __forceinline__ void bu_finish_vertex(const BatchArgs& a, BatchCtl* c
 // neighbours, so a lane keeps one accumulator and the W consecutive words of
 // a neighbour are read by W consecutive lanes.
 __device__ void b_bu_mid(const BatchArgs& a, BatchCtl* c, const unsigned long long* F, unsigned long long* NB,
-                         unsigned long long& my_m, unsigned long long& my_md) {
+                         unsigned long long& my_m, unsigned long long& my_md, unsigned long long* s_act) {
   const int W = a.W;
   const int lane = threadIdx.x & 31;
   const int w = lane % W, k = lane / W, NS = 32 / W;
   const int nxt = c->cur ^ 1;
   const int gw = (blockIdx.x * BB + threadIdx.x) >> 5, nw = (gridDim.x * BB) >> 5;
-  const unsigned long long mk = a.mask[w];
+  const unsigned long long mk = a.act[c->cur][w];
   const uint32_t* jfc = a.jfb[c->cur];
   for (int i = gw; i < a.n_mid; i += nw) {
     const int v = a.mid[i];
     if ((a.donebits[v >> 5] >> (v & 31)) & 1u) continue;
     const unsigned long long xv = a.X[(size_t)v * W + w];
     const unsigned long long need = mk & ~xv;
-    if (!__any_sync(FULL, need != 0)) continue;
+    if (!__any_sync(FULL, need != 0)) {  // every source it still lacks has finished
+      if (lane == 0) bu_finish_vertex(a, c, v, nxt, false, true, a.deg[v], my_m, my_md);
+      continue;
+    }
     const int64_t beg = a.off[v], end = a.off[v + 1];
     unsigned long long acc = 0, r = 0;
     for (int64_t e0 = beg; e0 < end; e0 += NS) {
@@ -299,6 +329,7 @@ __device__ void b_bu_mid(const BatchArgs& a, BatchCtl* c, const unsigned long lo
     if (k == 0 && nw_) {
       NB[(size_t)v * W + w] = nw_;
       a.X[(size_t)v * W + w] = xv | nw_;
+      note_act(s_act + w, nw_);
     }
     const bool gany = __any_sync(FULL, nw_ != 0);
     const bool gfull = __all_sync(FULL, ((xv | nw_) & mk) == mk);
@@ -309,26 +340,31 @@ __device__ void b_bu_mid(const BatchArgs& a, BatchCtl* c, const unsigned long lo
 // Large tier (degree >= batch_large_min): one CTA per vertex, reduced through shared
 // memory, early exit by block vote.
 __device__ void b_bu_large(const BatchArgs& a, BatchCtl* c, const unsigned long long* F, unsigned long long* NB,
-                           unsigned long long& my_m, unsigned long long& my_md) {
+                           unsigned long long& my_m, unsigned long long& my_md, unsigned long long* s_act) {
   __shared__ unsigned long long s_acc[32], s_need[32], s_x[32];
   __shared__ int s_skip;
   const int W = a.W;
   const int t = threadIdx.x, w = t % W, k = t / W, NS = BB / W;
   const int nxt = c->cur ^ 1;
   const uint32_t* jfc = a.jfb[c->cur];
+  const unsigned long long* ac = a.act[c->cur];
   for (int i = blockIdx.x; i < a.n_large; i += gridDim.x) {
     const int v = a.large[i];
     __syncthreads();
     if (t < W) {
       const unsigned long long x = a.X[(size_t)v * W + t];
       s_x[t] = x;
-      s_need[t] = a.mask[t] & ~x;
+      s_need[t] = ac[t] & ~x;
       s_acc[t] = 0;
     }
     if (t == 0) s_skip = (a.donebits[v >> 5] >> (v & 31)) & 1u;
     __syncthreads();
     bool need_any = t < W && s_need[t] != 0;
-    if (s_skip || !__syncthreads_or(need_any)) continue;
+    if (s_skip) continue;
+    if (!__syncthreads_or(need_any)) {  // every source it still lacks has finished
+      if (t == 0) bu_finish_vertex(a, c, v, nxt, false, true, a.deg[v], my_m, my_md);
+      continue;
+    }
     const int64_t beg = a.off[v], end = a.off[v + 1];
     for (int64_t e0 = beg; e0 < end; e0 += NS) {
       const int64_t e = e0 + k;
@@ -350,9 +386,10 @@ __device__ void b_bu_large(const BatchArgs& a, BatchCtl* c, const unsigned long 
       if (nw_) {
         NB[(size_t)v * W + t] = nw_;
         a.X[(size_t)v * W + t] = s_x[t] | nw_;
+        note_act(s_act + t, nw_);
         got = true;
       }
-      full = ((s_x[t] | nw_) & a.mask[t]) == a.mask[t];
+      full = ((s_x[t] | nw_) & ac[t]) == ac[t];
     }
     const bool gany = __syncthreads_or(got);
     const bool gfull = !__syncthreads_or(!full);
@@ -363,7 +400,7 @@ __device__ void b_bu_large(const BatchArgs& a, BatchCtl* c, const unsigned long 
 // Light tier (degree < batch_small_max): a group of G = W / WPL lanes handles one
 // vertex; each lane owns WPL words.
 template <int WPL>
-__device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long* s_red) {
+__device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long* s_red, unsigned long long* s_act) {
   const int cur = c->cur, nxt = cur ^ 1;
   const int slot = c->level - c->base;
   const unsigned long long* F = slot_ptr(a, slot);
@@ -379,7 +416,7 @@ __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
   const int64_t Wd = (a.V + 31) >> 5;
   unsigned long long mk[WPL];
 #pragma unroll
-  for (int j = 0; j < WPL; ++j) mk[j] = a.mask[gl * WPL + j];
+  for (int j = 0; j < WPL; ++j) mk[j] = a.act[cur][gl * WPL + j];
   const uint32_t* jfc = a.jfb[cur];
   unsigned long long my_m = 0, my_md = 0;
   for (int64_t wi = gw; wi < Wd; wi += nw) {
@@ -447,6 +484,7 @@ __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
           if (nw_) {
             nbv[j] = nw_;
             xw[j] = (mk[j] & ~need[j]) | nw_ | (xw[j] & ~mk[j]);
+            note_act(s_act + gl * WPL + j, nw_);
             got = true;
           }
           full &= (need[j] & ~nw_) == 0;
@@ -456,7 +494,7 @@ __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
         if (gl == 0 && gany) my_m += (unsigned long long)(e1 - e0);
         if (gl == 0 && gfull) {
           full_bits |= 1u << vl;
-          if (gany) my_md += (unsigned long long)(e1 - e0);
+          my_md += (unsigned long long)(e1 - e0);
         }
         if (gl == 0 && gany && e1 - e0 >= a.heavy_deg) {
           const int at = atomicAdd(&c->n_heavy[nxt], 1);
@@ -476,8 +514,9 @@ __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
     if (lane == 0 && full_bits) atomicOr(&a.donebits[wi], full_bits);
     if (lane == 0 && front_bits) atomicOr(&a.jfb[nxt][wi], front_bits);
   }
-  b_bu_mid(a, c, F, NB, my_m, my_md);
-  b_bu_large(a, c, F, NB, my_m, my_md);
+  b_bu_mid(a, c, F, NB, my_m, my_md, s_act);
+  b_bu_large(a, c, F, NB, my_m, my_md, s_act);
+  publish_act(a, s_act, a.act[nxt]);
   const int any = __syncthreads_or(my_m != 0 || my_md != 0);
   if (any) {
     unsigned long long r = bsum(my_m, s_red);
@@ -489,15 +528,17 @@ __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
 
 __global__ void __launch_bounds__(BB, 4) k_b_expand(BatchArgs a) {
   extern __shared__ unsigned long long s_f[];
-  __shared__ unsigned long long s_red[BB / 32];
+  __shared__ unsigned long long s_red[BB / 32], s_act[WMAX];
   BatchCtl* c = a.ctl;
   if (c->done) return;
   if (c->dir == 0) {
     b_td_expand(a, c, s_f);
   } else {
-    if (a.W == 1) b_bu_expand<1>(a, c, s_red);
-    else if (a.W == 2) b_bu_expand<2>(a, c, s_red);
-    else b_bu_expand<4>(a, c, s_red);
+    if ((int)threadIdx.x < WMAX) s_act[threadIdx.x] = 0;
+    __syncthreads();
+    if (a.W == 1) b_bu_expand<1>(a, c, s_red, s_act);
+    else if (a.W == 2) b_bu_expand<2>(a, c, s_red, s_act);
+    else b_bu_expand<4>(a, c, s_red, s_act);
   }
 }
 
@@ -506,7 +547,7 @@ __global__ void __launch_bounds__(BB, 4) k_b_expand(BatchArgs a) {
 // the frontier bitmap of level L (jfb[cur], its words hold only jf[cur]). Then the
 // last CTA advances the level and picks the next direction.
 __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
-  __shared__ unsigned long long s_red[BB / 32];
+  __shared__ unsigned long long s_red[BB / 32], s_act[WMAX];
   __shared__ int s_last;
   BatchCtl* c = a.ctl;
   if (c->done) {  // never leave the while node spinning on a finished traversal
@@ -525,16 +566,31 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
     const int slot = c->level - c->base;
     const unsigned long long* NB = slot_ptr(a, slot + 1);
     const int n = c->n_jf[nxt];
+    const unsigned long long* ac = a.act[cur];
     unsigned long long my_m = 0, my_md = 0;
+    const int lane = threadIdx.x & 31;
+    if ((int)threadIdx.x < WMAX) s_act[threadIdx.x] = 0;
+    __syncthreads();
     const int64_t gtid = blockIdx.x * (int64_t)BB + threadIdx.x, nth = (int64_t)gridDim.x * BB;
-    for (int64_t i = gtid; i < n; i += nth) {
-      const int v = a.jf[nxt][i];
+    // warp-uniform trip count: the claimed words are OR-reduced across the warp
+    for (int64_t i0 = gtid - lane; i0 < n; i0 += nth) {
+      const int64_t i = i0 + lane;
+      const bool valid = i < n;
+      const int v = valid ? a.jf[nxt][i] : 0;
       bool full = true;
       for (int w = 0; w < a.W; ++w) {
-        const unsigned long long x = a.X[(size_t)v * a.W + w] | NB[(size_t)v * a.W + w];
-        a.X[(size_t)v * a.W + w] = x;
-        full &= (x & a.mask[w]) == a.mask[w];
+        unsigned long long nb = 0;
+        if (valid) {
+          nb = NB[(size_t)v * a.W + w];
+          const unsigned long long x = a.X[(size_t)v * a.W + w] | nb;
+          a.X[(size_t)v * a.W + w] = x;
+          full &= (x & ac[w]) == ac[w];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nb |= __shfl_xor_sync(FULL, nb, o);
+        if (lane == 0 && nb) atomicOr(&s_act[w], nb);
       }
+      if (!valid) continue;
       const int d = a.deg[v];
       my_m += d;
       if (full) {
@@ -543,6 +599,7 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
       }
       if (d >= a.heavy_deg) a.heavy[nxt][atomicAdd(&c->n_heavy[nxt], 1)] = v;
     }
+    publish_act(a, s_act, a.act[nxt]);
     if (__syncthreads_or(my_m != 0 || my_md != 0)) {
       unsigned long long r = bsum(my_m, s_red);
       if (threadIdx.x == 0) atomicAdd(&c->acc_m, r);
@@ -564,6 +621,8 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
   if (dir == 0) vc->td_levels = vc->td_levels + 1; else vc->bu_levels = vc->bu_levels + 1;
   const int L = vc->level + 1;
   vc->level = L;
+  // level L's active set is spent: it collects level L+2's from here
+  for (int w = 0; w < a.W; ++w) a.act[cur][w] = 0;
   vc->cur = nxt;
   vc->n_jf[cur] = 0;
   vc->n_heavy[cur] = 0;
@@ -931,7 +990,7 @@ int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
   const size_t sz_mask = al(sizeof(unsigned long long) * W);
   const size_t sz_src = al(sizeof(int32_t) * w->cap_src);
   const size_t sz_st = al(sizeof(unsigned long long) * w->cap_src) * 2 + al(sizeof(int32_t) * w->cap_src);
-  const size_t total = sz_x + sz_log + 4 * sz_bits + 6 * sz_q + sz_mask + sz_src + sz_st + 256;
+  const size_t total = sz_x + sz_log + 4 * sz_bits + 6 * sz_q + 3 * sz_mask + sz_src + sz_st + 256;
   cudaError_t e = cudaMalloc(&w->slab, total);
   if (e != cudaSuccess) { destroy_batch_workspace(w); return fail(ENT_ERR_OOM, "batch workspace (%zu bytes) failed", total); }
   // Initialise on the graph's stream and wait (see create_workspace in
@@ -975,6 +1034,8 @@ int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
   a.mid = mid;
   a.large = large;
   a.mask = (const unsigned long long*)p; p += sz_mask;
+  a.act[0] = (unsigned long long*)p; p += sz_mask;
+  a.act[1] = (unsigned long long*)p; p += sz_mask;
   a.src = (const int32_t*)p; p += sz_src;
   w->stats_ptr = p;
   w->stats_bytes = sz_st;

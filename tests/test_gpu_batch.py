@@ -116,3 +116,43 @@ def test_multi_graph_one_launch(eb, orc):
     plan.close()
     for g in graphs:
         g.close()
+
+
+@pytest.mark.parametrize("n", [40, 130, 600])
+def test_sources_in_small_components(eb, orc, n):
+    """Sources of small components mixed with giant-component sources. Once a
+    small component's frontier is empty its source is no longer active, so the
+    giant component's vertices stop needing its bit and are marked done in
+    every bottom-up tier (light, mid, large); rows stay exact."""
+    base = eb.Csr.rmat(13, 16, seed=4242)
+    V0 = base.vert_count
+    s = np.repeat(np.arange(V0, dtype=np.int64), np.diff(base.beg_pos))
+    d = base.csr.astype(np.int64)
+    # appended components: a 30-vertex path, three pairs, one isolated vertex
+    path = np.arange(V0, V0 + 30, dtype=np.int64)
+    pairs = np.array([[V0 + 30, V0 + 31], [V0 + 32, V0 + 33], [V0 + 34, V0 + 35]], dtype=np.int64)
+    s = np.concatenate([s, path[:-1], pairs[:, 0]])
+    d = np.concatenate([d, path[1:], pairs[:, 1]])
+    csr = eb.Csr.from_edges(s, d, V0 + 37)
+    hub = int(np.argmax(np.diff(csr.beg_pos)))
+    reach, _ = orc.bfs(csr.beg_pos, csr.csr, hub)
+    deg = np.diff(csr.beg_pos)
+    small = [int(v) for v in np.nonzero((reach < 0) & (deg > 0))[0]][: max(4, n // 8)]
+    small += [V0, V0 + 29, V0 + 31, V0 + 36]
+    giant = eb.pick_sources(csr.beg_pos, 31 + n, n - len(small))
+    srcs = [int(x) for x in giant] + small
+    rng = np.random.default_rng(n)
+    rng.shuffle(srcs)
+    with eb.Graph.from_csr(csr) as g:
+        o = g.opts
+        o.batch_alpha = 4.0
+        o.batch_small_max = 8
+        o.batch_large_min = 64
+        g.opts = o
+        depth, stats = g.bfs_batch(srcs)
+        check = [i for i, x in enumerate(srcs) if x in small or reach[x] < 0] + list(range(0, n, max(1, n // 24)))
+        for i in sorted(set(check)):
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, int(srcs[i]))
+            np.testing.assert_array_equal(depth[i], exp, err_msg=f"row {i} (source {srcs[i]})")
+            assert stats[i].reached_vertices == (exp >= 0).sum()
+            assert stats[i].levels == int(exp.max()) + 1
