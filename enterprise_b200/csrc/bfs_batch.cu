@@ -289,62 +289,125 @@ __device__ __forceinline__ void bu_finish_vertex(const BatchArgs& a, BatchCtl* c
   }
 }
 
-// Mid tier (batch_small_max <= degree < batch_large_min): one warp per vertex. Lane = (word w,
-// neighbour slot k): lanes w, w+W, w+2W, ... OR word w of different
-// neighbours, so a lane keeps one accumulator and the W consecutive words of
-// a neighbour are read by W consecutive lanes.
+// Gathers the frontier words of two neighbour slots of a row (e and e + step,
+// each if below end): both ids, then both status bits, then both word loads
+// are in flight together. A thread owns WPT consecutive words (from wofs) of
+// every neighbour it visits and ORs them into acc.
+template <int WPT>
+__device__ __forceinline__ void bu_gather2(const BatchArgs& a, const uint32_t* jfc, const unsigned long long* F,
+                                           int64_t e, int64_t step, int64_t end, int wofs,
+                                           unsigned long long (&acc)[WPT]) {
+  const bool ok0 = e < end, ok1 = e + step < end;
+  const int u0 = ok0 ? __ldg(a.adj + e) : 0;
+  const int u1 = ok1 ? __ldg(a.adj + e + step) : 0;
+  const bool h0 = ok0 && ((__ldg(jfc + (u0 >> 5)) >> (u0 & 31)) & 1u);
+  const bool h1 = ok1 && ((__ldg(jfc + (u1 >> 5)) >> (u1 & 31)) & 1u);
+  unsigned long long f0[WPT], f1[WPT];
+#pragma unroll
+  for (int j = 0; j < WPT; ++j) f0[j] = f1[j] = 0;
+  if (h0) load_words<WPT>(F + (size_t)u0 * a.W + wofs, f0);
+  if (h1) load_words<WPT>(F + (size_t)u1 * a.W + wofs, f1);
+#pragma unroll
+  for (int j = 0; j < WPT; ++j) acc[j] |= f0[j] | f1[j];
+}
+
+// ORs r across the lanes of a warp that own the same words (lanes equal
+// modulo G). With G = 1 every lane owns the same words: one redux per half.
+template <int WPT>
+__device__ __forceinline__ void group_or(unsigned long long (&r)[WPT], int G) {
+  if (G == 1) {
+#pragma unroll
+    for (int j = 0; j < WPT; ++j) {
+      const unsigned lo = __reduce_or_sync(FULL, (unsigned)r[j]);
+      const unsigned hi = __reduce_or_sync(FULL, (unsigned)(r[j] >> 32));
+      r[j] = ((unsigned long long)hi << 32) | lo;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < WPT; ++j)
+      for (int o = G; o < 32; o <<= 1) r[j] |= __shfl_xor_sync(FULL, r[j], o);
+  }
+}
+
+// Mid tier (batch_small_max <= degree < batch_large_min): one warp per vertex.
+// G = W / WPT lanes cover a neighbour's W words (WPT each, one 8*WPT-byte
+// load), so a warp visits 32 / G neighbours per slot and two slots per step,
+// reading the row coalesced. Lanes accumulate in registers; the warp tests
+// coverage after steps 1, 3, 7, 11, ... (the interval doubles up to 4).
+template <int WPT>
 __device__ void b_bu_mid(const BatchArgs& a, BatchCtl* c, const unsigned long long* F, unsigned long long* NB,
                          unsigned long long& my_m, unsigned long long& my_md, unsigned long long* s_act) {
-  const int W = a.W;
-  const int lane = threadIdx.x & 31;
-  const int w = lane % W, k = lane / W, NS = 32 / W;
+  const int W = a.W, G = W / WPT, NS = 32 / G;
+  const int lane = threadIdx.x & 31, gl = lane % G, k = lane / G;
   const int nxt = c->cur ^ 1;
   const int gw = (blockIdx.x * BB + threadIdx.x) >> 5, nw = (gridDim.x * BB) >> 5;
-  const unsigned long long mk = a.act[c->cur][w];
+  const unsigned long long* ac = a.act[c->cur] + gl * WPT;
   const uint32_t* jfc = a.jfb[c->cur];
   for (int i = gw; i < a.n_mid; i += nw) {
     const int v = a.mid[i];
     if ((a.donebits[v >> 5] >> (v & 31)) & 1u) continue;
-    const unsigned long long xv = a.X[(size_t)v * W + w];
-    const unsigned long long need = mk & ~xv;
-    if (!__any_sync(FULL, need != 0)) {  // every source it still lacks has finished
+    unsigned long long* xv = a.X + (size_t)v * W + gl * WPT;
+    unsigned long long need[WPT], acc[WPT];
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < WPT; ++j) {
+      need[j] = ac[j] & ~xv[j];
+      acc[j] = 0;
+      any |= need[j] != 0;
+    }
+    if (!__any_sync(FULL, any)) {  // every source it still lacks has finished
       if (lane == 0) bu_finish_vertex(a, c, v, nxt, false, true, a.deg[v], my_m, my_md);
       continue;
     }
     const int64_t beg = a.off[v], end = a.off[v + 1];
-    unsigned long long acc = 0, r = 0;
-    for (int64_t e0 = beg; e0 < end; e0 += NS) {
-      const int64_t e = e0 + k;
-      if (e < end) {
-        const int u = __ldg(a.adj + e);
-        if ((__ldg(jfc + (u >> 5)) >> (u & 31)) & 1u) acc |= __ldg(F + (size_t)u * W + w);
+    int chk = 1, since = 0;
+    for (int64_t b0 = beg; b0 < end; b0 += 2 * NS) {
+      bu_gather2<WPT>(a, jfc, F, b0 + k, NS, end, gl * WPT, acc);
+      if (++since == chk) {
+        since = 0;
+        if (chk < 4) chk <<= 1;
+        unsigned long long r[WPT];
+        bool mine = true;
+#pragma unroll
+        for (int j = 0; j < WPT; ++j) r[j] = acc[j];
+        group_or<WPT>(r, G);
+#pragma unroll
+        for (int j = 0; j < WPT; ++j) mine &= (r[j] & need[j]) == need[j];
+        if (__all_sync(FULL, mine)) break;
       }
-      r = acc;
-      for (int o = W; o < 32; o <<= 1) r |= __shfl_xor_sync(FULL, r, o);
-      if (__all_sync(FULL, (r & need) == need)) break;
     }
-    r = acc;
-    for (int o = W; o < 32; o <<= 1) r |= __shfl_xor_sync(FULL, r, o);
-    const unsigned long long nw_ = r & need;
-    if (k == 0 && nw_) {
-      NB[(size_t)v * W + w] = nw_;
-      a.X[(size_t)v * W + w] = xv | nw_;
-      note_act(s_act + w, nw_);
+    group_or<WPT>(acc, G);
+    bool got = false, full = true;
+#pragma unroll
+    for (int j = 0; j < WPT; ++j) {
+      const unsigned long long nw_ = acc[j] & need[j];
+      if (nw_) {
+        got = true;
+        if (k == 0) {
+          NB[(size_t)v * W + gl * WPT + j] = nw_;
+          xv[j] = xv[j] | nw_;
+          note_act(s_act + gl * WPT + j, nw_);
+        }
+      }
+      full &= (need[j] & ~nw_) == 0;
     }
-    const bool gany = __any_sync(FULL, nw_ != 0);
-    const bool gfull = __all_sync(FULL, ((xv | nw_) & mk) == mk);
+    const bool gany = __any_sync(FULL, got);
+    const bool gfull = __all_sync(FULL, full);
     if (lane == 0) bu_finish_vertex(a, c, v, nxt, gany, gfull, end - beg, my_m, my_md);
   }
 }
 
-// Large tier (degree >= batch_large_min): one CTA per vertex, reduced through shared
-// memory, early exit by block vote.
+// Large tier (degree >= batch_large_min): one CTA per vertex, the same lane
+// layout over BB / G neighbours per slot. Threads accumulate in registers; at
+// coverage tests (after steps 1, 3, 7, 15, 23, ...: the interval doubles up to
+// 8) each warp folds its words into shared memory and the block votes.
+template <int WPT>
 __device__ void b_bu_large(const BatchArgs& a, BatchCtl* c, const unsigned long long* F, unsigned long long* NB,
                            unsigned long long& my_m, unsigned long long& my_md, unsigned long long* s_act) {
-  __shared__ unsigned long long s_acc[32], s_need[32], s_x[32];
+  __shared__ unsigned long long s_acc[WMAX], s_need[WMAX];
   __shared__ int s_skip;
-  const int W = a.W;
-  const int t = threadIdx.x, w = t % W, k = t / W, NS = BB / W;
+  const int W = a.W, G = W / WPT, NS = BB / G;
+  const int t = threadIdx.x, lane = t & 31, gl = t % G, k = t / G;
   const int nxt = c->cur ^ 1;
   const uint32_t* jfc = a.jfb[c->cur];
   const unsigned long long* ac = a.act[c->cur];
@@ -352,44 +415,56 @@ __device__ void b_bu_large(const BatchArgs& a, BatchCtl* c, const unsigned long 
     const int v = a.large[i];
     __syncthreads();
     if (t < W) {
-      const unsigned long long x = a.X[(size_t)v * W + t];
-      s_x[t] = x;
-      s_need[t] = ac[t] & ~x;
+      s_need[t] = ac[t] & ~a.X[(size_t)v * W + t];
       s_acc[t] = 0;
     }
     if (t == 0) s_skip = (a.donebits[v >> 5] >> (v & 31)) & 1u;
     __syncthreads();
-    bool need_any = t < W && s_need[t] != 0;
     if (s_skip) continue;
-    if (!__syncthreads_or(need_any)) {  // every source it still lacks has finished
+    if (!__syncthreads_or(t < W && s_need[t] != 0)) {  // every source it still lacks has finished
       if (t == 0) bu_finish_vertex(a, c, v, nxt, false, true, a.deg[v], my_m, my_md);
       continue;
     }
-    const int64_t beg = a.off[v], end = a.off[v + 1];
-    for (int64_t e0 = beg; e0 < end; e0 += NS) {
-      const int64_t e = e0 + k;
-      if (e < end) {
-        const int u = __ldg(a.adj + e);
-        if ((__ldg(jfc + (u >> 5)) >> (u & 31)) & 1u) {
-          const unsigned long long f = __ldg(F + (size_t)u * W + w);
-          if (f) atomicOr(&s_acc[w], f);
-        }
-      }
-      __syncthreads();
-      const bool open = t < W && (s_acc[t] & s_need[t]) != s_need[t];
-      if (!__syncthreads_or(open)) break;
+    unsigned long long need[WPT], acc[WPT];
+#pragma unroll
+    for (int j = 0; j < WPT; ++j) {
+      need[j] = s_need[gl * WPT + j];
+      acc[j] = 0;
     }
+    const int64_t beg = a.off[v], end = a.off[v + 1];
+    int chk = 1, since = 0;
+    for (int64_t b0 = beg; b0 < end; b0 += 2 * NS) {
+      bu_gather2<WPT>(a, jfc, F, b0 + k, NS, end, gl * WPT, acc);
+      if (++since == chk) {
+        since = 0;
+        if (chk < 8) chk <<= 1;
+        unsigned long long r[WPT];
+#pragma unroll
+        for (int j = 0; j < WPT; ++j) r[j] = acc[j];
+        group_or<WPT>(r, G);
+        if (lane < G)
+#pragma unroll
+          for (int j = 0; j < WPT; ++j) note_act(s_acc + gl * WPT + j, r[j] & need[j]);
+        __syncthreads();
+        const bool open = t < W && (s_acc[t] & s_need[t]) != s_need[t];
+        if (!__syncthreads_or(open)) break;
+      }
+    }
+    group_or<WPT>(acc, G);
+    if (lane < G)
+#pragma unroll
+      for (int j = 0; j < WPT; ++j) note_act(s_acc + gl * WPT + j, acc[j] & need[j]);
     __syncthreads();
     bool got = false, full = true;
     if (t < W) {
       const unsigned long long nw_ = s_acc[t] & s_need[t];
       if (nw_) {
         NB[(size_t)v * W + t] = nw_;
-        a.X[(size_t)v * W + t] = s_x[t] | nw_;
+        a.X[(size_t)v * W + t] = a.X[(size_t)v * W + t] | nw_;
         note_act(s_act + t, nw_);
         got = true;
       }
-      full = ((s_x[t] | nw_) & ac[t]) == ac[t];
+      full = (s_need[t] & ~nw_) == 0;
     }
     const bool gany = __syncthreads_or(got);
     const bool gfull = !__syncthreads_or(!full);
@@ -514,8 +589,8 @@ __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
     if (lane == 0 && full_bits) atomicOr(&a.donebits[wi], full_bits);
     if (lane == 0 && front_bits) atomicOr(&a.jfb[nxt][wi], front_bits);
   }
-  b_bu_mid(a, c, F, NB, my_m, my_md, s_act);
-  b_bu_large(a, c, F, NB, my_m, my_md, s_act);
+  b_bu_mid<WPL>(a, c, F, NB, my_m, my_md, s_act);
+  b_bu_large<WPL>(a, c, F, NB, my_m, my_md, s_act);
   publish_act(a, s_act, a.act[nxt]);
   const int any = __syncthreads_or(my_m != 0 || my_md != 0);
   if (any) {
