@@ -721,16 +721,22 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
 
 // ----------------------------------------------------------- flush --------
 // Converts log slots [first, last] (levels base+first .. base+last) into the
-// source-major depth rows. A CTA takes a span of vertices and walks the W
-// word columns in groups of CG = min(W, 4): it reads each vertex's CG words
-// of a slot with one 8*CG-byte load (whole sectors), decodes the 64*CG
-// sources into a shared byte tile [source][vertex] (slot index or 0xFF), then
-// each warp writes whole row segments (VS int32 contiguous, 16-byte stores)
-// and reduces that row's statistics once. The first window writes every
-// (source, vertex) pair (-1 where not found); later windows only the pairs
-// they found. Recycling the slots (zeroing, carrying the last one into slot
-// 0) is left to k_b_recycle, which streams them contiguously.
-constexpr int TILE_BYTES = 64 * 1024;  // 64*CG rows x VS vertices
+// source-major depth rows. A CTA takes a span of 1024 vertices and walks the W
+// word columns in groups of CG = min(W, 4), VS = 1024 / CG vertices per pass.
+// Decode (thread per vertex): the slots of a vertex are disjoint bit sets, so
+// the vertex's CG words of every slot fold into a found mask and four bit
+// planes of the slot index; each 4-source nibble of those becomes one 32-bit
+// word of four bytes (slot index, 0xFF where not found) by multiply-spreading
+// the nibbles, stored in a vertex-major byte tile [vertex][64*CG sources]
+// whose 32-bit words are XOR-swizzled so that the 32 lanes of a warp hit 32
+// banks in both phases. Write (warp per 4 sources): a lane reads one tile
+// word per vertex, sign-extends its four bytes into the four rows' depths
+// (coalesced 128-byte stores per row) and keeps the rows' statistics. The
+// first window writes every (source, vertex) pair (-1 where not found); later
+// windows only the pairs they found. Recycling the slots (zeroing, carrying
+// the last one into slot 0) is left to k_b_recycle, which streams them
+// contiguously.
+constexpr int TILE_BYTES = 64 * 1024;  // VS vertices x 64*CG source bytes
 constexpr int FLUSH_TILE_BYTES = TILE_BYTES + 1024 * 4;
 
 template <int CG>
@@ -747,90 +753,132 @@ __device__ __forceinline__ void load_cols(const unsigned long long* p, unsigned 
   }
 }
 
+// Tile word c (4 sources) of vertex vi: rows of 16*CG words, the word index
+// XOR-swizzled by the vertex so that 32 consecutive vertices use 32 banks.
 template <int CG>
-__device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, int last, int base, int windows,
-                           int nsrc, int32_t* depth, const int32_t* row_map, bool vec_ok, unsigned char* tile,
-                           const int* s_deg, unsigned* s_cnt, int* s_maxd, unsigned long long* s_edg) {
-  constexpr int VS = TILE_BYTES / (64 * CG);  // vertices per pass
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int64_t sub = 0; sub < nv; sub += VS) {
-    const int nsub = (int)min((int64_t)VS, (int64_t)nv - sub);
-    for (int cg = 0; cg < a.W; cg += CG) {
-      if (cg * 64 >= nsrc) break;
-      int4* t4 = reinterpret_cast<int4*>(tile);
-      for (int i = threadIdx.x; i < TILE_BYTES / 16; i += BB) t4[i] = make_int4(-1, -1, -1, -1);
-      __syncthreads();
-      for (int vi = threadIdx.x; vi < nsub; vi += BB) {
-        const size_t at = (size_t)(v0 + sub + vi) * a.W + cg;
-        for (int k0 = first; k0 <= last; k0 += 4) {
-          unsigned long long w[4][CG];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            if (k0 + q <= last) load_cols<CG>(slot_ptr(a, k0 + q) + at, w[q]);
-            else
-#pragma unroll
-              for (int cc = 0; cc < CG; ++cc) w[q][cc] = 0;
-          }
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int cc = 0; cc < CG; ++cc)
-              for (unsigned long long m = w[q][cc]; m; m &= m - 1)
-                tile[(cc * 64 + __ffsll((long long)m) - 1) * VS + vi] = (unsigned char)(k0 + q);
-        }
-      }
-      __syncthreads();
-      for (int r = warp; r < 64 * CG; r += BB / 32) {
-        const int s = cg * 64 + r;
-        if (s >= nsrc) break;
-        const uint32_t* row = reinterpret_cast<const uint32_t*>(tile + r * VS);
-        int32_t* out = depth + (size_t)(row_map ? row_map[s] : s) * a.V + v0 + sub;
-        const int* dg = s_deg + sub;
-        unsigned cnt = 0;
-        unsigned long long edg = 0;
-        int mx = -1;
-        for (int q = lane; q * 4 < nsub; q += 32) {
-          const uint32_t wq = row[q];
-          int dq[4];
-          bool fq[4];
-#pragma unroll
-          for (int b = 0; b < 4; ++b) {
-            const int vi = q * 4 + b;
-            const uint32_t byte = (wq >> (8 * b)) & 0xFFu;
-            fq[b] = vi < nsub && byte != 0xFFu;
-            dq[b] = fq[b] ? base + (int)byte : -1;
-            if (fq[b]) {
-              ++cnt;
-              edg += (unsigned long long)dg[vi];
-              mx = max(mx, dq[b]);
-            }
-          }
-          if (windows == 0 && vec_ok && q * 4 + 4 <= nsub) {
-            *reinterpret_cast<int4*>(out + q * 4) = make_int4(dq[0], dq[1], dq[2], dq[3]);
-          } else {
-#pragma unroll
-            for (int b = 0; b < 4; ++b)
-              if ((windows == 0 && q * 4 + b < nsub) || fq[b]) out[q * 4 + b] = dq[b];
-          }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          cnt += __shfl_xor_sync(FULL, cnt, o);
-          edg += __shfl_xor_sync(FULL, edg, o);
-          mx = max(mx, __shfl_xor_sync(FULL, mx, o));
-        }
-        if (lane == 0 && cnt) {
-          s_cnt[s] += cnt;
-          s_edg[s] += edg;
-          s_maxd[s] = max(s_maxd[s], mx);
-        }
-      }
-      __syncthreads();
-    }
-  }
+__device__ __forceinline__ int tile_word(int vi, int c) {
+  if constexpr (CG == 1) return vi * 16 + (c ^ ((vi >> 1) & 15));
+  else return vi * 16 * CG + (c ^ (vi & 31));
 }
 
-__global__ void __launch_bounds__(BB) k_b_flush(BatchArgs a, int final_flush) {
+// Bit i (i < 4) of the nibble n moves to bit 8*i + sh: x * 0x00204081 puts
+// copies of n at bits 0, 7, 14, 21, which do not overlap, so no carries.
+__device__ __forceinline__ uint32_t spread4(uint32_t n, int sh) {
+  return ((n * 0x00204081u) & 0x01010101u) << sh;
+}
+
+template <int CG>
+__device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, int last, int base, int windows,
+                           int nsrc, int32_t* depth, const int32_t* row_map, uint32_t* tile, const int* s_deg,
+                           unsigned* s_cnt, int* s_maxd, unsigned long long* s_edg) {
+  constexpr int VS = 1024 / CG;  // vertices per pass
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool four_planes = last >= 8;
+  for (int sub = 0; sub < nv; sub += VS) {
+    const int nsub = min(VS, nv - sub);
+    for (int cg = 0; cg < a.W; cg += CG) {
+      if (cg * 64 >= nsrc) break;
+      __syncthreads();  // the previous tile has been written out
+      for (int vi = threadIdx.x; vi < VS; vi += BB) {
+        unsigned long long f[CG], p0[CG], p1[CG], p2[CG], p3[CG];
+#pragma unroll
+        for (int cc = 0; cc < CG; ++cc) f[cc] = p0[cc] = p1[cc] = p2[cc] = p3[cc] = 0;
+        if (vi < nsub) {
+          const size_t at = (size_t)(v0 + sub + vi) * a.W + cg;
+          for (int k0 = first; k0 <= last; k0 += 2) {
+            unsigned long long w[2][CG];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+              if (k0 + q <= last) load_cols<CG>(slot_ptr(a, k0 + q) + at, w[q]);
+              else
+#pragma unroll
+                for (int cc = 0; cc < CG; ++cc) w[q][cc] = 0;
+            }
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+              const int k = k0 + q;
+#pragma unroll
+              for (int cc = 0; cc < CG; ++cc) {
+                const unsigned long long x = w[q][cc];
+                f[cc] |= x;
+                if (k & 1) p0[cc] |= x;
+                if (k & 2) p1[cc] |= x;
+                if (k & 4) p2[cc] |= x;
+                if (k & 8) p3[cc] |= x;
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int cc = 0; cc < CG; ++cc) {
+#pragma unroll
+          for (int hw = 0; hw < 2; ++hw) {
+            const uint32_t fh = (uint32_t)(f[cc] >> (32 * hw)), h0 = (uint32_t)(p0[cc] >> (32 * hw)),
+                           h1 = (uint32_t)(p1[cc] >> (32 * hw)), h2 = (uint32_t)(p2[cc] >> (32 * hw)),
+                           h3 = (uint32_t)(p3[cc] >> (32 * hw));
+#pragma unroll
+            for (int n = 0; n < 8; ++n) {
+              const int sh = 4 * n;
+              uint32_t o = ~(spread4((fh >> sh) & 15u, 0) * 0xFFu);  // 0xFF where not found
+              o |= spread4((h0 >> sh) & 15u, 0) | spread4((h1 >> sh) & 15u, 1) | spread4((h2 >> sh) & 15u, 2);
+              if (four_planes) o |= spread4((h3 >> sh) & 15u, 3);
+              tile[tile_word<CG>(vi, cc * 16 + hw * 8 + n)] = o;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      for (int r0 = warp * 4; r0 < 64 * CG; r0 += BB / 32 * 4) {
+        const int s0 = cg * 64 + r0;
+        if (s0 >= nsrc) break;
+        int32_t* out[4];
+        bool rv[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          rv[j] = s0 + j < nsrc;
+          out[j] = rv[j] ? depth + (size_t)(row_map ? row_map[s0 + j] : s0 + j) * a.V + v0 + sub : depth;
+        }
+        unsigned cnt[4] = {0, 0, 0, 0};
+        unsigned long long edg[4] = {0, 0, 0, 0};
+        int mx[4] = {-1, -1, -1, -1};
+        for (int vi = lane; vi < nsub; vi += 32) {
+          const uint32_t wv = tile[tile_word<CG>(vi, r0 >> 2)];
+          const int dg = s_deg[sub + vi];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            int d = (int)(signed char)(uint8_t)(wv >> (8 * j));
+            if (d >= 0) d += base;
+            if (rv[j]) {
+              if (windows == 0 || d >= 0) out[j][vi] = d;
+              if (d >= 0) {
+                ++cnt[j];
+                edg[j] += (unsigned long long)dg;
+                mx[j] = max(mx[j], d);
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            cnt[j] += __shfl_xor_sync(FULL, cnt[j], o);
+            edg[j] += __shfl_xor_sync(FULL, edg[j], o);
+            mx[j] = max(mx[j], __shfl_xor_sync(FULL, mx[j], o));
+          }
+          if (lane == 0 && rv[j] && cnt[j]) {
+            s_cnt[s0 + j] += cnt[j];
+            s_edg[s0 + j] += edg[j];
+            s_maxd[s0 + j] = max(s_maxd[s0 + j], mx[j]);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(BB, 3) k_b_flush(BatchArgs a, int final_flush) {
   extern __shared__ __align__(16) unsigned char s_flush[];
   BatchCtl* c = a.ctl;
   if (!final_flush && !c->flush_now) return;
@@ -840,14 +888,13 @@ __global__ void __launch_bounds__(BB) k_b_flush(BatchArgs a, int final_flush) {
   const int first = windows == 0 ? 0 : 1;
   const int nsrc = c->n_src;
   const int NSRC = a.W * 64;
-  unsigned char* tile = s_flush;
+  uint32_t* tile = reinterpret_cast<uint32_t*>(s_flush);
   int* s_deg = reinterpret_cast<int*>(s_flush + TILE_BYTES);  // [1024]
   unsigned* s_cnt = reinterpret_cast<unsigned*>(s_flush + FLUSH_TILE_BYTES);
   int* s_maxd = reinterpret_cast<int*>(s_cnt + NSRC);
   unsigned long long* s_edg = reinterpret_cast<unsigned long long*>(s_maxd + NSRC);
   for (int i = threadIdx.x; i < NSRC; i += BB) { s_cnt[i] = 0; s_maxd[i] = -1; s_edg[i] = 0; }
   int32_t* depth = c->depth;
-  const bool vec_ok = (a.V % 4 == 0) && ((((uintptr_t)depth) & 15) == 0);
   const int64_t units = (a.V + 1023) / 1024;
   for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
     const int64_t v0 = u * 1024;
@@ -856,9 +903,9 @@ __global__ void __launch_bounds__(BB) k_b_flush(BatchArgs a, int final_flush) {
     for (int i = threadIdx.x; i < 1024; i += BB) s_deg[i] = i < nv ? a.deg[v0 + i] : 0;
     __syncthreads();
     const int32_t* row_map = c->row_map;
-    if (a.W == 1) flush_span<1>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
-    else if (a.W == 2) flush_span<2>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
-    else flush_span<4>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, vec_ok, tile, s_deg, s_cnt, s_maxd, s_edg);
+    if (a.W == 1) flush_span<1>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, tile, s_deg, s_cnt, s_maxd, s_edg);
+    else if (a.W == 2) flush_span<2>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, tile, s_deg, s_cnt, s_maxd, s_edg);
+    else flush_span<4>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, tile, s_deg, s_cnt, s_maxd, s_edg);
   }
   __syncthreads();
   for (int s = threadIdx.x; s < nsrc; s += BB) {
