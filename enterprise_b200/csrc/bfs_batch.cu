@@ -48,7 +48,7 @@ struct BatchCtl {
   int32_t flush_now; // the window is full: flush before the next level
   int32_t td_levels, bu_levels;
   int32_t n_src;
-  int32_t pad;
+  int32_t td_scan;   // top-down level of many edges: claims by no-return atomics, the commit rebuilds jf from jfb
   int32_t* depth;    // [n_src][V] output of this run
   const int32_t* row_map;  // optional: source s writes row row_map[s] of depth
   unsigned long long acc_m, acc_mdone;
@@ -174,6 +174,7 @@ __global__ void k_b_seed(BatchArgs a) {
     c->err = 0;
     c->cur = 0;
     c->n_jf[0] = s_n;
+    c->td_scan = 0;
     c->n_jf[1] = 0;
     c->n_heavy[0] = s_h;
     c->n_heavy[1] = 0;
@@ -193,8 +194,26 @@ __global__ void k_b_seed(BatchArgs a) {
 
 // ----------------------------------------------------------- top-down -----
 // Claims the bits of frontier vertex u (frontier words fu) for neighbour v.
+// With `scan` (uniform) the words and the frontier bit are ORed by atomics
+// whose results are not used, so nothing waits on memory; the commit then
+// drops the bits v already had. Otherwise v's visited words filter the bits
+// and the first claimant appends v to the next frontier.
 __device__ __forceinline__ void td_edge(const BatchArgs& a, BatchCtl* c, const unsigned long long* fu, int v,
-                                        bool valid, unsigned long long* nb, int nxt) {
+                                        bool valid, unsigned long long* nb, int nxt, bool scan) {
+  if (scan) {
+    if (valid) {
+      bool any = false;
+      for (int w = 0; w < a.W; ++w) {
+        const unsigned long long f = fu[w];
+        if (f) {
+          atomicOr(nb + (size_t)v * a.W + w, f);
+          any = true;
+        }
+      }
+      if (any) atomicOr(&a.jfb[nxt][v >> 5], 1u << (v & 31));
+    }
+    return;
+  }
   bool first = false;
   if (valid) {
     const unsigned long long* xv = a.X + (size_t)v * a.W;
@@ -221,6 +240,7 @@ __device__ void b_td_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
   const int slot = c->level - c->base;
   const unsigned long long* F = slot_ptr(a, slot);
   unsigned long long* NB = slot_ptr(a, slot + 1);
+  const bool scan = c->td_scan != 0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // Heavy frontier vertices: every CTA takes an interleaved slice of the edges.
   const int nh = c->n_heavy[cur];
@@ -233,7 +253,7 @@ __device__ void b_td_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
     for (int64_t e0 = beg + (int64_t)blockIdx.x * BB; e0 < end; e0 += (int64_t)gridDim.x * BB) {
       const int64_t e = e0 + threadIdx.x;
       const bool valid = e < end;
-      td_edge(a, c, s_f, valid ? __ldg(a.adj + e) : 0, valid, NB, nxt);
+      td_edge(a, c, s_f, valid ? __ldg(a.adj + e) : 0, valid, NB, nxt, scan);
     }
   }
   // Light frontier vertices: one warp each; the warp keeps F[u] in shared memory.
@@ -251,7 +271,7 @@ __device__ void b_td_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
     for (int64_t e0 = beg; e0 < end; e0 += 32) {
       const int64_t e = e0 + lane;
       const bool valid = e < end;
-      td_edge(a, c, fw, valid ? __ldg(a.adj + e) : 0, valid, NB, nxt);
+      td_edge(a, c, fw, valid ? __ldg(a.adj + e) : 0, valid, NB, nxt, scan);
     }
   }
 }
@@ -618,6 +638,33 @@ __global__ void __launch_bounds__(BB, 4) k_b_expand(BatchArgs a) {
 }
 
 // ----------------------------------------------------------- commit -------
+// Folds v's claimed words NB[v] into X[v] (warp-uniform call; `valid` lanes
+// only): the bits v already had are cleared from NB, got = a bit was new,
+// full = v now holds every active source. The new words are OR-reduced across
+// the warp into the CTA's active-source words.
+__device__ __forceinline__ void td_commit_words(const BatchArgs& a, unsigned long long* NB,
+                                                const unsigned long long* ac, int v, bool valid,
+                                                unsigned long long* s_act, bool& got, bool& full) {
+  const int lane = threadIdx.x & 31;
+  got = false;
+  full = true;
+  for (int w = 0; w < a.W; ++w) {
+    unsigned long long nn = 0;
+    if (valid) {
+      const size_t at = (size_t)v * a.W + w;
+      const unsigned long long nb = NB[at], x = a.X[at];
+      nn = nb & ~x;
+      if (nn != nb) NB[at] = nn;
+      if (nn) a.X[at] = x | nn;
+      got |= nn != 0;
+      full &= ((x | nn) & ac[w]) == ac[w];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nn |= __shfl_xor_sync(FULL, nn, o);
+    if (lane == 0) note_act(s_act + w, nn);
+  }
+}
+
 // Top-down: fold the claimed bits into X and count. Both directions: clear
 // the frontier bitmap of level L (jfb[cur], its words hold only jf[cur]). Then the
 // last CTA advances the level and picks the next direction.
@@ -639,7 +686,7 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
   }
   if (dir == 0) {
     const int slot = c->level - c->base;
-    const unsigned long long* NB = slot_ptr(a, slot + 1);
+    unsigned long long* NB = slot_ptr(a, slot + 1);
     const int n = c->n_jf[nxt];
     const unsigned long long* ac = a.act[cur];
     unsigned long long my_m = 0, my_md = 0;
@@ -647,25 +694,9 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
     if ((int)threadIdx.x < WMAX) s_act[threadIdx.x] = 0;
     __syncthreads();
     const int64_t gtid = blockIdx.x * (int64_t)BB + threadIdx.x, nth = (int64_t)gridDim.x * BB;
-    // warp-uniform trip count: the claimed words are OR-reduced across the warp
-    for (int64_t i0 = gtid - lane; i0 < n; i0 += nth) {
-      const int64_t i = i0 + lane;
-      const bool valid = i < n;
-      const int v = valid ? a.jf[nxt][i] : 0;
-      bool full = true;
-      for (int w = 0; w < a.W; ++w) {
-        unsigned long long nb = 0;
-        if (valid) {
-          nb = NB[(size_t)v * a.W + w];
-          const unsigned long long x = a.X[(size_t)v * a.W + w] | nb;
-          a.X[(size_t)v * a.W + w] = x;
-          full &= (x & ac[w]) == ac[w];
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) nb |= __shfl_xor_sync(FULL, nb, o);
-        if (lane == 0 && nb) atomicOr(&s_act[w], nb);
-      }
-      if (!valid) continue;
+    // bookkeeping for a vertex that gained a bit (got)
+    const auto vertex_done = [&](int v, bool got, bool full) {
+      if (!got) return;
       const int d = a.deg[v];
       my_m += d;
       if (full) {
@@ -673,6 +704,39 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
         my_md += d;
       }
       if (d >= a.heavy_deg) a.heavy[nxt][atomicAdd(&c->n_heavy[nxt], 1)] = v;
+    };
+    if (c->td_scan) {
+      // a warp takes 32 consecutive jfb words (lane = word) and walks their
+      // set bits in rounds, one vertex per lane per round
+      uint32_t* jn = a.jfb[nxt];
+      const int64_t Wd = (a.V + 31) >> 5;
+      for (int64_t wb = gtid - lane; wb < Wd; wb += nth) {
+        const int64_t wi = wb + lane;
+        const uint32_t orig = wi < Wd ? jn[wi] : 0u;
+        uint32_t bits = orig, keep = orig;
+        while (__any_sync(FULL, bits != 0)) {
+          const bool valid = bits != 0;
+          const int b = valid ? __ffs(bits) - 1 : 0;
+          bits &= bits - 1;
+          const int v = (int)(wi * 32 + b);
+          bool got, full;
+          td_commit_words(a, NB, ac, v, valid, s_act, got, full);
+          if (valid && !got) keep &= ~(1u << b);
+          wappend(valid && got, v, a.jf[nxt], &c->n_jf[nxt]);
+          if (valid) vertex_done(v, got, full);
+        }
+        if (keep != orig) jn[wi] = keep;
+      }
+    } else {
+      // warp-uniform trip count: the claimed words are OR-reduced across the warp
+      for (int64_t i0 = gtid - lane; i0 < n; i0 += nth) {
+        const int64_t i = i0 + lane;
+        const bool valid = i < n;
+        const int v = valid ? a.jf[nxt][i] : 0;
+        bool got, full;
+        td_commit_words(a, NB, ac, v, valid, s_act, got, full);
+        if (valid) vertex_done(v, true, full);
+      }
     }
     publish_act(a, s_act, a.act[nxt]);
     if (__syncthreads_or(my_m != 0 || my_md != 0)) {
@@ -704,6 +768,8 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
   vc->m_f = m_next;
   const double m_u = (double)(a.E - vc->m_done);
   vc->dir = ((double)m_next * a.alpha > m_u) ? 1 : 0;
+  // a top-down level over at least V/4 edges claims without waiting on memory
+  vc->td_scan = vc->dir == 0 && m_next * 4 >= a.V;
   int done = n_next == 0;
   if (L >= a.max_levels && !done) {
     vc->err = vc->err | 4;
