@@ -198,6 +198,7 @@ def run_ours(args, rank, world, dist):
         per_bfs.append(t_each)
         step_ms.append(t_step)
     clocks = clk.stop()
+    depth_ref_last = depth.cpu().numpy()  # the last source's depths from the device-timed run
     if dist:
         dist.barrier()
     from enterprise_b200 import replicas
@@ -216,23 +217,34 @@ def run_ours(args, rank, world, dist):
     traffic = profiled_traffic("bfs_rmat_s24_traffic.txt") if args.scale == 24 else None  # bytes per traversal
 
     # ------------------------------------------------ e2e through the C ABI
-    host_depth = np.empty(V, dtype=np.int32)
+    # ent_bfs_many: the reference's per-source loop (traverse, copy the depths
+    # to the host) as one call, each source's depths landing in its own pinned
+    # host row; the copy of one source overlaps the next traversal.
+    src_list = [int(s) for s in srcs]
+    rows = len(src_list)
+    try:
+        import psutil
+        if psutil.virtual_memory().available < 3 * rows * V * 4:
+            rows = 2  # not enough host memory for a row per source: alternate two rows
+    except Exception:
+        rows = 2
+    host_depth = np.empty((rows, V), dtype=np.int32)
     try:
         eb.host_register(host_depth)
         pinned = True
     except Exception:
         pinned = False
+    outs = [host_depth[i % rows] for i in range(len(src_list))]
     e2e_steps = max(1, min(args.steps, 3))
-    for s in srcs[:4]:
-        g.bfs(int(s), depth_out=host_depth)
+    g.bfs_many(src_list[:4], outs[:4])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        for s in srcs:
-            g.bfs(int(s), depth_out=host_depth)
+        g.bfs_many(src_list, outs)
     e2e_s = time.perf_counter() - t0
     _, _, e2e_rate = replicas.job_rate(edges_per_step * e2e_steps, e2e_s, dist, dev)
     e2e_value = e2e_rate / 1e9
+    e2e_rows_ok = bool(np.array_equal(outs[-1], depth_ref_last)) if depth_ref_last is not None else None
     if pinned:
         eb.host_unregister(host_depth)
 
@@ -279,8 +291,10 @@ def run_ours(args, rank, world, dist):
                             "algorithmic bytes 4*m_c + 8*n_c + 4*V",
         },
         "e2e": {"value": round(e2e_value, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),
-                "d2h_bytes_per_step": 4 * V * len(srcs), "api": "ent_bfs (C ABI) with host depth buffer",
-                "host_buffer_pinned": pinned},
+                "d2h_bytes_per_step": 4 * V * len(srcs),
+                "api": "ent_bfs_many (C ABI): every source's depths copied to a host row, "
+                       "the copy overlapping the next traversal",
+                "host_rows": rows, "host_buffer_pinned": pinned, "last_row_matches_device_run": e2e_rows_ok},
         "gpu_launches": launches,
         "clocks": clocks,
     }

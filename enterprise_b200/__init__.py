@@ -198,6 +198,7 @@ def lib() -> C.CDLL:
         "ent_graph_destroy": (C.c_int, [_P]),
         "ent_bfs": (C.c_int, [_P, C.c_int32, _I32P, _I32P, C.POINTER(_Stats)]),
         "ent_bfs_device": (C.c_int, [_P, C.c_int32, _P, _P, _P, C.POINTER(_Stats)]),
+        "ent_bfs_many": (C.c_int, [_P, _I32P, C.c_int32, C.POINTER(_P), C.POINTER(_Stats)]),
         "ent_bfs_trace": (C.c_int, [_P, C.c_int32, C.POINTER(_Trace), C.c_int32, _I32P, C.POINTER(_Stats)]),
         "ent_validate": (C.c_int, [_P, C.c_int32, _P, _P, _I32P, _I64P, _I32P, _I64P]),
         "ent_bfs_batch": (C.c_int, [_P, _I32P, C.c_int32, _I32P, C.POINTER(_Stats)]),
@@ -448,6 +449,27 @@ class Graph:
         _check(lib().ent_bfs(self.handle, int(src), _i32p(depth), _i32p(par) if par is not None else None,
                              C.byref(st)))
         return depth, par, Stats._from_c(st)
+
+    def bfs_many(self, srcs: Sequence[int], depth_outs: Sequence[Optional[np.ndarray]]) -> list:
+        """One BFS per source in order (``ent_bfs_many``), source i's depths
+        copied into host array depth_outs[i] (int32[V], None = no copy; an
+        array may repeat, the later source wins) while source i+1 traverses.
+        Returns the per-source Stats."""
+        V = self.vert_count
+        s = np.ascontiguousarray(srcs, dtype=np.int32)
+        if len(depth_outs) != len(s):
+            raise ValueError("one output entry per source")
+        ptrs = (_P * max(1, len(s)))()
+        for i, d in enumerate(depth_outs):
+            if d is None:
+                ptrs[i] = None
+                continue
+            if d.dtype != np.int32 or d.size != V or not d.flags["C_CONTIGUOUS"] or not d.flags["WRITEABLE"]:
+                raise ValueError(f"depth_outs[{i}] must be a writable contiguous int32 array of {V} entries")
+            ptrs[i] = d.ctypes.data
+        st = (_Stats * max(1, len(s)))()
+        _check(lib().ent_bfs_many(self.handle, _i32p(s), len(s), ptrs, st))
+        return [Stats._from_c(st[i]) for i in range(len(s))]
 
     def bfs_device(self, src: int, depth_ptr: int, parent_ptr: int = 0, stream: int = 0,
                    stats: bool = True) -> Optional[Stats]:

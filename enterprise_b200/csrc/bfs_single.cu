@@ -43,6 +43,7 @@
 //    whose body is [expand, inspect, if(narrow){narrow}]; the inspector sets
 //    both conditions.
 #include <algorithm>
+#include <vector>
 #include <string.h>
 
 #include <cooperative_groups.h>
@@ -1087,6 +1088,12 @@ struct BfsWorkspace {
   cudaGraphNode_t reset_node = nullptr;
   cudaGraphNode_t init_node = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // ent_bfs_many: a second depth buffer, a copy stream and pinned per-source
+  // copies of the control block (created on first use)
+  int32_t* depth_b = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  BfsCtl* many_ctl_h = nullptr;
+  int32_t many_cap = 0;
 };
 
 void destroy_bfs_workspace(BfsWorkspace* w) {
@@ -1100,6 +1107,9 @@ void destroy_bfs_workspace(BfsWorkspace* w) {
   if (w->parent) cudaFree(w->parent);
   if (w->ev0) cudaEventDestroy(w->ev0);
   if (w->ev1) cudaEventDestroy(w->ev1);
+  if (w->depth_b) cudaFree(w->depth_b);
+  if (w->copy_stream) cudaStreamDestroy(w->copy_stream);
+  if (w->many_ctl_h) cudaFreeHost(w->many_ctl_h);
   delete w;
 }
 
@@ -1528,6 +1538,109 @@ int ent_bfs(ent_graph* g, int32_t src, int32_t* depth_out, int32_t* parent_out, 
   if (parent_out)
     ENT_CUDA(cudaMemcpyAsync(parent_out, w->parent, sizeof(int32_t) * g->V, cudaMemcpyDeviceToHost, g->stream));
   ENT_CUDA(cudaStreamSynchronize(g->stream));
+  return ENT_OK;
+}
+
+// The reference's source loop (bfs_gpu_opt.cuh:370-431: per source, reset,
+// traverse, copy the depths to the host) as one call, pipelined: traversals
+// alternate between two device depth buffers on the graph's stream while a
+// copy stream moves the previous source's depths to its host array, so the
+// copy of source i overlaps the traversal of source i+1.
+int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const* depth_out, ent_stats* stats) {
+  clear_error();
+  if (!g) return fail(ENT_ERR_INVALID_ARG, "null graph");
+  if (n_src < 0) return fail(ENT_ERR_INVALID_ARG, "negative source count %d", n_src);
+  if (n_src > 0 && !src) return fail(ENT_ERR_INVALID_ARG, "null source list");
+  for (int32_t i = 0; i < n_src; ++i)
+    if (src[i] < 0 || src[i] >= g->V)
+      return fail(ENT_ERR_INVALID_ARG, "source %d (index %d) out of range [0,%lld)", src[i], i, (long long)g->V);
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard dg(g->device);
+  if (!g->ws) {
+    int rc = create_workspace(g, &g->ws);
+    if (rc != ENT_OK) return rc;
+  }
+  if (n_src == 0) return ENT_OK;
+  BfsWorkspace* w = g->ws;
+  if (!w->depth_b && cudaMalloc(&w->depth_b, sizeof(int32_t) * g->V) != cudaSuccess) {
+    w->depth_b = nullptr;
+    return fail(ENT_ERR_OOM, "second depth buffer (%lld bytes) failed", (long long)(sizeof(int32_t) * g->V));
+  }
+  if (!w->copy_stream) ENT_CUDA(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking));
+  if (w->many_cap < n_src) {
+    if (w->many_ctl_h) cudaFreeHost(w->many_ctl_h);
+    w->many_ctl_h = nullptr;
+    w->many_cap = 0;
+    if (cudaMallocHost(&w->many_ctl_h, sizeof(BfsCtl) * n_src) != cudaSuccess) {
+      w->many_ctl_h = nullptr;
+      return fail(ENT_ERR_OOM, "pinned control copies failed");
+    }
+    w->many_cap = n_src;
+  }
+  const cudaStream_t s = g->stream, cs = w->copy_stream;
+  // events: [2i] / [2i+1] bracket traversal i; the last two mark each depth
+  // buffer's latest copy as done
+  std::vector<cudaEvent_t> ev(2 * (size_t)n_src + 2, nullptr);
+  const auto destroy_events = [&]() {
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+  };
+  for (size_t k = 0; k < ev.size(); ++k) {
+    const unsigned flags = k < 2 * (size_t)n_src ? cudaEventDefault : cudaEventDisableTiming;
+    if (cudaEventCreateWithFlags(&ev[k], flags) != cudaSuccess) {
+      ev[k] = nullptr;
+      destroy_events();
+      return fail(ENT_ERR_CUDA, "event creation failed");
+    }
+  }
+  int32_t* buf[2] = {w->depth, w->depth_b};
+  cudaEvent_t freed[2] = {ev[2 * (size_t)n_src], ev[2 * (size_t)n_src + 1]};
+  bool copied[2] = {false, false};
+  const size_t bytes = sizeof(int32_t) * g->V;
+  int rc = ENT_OK;
+  cudaError_t ce = cudaSuccess;
+  int32_t done = 0;
+  for (int32_t i = 0; i < n_src && rc == ENT_OK && ce == cudaSuccess; ++i) {
+    const int b = i & 1;
+    if (copied[b]) ce = cudaStreamWaitEvent(s, freed[b], 0);  // source i-2's copy has read buf[b]
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev[2 * (size_t)i], s);
+    if (ce != cudaSuccess) break;
+    rc = run_bfs_single(g, src[i], buf[b], nullptr, s, nullptr);
+    if (rc != ENT_OK) break;
+    ce = cudaEventRecord(ev[2 * (size_t)i + 1], s);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(&w->many_ctl_h[i], w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess && depth_out && depth_out[i]) {
+      ce = cudaStreamWaitEvent(cs, ev[2 * (size_t)i + 1], 0);
+      if (ce == cudaSuccess) ce = cudaMemcpyAsync(depth_out[i], buf[b], bytes, cudaMemcpyDeviceToHost, cs);
+      if (ce == cudaSuccess) ce = cudaEventRecord(freed[b], cs);
+      copied[b] = true;
+    }
+    if (ce == cudaSuccess) done = i + 1;
+  }
+  const cudaError_t se = cudaStreamSynchronize(s);
+  const cudaError_t sc = cudaStreamSynchronize(cs);
+  if (rc == ENT_OK && ce == cudaSuccess) ce = se != cudaSuccess ? se : sc;
+  if (rc == ENT_OK && ce != cudaSuccess) {
+    destroy_events();
+    return fail(ENT_ERR_CUDA, "pipelined traversals: %s", cudaGetErrorString(ce));
+  }
+  int first_bad = -1;
+  for (int32_t i = 0; i < done; ++i) {
+    const BfsCtl& h = w->many_ctl_h[i];
+    ent_stats st;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[2 * (size_t)i], ev[2 * (size_t)i + 1]);
+    fill_stats(h, ms, &st);
+    if (g->opts.loop == ENT_LOOP_GRAPH) g_kernel_launches += st.launches - 2;
+    if (stats) stats[i] = st;
+    if (h.err && first_bad < 0) first_bad = i;
+  }
+  destroy_events();
+  if (rc != ENT_OK) return rc;
+  if (first_bad >= 0)
+    return fail(ENT_ERR_TIMEOUT, "traversal %d (source %d) reported error flags 0x%x", first_bad, src[first_bad],
+                w->many_ctl_h[first_bad].err);
   return ENT_OK;
 }
 

@@ -210,6 +210,16 @@ int ent_bfs(ent_graph* g, int32_t src, int32_t* depth_out, int32_t* parent_out,
  * own stream) unless stats is non-NULL, which synchronises. */
 int ent_bfs_device(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* parent_dev,
                    void* stream, ent_stats* stats);
+/* One traversal per source, in order, with each source's depths copied to a
+ * HOST array: the reference's per-source loop (bfs_gpu_opt.cuh:370-431:
+ * reset, traverse, depth D2H) as one call. depth_out[i] (V int32) receives
+ * source i's depths; an entry may be NULL (no copy) or repeat an earlier one
+ * (the later source's depths win). The copy of source i overlaps the
+ * traversal of source i+1, which needs page-locked host arrays to overlap
+ * (pageable ones still work, serialised). stats (n_src entries) may be NULL.
+ * Returns once every copy has landed. */
+int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const* depth_out,
+                 ent_stats* stats);
 
 /* Per-level trace of one traversal (tracing / profiling aid). Runs the level
  * loop host-driven with CUDA events around each kernel; depths are the same

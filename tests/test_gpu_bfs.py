@@ -128,6 +128,40 @@ def test_device_api_matches_host_api(eb, orc):
             assert st.reached_vertices == (exp >= 0).sum()
 
 
+@pytest.mark.parametrize("loop", ["graph", "host"])
+def test_many_sources_pipelined_to_host(eb, orc, loop):
+    """ent_bfs_many: every source's host array equals the oracle and the
+    single-call result; stats match; NULL entries skip the copy; a repeated
+    array holds the later source; pinned and pageable arrays both work."""
+    csr = eb.Csr.rmat(14, 16, seed=21)
+    srcs = [int(s) for s in eb.pick_sources(csr.beg_pos, 22, 9)]
+    V = csr.vert_count
+    with _graph(eb, csr, loop=loop) as g:
+        outs = [np.full(V, 7, dtype=np.int32) for _ in srcs]
+        pinned = outs[1]
+        eb.host_register(pinned)
+        try:
+            stats = g.bfs_many(srcs, outs)
+        finally:
+            eb.host_unregister(pinned)
+        for s, d, st in zip(srcs, outs, stats):
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, s)
+            np.testing.assert_array_equal(d, exp, err_msg=f"source {s}")
+            e, v = orc.report(csr.beg_pos, exp)
+            assert (st.traversed_edges, st.reached_vertices, st.status) == (e, v, 0)
+            assert st.levels == int(exp.max()) + 1
+            one = g.bfs(s)[2]
+            assert (one.traversed_edges, one.levels) == (st.traversed_edges, st.levels)
+        shared = np.full(V, 7, dtype=np.int32)
+        skipped = np.full(V, 7, dtype=np.int32)
+        g.bfs_many(srcs[:3], [shared, None, shared])
+        np.testing.assert_array_equal(shared, orc.bfs(csr.beg_pos, csr.csr, srcs[2])[0])
+        assert (skipped == 7).all()
+        assert g.bfs_many([], []) == []
+        with pytest.raises(eb.EntError):
+            g.bfs_many([srcs[0], V], [None, None])
+
+
 def test_repeated_traversals_are_independent(eb, orc):
     """State from one traversal never leaks into the next (bitmaps, queues, hubs)."""
     csr = eb.Csr.rmat(12, 16, seed=8)
