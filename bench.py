@@ -217,36 +217,44 @@ def run_ours(args, rank, world, dist):
     traffic = profiled_traffic("bfs_rmat_s24_traffic.txt") if args.scale == 24 else None  # bytes per traversal
 
     # ------------------------------------------------ e2e through the C ABI
-    # ent_bfs_many: the reference's per-source loop (traverse, copy the depths
-    # to the host) as one call, each source's depths landing in its own pinned
-    # host row; the copy of one source overlaps the next traversal.
+    # The reference's per-source loop (traverse, copy the depths to the host)
+    # as one call: ent_bfs_many_u8 returns the reference's own depth type (one
+    # byte per vertex, 255 = unreached); ent_bfs_many returns int32 depths.
+    # Each source's depths land in their own pinned host row; the copy of one
+    # source overlaps the next traversal.
     src_list = [int(s) for s in srcs]
-    rows = len(src_list)
-    try:
-        import psutil
-        if psutil.virtual_memory().available < 3 * rows * V * 4:
-            rows = 2  # not enough host memory for a row per source: alternate two rows
-    except Exception:
-        rows = 2
-    host_depth = np.empty((rows, V), dtype=np.int32)
-    try:
-        eb.host_register(host_depth)
-        pinned = True
-    except Exception:
-        pinned = False
-    outs = [host_depth[i % rows] for i in range(len(src_list))]
     e2e_steps = max(1, min(args.steps, 3))
-    g.bfs_many(src_list[:4], outs[:4])
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        g.bfs_many(src_list, outs)
-    e2e_s = time.perf_counter() - t0
-    _, _, e2e_rate = replicas.job_rate(edges_per_step * e2e_steps, e2e_s, dist, dev)
-    e2e_value = e2e_rate / 1e9
-    e2e_rows_ok = bool(np.array_equal(outs[-1], depth_ref_last)) if depth_ref_last is not None else None
-    if pinned:
-        eb.host_unregister(host_depth)
+
+    def e2e_run(dtype):
+        rows = len(src_list)
+        try:
+            import psutil
+            if psutil.virtual_memory().available < 3 * rows * V * np.dtype(dtype).itemsize:
+                rows = 2  # not enough host memory for a row per source: alternate two rows
+        except Exception:
+            rows = 2
+        host = np.empty((rows, V), dtype=dtype)
+        try:
+            eb.host_register(host)
+            pinned = True
+        except Exception:
+            pinned = False
+        outs = [host[i % rows] for i in range(len(src_list))]
+        g.bfs_many(src_list[:4], outs[:4])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            g.bfs_many(src_list, outs)
+        el = time.perf_counter() - t0
+        _, _, rate = replicas.job_rate(edges_per_step * e2e_steps, el, dist, dev)
+        want = depth_ref_last if dtype == np.int32 else np.where(depth_ref_last < 0, 255, depth_ref_last).astype(np.uint8)
+        ok = bool(np.array_equal(outs[-1], want))
+        if pinned:
+            eb.host_unregister(host)
+        return rate / 1e9, rows, pinned, ok
+
+    e2e_value, e2e_rows, pinned, e2e_ok = e2e_run(np.uint8)
+    e2e_i32, _, _, e2e_ok32 = e2e_run(np.int32)
 
     # ------------------------------------------- CPU baseline (rank 0, N=1)
     cpu = None
@@ -291,10 +299,12 @@ def run_ours(args, rank, world, dist):
                             "algorithmic bytes 4*m_c + 8*n_c + 4*V",
         },
         "e2e": {"value": round(e2e_value, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),
-                "d2h_bytes_per_step": 4 * V * len(srcs),
-                "api": "ent_bfs_many (C ABI): every source's depths copied to a host row, "
-                       "the copy overlapping the next traversal",
-                "host_rows": rows, "host_buffer_pinned": pinned, "last_row_matches_device_run": e2e_rows_ok},
+                "d2h_bytes_per_step": V * len(srcs),
+                "api": "ent_bfs_many_u8 (C ABI): every source's depths, in the reference's byte depth "
+                       "type, copied to a host row, the copy overlapping the next traversal",
+                "host_rows": e2e_rows, "host_buffer_pinned": pinned, "last_row_matches_device_run": e2e_ok,
+                "int32_depths": {"value": round(e2e_i32, 3), "api": "ent_bfs_many",
+                                 "d2h_bytes_per_step": 4 * V * len(srcs), "last_row_matches_device_run": e2e_ok32}},
         "gpu_launches": launches,
         "clocks": clocks,
     }

@@ -199,6 +199,7 @@ def lib() -> C.CDLL:
         "ent_bfs": (C.c_int, [_P, C.c_int32, _I32P, _I32P, C.POINTER(_Stats)]),
         "ent_bfs_device": (C.c_int, [_P, C.c_int32, _P, _P, _P, C.POINTER(_Stats)]),
         "ent_bfs_many": (C.c_int, [_P, _I32P, C.c_int32, C.POINTER(_P), C.POINTER(_Stats)]),
+        "ent_bfs_many_u8": (C.c_int, [_P, _I32P, C.c_int32, C.POINTER(_P), C.POINTER(_Stats)]),
         "ent_bfs_trace": (C.c_int, [_P, C.c_int32, C.POINTER(_Trace), C.c_int32, _I32P, C.POINTER(_Stats)]),
         "ent_validate": (C.c_int, [_P, C.c_int32, _P, _P, _I32P, _I64P, _I32P, _I64P]),
         "ent_bfs_batch": (C.c_int, [_P, _I32P, C.c_int32, _I32P, C.POINTER(_Stats)]),
@@ -451,24 +452,31 @@ class Graph:
         return depth, par, Stats._from_c(st)
 
     def bfs_many(self, srcs: Sequence[int], depth_outs: Sequence[Optional[np.ndarray]]) -> list:
-        """One BFS per source in order (``ent_bfs_many``), source i's depths
-        copied into host array depth_outs[i] (int32[V], None = no copy; an
-        array may repeat, the later source wins) while source i+1 traverses.
-        Returns the per-source Stats."""
+        """One BFS per source in order, source i's depths copied into host
+        array depth_outs[i] (None = no copy; an array may repeat, the later
+        source wins) while source i+1 traverses. int32[V] arrays take int32
+        depths (``ent_bfs_many``); uint8[V] arrays take the reference's byte
+        depths, 255 = unreached (``ent_bfs_many_u8``). Returns the per-source
+        Stats."""
         V = self.vert_count
         s = np.ascontiguousarray(srcs, dtype=np.int32)
         if len(depth_outs) != len(s):
             raise ValueError("one output entry per source")
+        kinds = {d.dtype for d in depth_outs if d is not None}
+        if len(kinds) > 1 or not kinds <= {np.dtype(np.int32), np.dtype(np.uint8)}:
+            raise ValueError("depth_outs must all be int32 or all uint8 arrays")
+        byte_rows = kinds == {np.dtype(np.uint8)}
         ptrs = (_P * max(1, len(s)))()
         for i, d in enumerate(depth_outs):
             if d is None:
                 ptrs[i] = None
                 continue
-            if d.dtype != np.int32 or d.size != V or not d.flags["C_CONTIGUOUS"] or not d.flags["WRITEABLE"]:
-                raise ValueError(f"depth_outs[{i}] must be a writable contiguous int32 array of {V} entries")
+            if d.size != V or not d.flags["C_CONTIGUOUS"] or not d.flags["WRITEABLE"]:
+                raise ValueError(f"depth_outs[{i}] must be a writable contiguous array of {V} entries")
             ptrs[i] = d.ctypes.data
         st = (_Stats * max(1, len(s)))()
-        _check(lib().ent_bfs_many(self.handle, _i32p(s), len(s), ptrs, st))
+        fn = lib().ent_bfs_many_u8 if byte_rows else lib().ent_bfs_many
+        _check(fn(self.handle, _i32p(s), len(s), ptrs, st))
         return [Stats._from_c(st[i]) for i in range(len(s))]
 
     def bfs_device(self, src: int, depth_ptr: int, parent_ptr: int = 0, stream: int = 0,

@@ -1069,6 +1069,26 @@ __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
   __threadfence();
 }
 
+// Packs int32 depths into the reference's byte format (depth_t = unsigned
+// char, comm.h:69): depth d (0..254) as d, unreached (-1) as 255 (INFTY,
+// comm.h:131). A thread packs 16 depths: four 16-byte loads, one 16-byte store.
+__global__ void __launch_bounds__(256) k_depth_u8(const int32_t* __restrict__ d, uint8_t* __restrict__ o, int64_t V) {
+  const auto pk = [](int x) { return (uint32_t)(x < 0 ? 255 : x) & 0xFFu; };
+  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 16;
+  if (i + 16 <= V) {  // both buffers are allocation bases and i % 16 == 0: 16-byte aligned
+    const int4* p = reinterpret_cast<const int4*>(d + i);
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int4 x = __ldcs(p + q);
+      w[q] = pk(x.x) | pk(x.y) << 8 | pk(x.z) << 16 | pk(x.w) << 24;
+    }
+    *reinterpret_cast<uint4*>(o + i) = make_uint4(w[0], w[1], w[2], w[3]);
+  } else {
+    for (int64_t j = i; j < V; ++j) o[j] = (uint8_t)pk(d[j]);
+  }
+}
+
 // ------------------------------------------------------------- host -------
 struct BfsWorkspace {
   int device = 0;
@@ -1091,6 +1111,7 @@ struct BfsWorkspace {
   // ent_bfs_many: a second depth buffer, a copy stream and pinned per-source
   // copies of the control block (created on first use)
   int32_t* depth_b = nullptr;
+  uint8_t* depth8[2] = {nullptr, nullptr};  // byte depths (ent_bfs_many_u8)
   cudaStream_t copy_stream = nullptr;
   BfsCtl* many_ctl_h = nullptr;
   int32_t many_cap = 0;
@@ -1108,6 +1129,8 @@ void destroy_bfs_workspace(BfsWorkspace* w) {
   if (w->ev0) cudaEventDestroy(w->ev0);
   if (w->ev1) cudaEventDestroy(w->ev1);
   if (w->depth_b) cudaFree(w->depth_b);
+  for (int i = 0; i < 2; ++i)
+    if (w->depth8[i]) cudaFree(w->depth8[i]);
   if (w->copy_stream) cudaStreamDestroy(w->copy_stream);
   if (w->many_ctl_h) cudaFreeHost(w->many_ctl_h);
   delete w;
@@ -1546,7 +1569,8 @@ int ent_bfs(ent_graph* g, int32_t src, int32_t* depth_out, int32_t* parent_out, 
 // alternate between two device depth buffers on the graph's stream while a
 // copy stream moves the previous source's depths to its host array, so the
 // copy of source i overlaps the traversal of source i+1.
-int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const* depth_out, ent_stats* stats) {
+static int bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, void* const* depth_out, bool bytes,
+                    ent_stats* stats) {
   clear_error();
   if (!g) return fail(ENT_ERR_INVALID_ARG, "null graph");
   if (n_src < 0) return fail(ENT_ERR_INVALID_ARG, "negative source count %d", n_src);
@@ -1566,6 +1590,11 @@ int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const
     w->depth_b = nullptr;
     return fail(ENT_ERR_OOM, "second depth buffer (%lld bytes) failed", (long long)(sizeof(int32_t) * g->V));
   }
+  for (int i = 0; bytes && i < 2; ++i)
+    if (!w->depth8[i] && cudaMalloc(&w->depth8[i], (size_t)g->V) != cudaSuccess) {
+      w->depth8[i] = nullptr;
+      return fail(ENT_ERR_OOM, "byte depth buffer (%lld bytes) failed", (long long)g->V);
+    }
   if (!w->copy_stream) ENT_CUDA(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking));
   if (w->many_cap < n_src) {
     if (w->many_ctl_h) cudaFreeHost(w->many_ctl_h);
@@ -1578,9 +1607,9 @@ int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const
     w->many_cap = n_src;
   }
   const cudaStream_t s = g->stream, cs = w->copy_stream;
-  // events: [2i] / [2i+1] bracket traversal i; the last two mark each depth
-  // buffer's latest copy as done
-  std::vector<cudaEvent_t> ev(2 * (size_t)n_src + 2, nullptr);
+  // events: [2i] / [2i+1] bracket traversal i; the next two mark each depth
+  // buffer's latest copy as done, the last one that a byte row is packed
+  std::vector<cudaEvent_t> ev(2 * (size_t)n_src + 3, nullptr);
   const auto destroy_events = [&]() {
     for (cudaEvent_t e : ev)
       if (e) cudaEventDestroy(e);
@@ -1595,8 +1624,10 @@ int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const
   }
   int32_t* buf[2] = {w->depth, w->depth_b};
   cudaEvent_t freed[2] = {ev[2 * (size_t)n_src], ev[2 * (size_t)n_src + 1]};
+  const cudaEvent_t packed = ev[2 * (size_t)n_src + 2];
   bool copied[2] = {false, false};
-  const size_t bytes = sizeof(int32_t) * g->V;
+  const size_t row_bytes = (bytes ? 1 : sizeof(int32_t)) * g->V;
+  const unsigned pack_grid = (unsigned)((g->V + 16 * 256 - 1) / (16 * 256));
   int rc = ENT_OK;
   cudaError_t ce = cudaSuccess;
   int32_t done = 0;
@@ -1611,8 +1642,18 @@ int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const
     if (ce == cudaSuccess)
       ce = cudaMemcpyAsync(&w->many_ctl_h[i], w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s);
     if (ce == cudaSuccess && depth_out && depth_out[i]) {
-      ce = cudaStreamWaitEvent(cs, ev[2 * (size_t)i + 1], 0);
-      if (ce == cudaSuccess) ce = cudaMemcpyAsync(depth_out[i], buf[b], bytes, cudaMemcpyDeviceToHost, cs);
+      const void* from = buf[b];
+      cudaEvent_t ready = ev[2 * (size_t)i + 1];
+      if (bytes) {  // pack on the traversal stream; buf[b] is reused only after this
+        k_depth_u8<<<pack_grid, 256, 0, s>>>(buf[b], w->depth8[b], g->V);
+        g_kernel_launches += 1;
+        ce = cudaGetLastError();
+        if (ce == cudaSuccess) ce = cudaEventRecord(packed, s);
+        from = w->depth8[b];
+        ready = packed;
+      }
+      if (ce == cudaSuccess) ce = cudaStreamWaitEvent(cs, ready, 0);
+      if (ce == cudaSuccess) ce = cudaMemcpyAsync(depth_out[i], from, row_bytes, cudaMemcpyDeviceToHost, cs);
       if (ce == cudaSuccess) ce = cudaEventRecord(freed[b], cs);
       copied[b] = true;
     }
@@ -1625,7 +1666,7 @@ int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const
     destroy_events();
     return fail(ENT_ERR_CUDA, "pipelined traversals: %s", cudaGetErrorString(ce));
   }
-  int first_bad = -1;
+  int first_bad = -1, first_deep = -1;
   for (int32_t i = 0; i < done; ++i) {
     const BfsCtl& h = w->many_ctl_h[i];
     ent_stats st;
@@ -1635,13 +1676,28 @@ int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const
     if (g->opts.loop == ENT_LOOP_GRAPH) g_kernel_launches += st.launches - 2;
     if (stats) stats[i] = st;
     if (h.err && first_bad < 0) first_bad = i;
+    if (bytes && st.levels > 255 && first_deep < 0) first_deep = i;
   }
   destroy_events();
   if (rc != ENT_OK) return rc;
   if (first_bad >= 0)
     return fail(ENT_ERR_TIMEOUT, "traversal %d (source %d) reported error flags 0x%x", first_bad, src[first_bad],
                 w->many_ctl_h[first_bad].err);
+  if (first_deep >= 0)
+    return fail(ENT_ERR_UNSUPPORTED, "source %d (index %d) reaches depth %d; byte depths hold 0..254",
+                src[first_deep], first_deep, w->many_ctl_h[first_deep].level - 1);
   return ENT_OK;
+}
+
+int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const* depth_out, ent_stats* stats) {
+  return bfs_many(g, src, n_src, reinterpret_cast<void* const*>(depth_out), false, stats);
+}
+
+// The same loop returning the reference's own depth type: one byte per vertex
+// (depth_t, comm.h:69; 255 = unreached, comm.h:131), a quarter of the bytes
+// to copy to the host.
+int ent_bfs_many_u8(ent_graph* g, const int32_t* src, int32_t n_src, uint8_t* const* depth_out, ent_stats* stats) {
+  return bfs_many(g, src, n_src, reinterpret_cast<void* const*>(depth_out), true, stats);
 }
 
 }  // extern "C"

@@ -220,6 +220,14 @@ int ent_bfs_device(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* paren
  * Returns once every copy has landed. */
 int ent_bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* const* depth_out,
                  ent_stats* stats);
+/* The same loop with the reference's own depth type: depth_out[i] is a HOST
+ * array of V bytes (depth_t = unsigned char, comm.h:69), depth d as d and
+ * unreached as 255 (INFTY, comm.h:131), a quarter of the bytes to copy. The
+ * reference wraps depths above 254 around; here a source whose traversal
+ * goes deeper returns ENT_ERR_UNSUPPORTED (its row then holds the low byte
+ * of each depth; the other sources' rows are complete). */
+int ent_bfs_many_u8(ent_graph* g, const int32_t* src, int32_t n_src, uint8_t* const* depth_out,
+                    ent_stats* stats);
 
 /* Per-level trace of one traversal (tracing / profiling aid). Runs the level
  * loop host-driven with CUDA events around each kernel; depths are the same

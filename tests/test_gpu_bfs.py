@@ -162,6 +162,30 @@ def test_many_sources_pipelined_to_host(eb, orc, loop):
             g.bfs_many([srcs[0], V], [None, None])
 
 
+def test_many_sources_byte_depths(eb, orc):
+    """ent_bfs_many_u8: the reference's byte depths (255 = unreached) equal
+    the oracle's depths; a traversal deeper than 254 levels is refused while
+    the other sources' rows are still written."""
+    csr = eb.Csr.rmat(13, 8, seed=23)  # isolated vertices give 255 entries
+    srcs = [int(s) for s in eb.pick_sources(csr.beg_pos, 24, 5)]
+    V = csr.vert_count
+    with eb.Graph.from_csr(csr) as g:
+        outs = [np.zeros(V, dtype=np.uint8) for _ in srcs]
+        stats = g.bfs_many(srcs, outs)
+        for s, d, st in zip(srcs, outs, stats):
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, s)
+            np.testing.assert_array_equal(d, np.where(exp < 0, 255, exp).astype(np.uint8))
+            assert st.reached_vertices == (exp >= 0).sum()
+    n = 300  # a path: depths up to 299
+    path = eb.Csr.from_edges(np.arange(n - 1), np.arange(1, n), n)
+    with eb.Graph.from_csr(path) as g:
+        near, far = np.zeros(n, dtype=np.uint8), np.zeros(n, dtype=np.uint8)
+        with pytest.raises(eb.EntError, match="byte depths"):
+            g.bfs_many([150, 0], [near, far])
+        exp, _ = orc.bfs(path.beg_pos, path.csr, 150)
+        np.testing.assert_array_equal(near, exp.astype(np.uint8))
+
+
 def test_repeated_traversals_are_independent(eb, orc):
     """State from one traversal never leaks into the next (bitmaps, queues, hubs)."""
     csr = eb.Csr.rmat(12, 16, seed=8)
