@@ -359,7 +359,7 @@ def run_batched(args):
         tuned = {"batch_alpha": opts.batch_alpha, "batch_small_max": opts.batch_small_max,
                  "batch_large_min": opts.batch_large_min, "batch_heavy": opts.batch_heavy, "cached": hit}
         out["autotuned"] = tuned
-    for n in (64, 256, 1024):
+    for n in [int(x) for x in args.batch_sizes.split(",")]:
         dd = torch.empty((n, V), dtype=torch.int32, device="cuda")
         times, edges = [], 0
         for rep in range(4):
@@ -373,8 +373,12 @@ def run_batched(args):
                             "levels": stb[0].td_levels + stb[0].bu_levels}
         del dd
         torch.cuda.empty_cache()
-    out["batch_256_vs_sequential_256"] = round(out["sequential_256"]["ms"] / out["batch_256"]["ms"], 3)
+    if "batch_256" in out:
+        out["batch_256_vs_sequential_256"] = round(out["sequential_256"]["ms"] / out["batch_256"]["ms"], 3)
     g.close()
+    if args.no_multi:
+        torch.cuda.empty_cache()
+        return out
     # 48 graphs of uneven sizes, 64 sources each, one launch
     rng = np.random.default_rng(0x48)
     graphs, sources, total_v = [], [], 0
@@ -698,6 +702,8 @@ def main():
                     help="level loop driver; host launches each kernel (profilers can see them)")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")
     ap.add_argument("--batch-scale", type=int, default=22)
+    ap.add_argument("--batch-sizes", default="64,256,1024", help="sources per batch in the batched leg")
+    ap.add_argument("--no-multi", action="store_true", help="skip the 48-graph launch of the batched leg")
     ap.add_argument("--serve-seconds", type=float, default=10.0, help="serving run length (config: 60)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-batch", type=int, default=64)
