@@ -14,6 +14,10 @@
 //   --policy P      beamer | reference | td | bu
 //   --loop L        graph | host
 //   --gpu G         device id (default 0, as main.cu:49)
+//   --batch [N]     run the sources as bitwise multi-source batches of up to N
+//                   (default 64) sources, one launch per batch
+// The csr file may hold int64 (the reference's format) or int32 ids: the
+// width follows from its size against beg_pos[V].
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -30,7 +34,7 @@ int main(int argc, char** argv) {
     return -1;
   }
   long long seed = -1;
-  int n_sources = 64, gpu = 0;
+  int n_sources = 64, gpu = 0, batch = 0;
   const char* json_path = nullptr;
   ent_bfs_opts opts;
   ent_bfs_opts_default(&opts);
@@ -47,6 +51,14 @@ int main(int argc, char** argv) {
     else if (a == "--sources") n_sources = atoi(need("--sources"));
     else if (a == "--json") json_path = need("--json");
     else if (a == "--gpu") gpu = atoi(need("--gpu"));
+    else if (a == "--batch") {
+      batch = 64;
+      if (i + 1 < argc && argv[i + 1][0] != '-') batch = atoi(argv[++i]);
+      if (batch < 1) {
+        printf("Wrong input: --batch needs a positive size\n");
+        return -1;
+      }
+    }
     else if (a == "--policy") {
       std::string p = need("--policy");
       if (p == "beamer") opts.policy = ENT_POLICY_BEAMER;
@@ -96,6 +108,7 @@ int main(int argc, char** argv) {
   }
   ent_compat::RunOptions ro;
   ro.n_sources = n_sources;
+  ro.batch = batch;
   ro.opts = &opts;
   ro.json = jf;
   rc = ent_compat::run(src.data(), beg, ent_csr_adj(g), V, E, gpu, ro);

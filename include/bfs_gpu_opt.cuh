@@ -35,6 +35,9 @@ struct RunOptions {
   const ent_bfs_opts* opts = nullptr;
   FILE* json = nullptr;        /* optional machine-readable per-source lines */
   int check_samples = 64;      /* reached vertices checked per source */
+  int batch = 0;               /* > 0: run the sources as bitwise batches of up to this many
+                                  (ent_bfs_batch, one launch per batch); each source's time
+                                  line shows its batch's time divided by the batch's sources */
 };
 
 /* Local depth rule on one reached vertex b: every neighbour c has
@@ -70,30 +73,23 @@ inline int run(const int32_t* src_list, const int64_t* beg_pos, const int32_t* c
     return 1;
   }
   printf("In gpu bfs\n");
-  std::vector<int32_t> depth((size_t)vert_count);
   double average_teps = 0.0, inv_sum = 0.0;
   int64_t validate_count = 0;
   int failures = 0;
   uint64_t rng = 0x9E3779B97F4A7C15ull;
-  for (int i = 0; i < ro.n_sources; ++i) {
+  /* the reference's per-source block (bfs_gpu_opt.cuh:372-431) for source i */
+  const auto report = [&](int i, const ent_stats& st, const int32_t* depth, double tm) {
     printf("Test %d\n", i + 1);
     printf("Started from: %d\n", src_list[i]);
-    ent_stats st;
-    if (ent_bfs(g, src_list[i], depth.data(), nullptr, &st) != ENT_OK) {
-      printf("BFS failed: %s\n", ent_last_error());
-      ent_graph_destroy(g);
-      return 1;
-    }
     if (st.levels > 2) {
       ++validate_count;
-      const double tm = st.device_ms * 1e-3;
       /* sampled local checks on reached vertices */
       int ret = 0;
       for (int k = 0; k < ro.check_samples && ret == 0; ++k) {
         for (int tries = 0; tries < 1000; ++tries) {
           rng ^= rng << 13; rng ^= rng >> 7; rng ^= rng << 17;
           int64_t b = (int64_t)(rng % (uint64_t)vert_count);
-          if (depth[b] >= 0) { ret = local_check(beg_pos, csr, depth.data(), b); break; }
+          if (depth[b] >= 0) { ret = local_check(beg_pos, csr, depth, b); break; }
         }
       }
       if (ret != 0) ++failures;
@@ -108,13 +104,40 @@ inline int run(const int32_t* src_list, const int64_t* beg_pos, const int32_t* c
       if (ro.json)
         fprintf(ro.json,
                 "{\"source\": %d, \"levels\": %d, \"td_levels\": %d, \"bu_levels\": %d, \"reached\": %lld, "
-                "\"edges\": %lld, \"ms\": %.6f, \"gteps\": %.6f, \"check\": %d}\n",
+                "\"edges\": %lld, \"ms\": %.6f, \"gteps\": %.6f, \"check\": %d, \"batched\": %s}\n",
                 src_list[i], st.levels, st.td_levels, st.bu_levels, (long long)st.reached_vertices,
-                (long long)st.traversed_edges, st.device_ms, curr_teps, ret);
+                (long long)st.traversed_edges, tm * 1e3, curr_teps, ret, ro.batch > 0 ? "true" : "false");
     } else {
       printf("Traverse depth is %d\n", st.levels);
     }
     printf("\n====================================\n");
+  };
+  if (ro.batch > 0) {
+    for (int first = 0; first < ro.n_sources; first += ro.batch) {
+      const int k = ro.n_sources - first < ro.batch ? ro.n_sources - first : ro.batch;
+      std::vector<int32_t> rows((size_t)k * (size_t)vert_count);
+      std::vector<ent_stats> st((size_t)k);
+      if (ent_bfs_batch(g, src_list + first, k, rows.data(), st.data()) != ENT_OK) {
+        printf("BFS failed: %s\n", ent_last_error());
+        ent_graph_destroy(g);
+        return 1;
+      }
+      const double tm = st[0].device_ms * 1e-3 / k;  /* the batch's time, shared by its sources */
+      for (int j = 0; j < k; ++j) report(first + j, st[j], rows.data() + (size_t)j * (size_t)vert_count, tm);
+    }
+  } else {
+    std::vector<int32_t> depth((size_t)vert_count);
+    for (int i = 0; i < ro.n_sources; ++i) {
+      ent_stats st;
+      if (ent_bfs(g, src_list[i], depth.data(), nullptr, &st) != ENT_OK) {
+        printf("Test %d\n", i + 1);
+        printf("Started from: %d\n", src_list[i]);
+        printf("BFS failed: %s\n", ent_last_error());
+        ent_graph_destroy(g);
+        return 1;
+      }
+      report(i, st, depth.data(), st.device_ms * 1e-3);
+    }
   }
   printf("Final Average TEPS (Billion): %g\n", average_teps);
   if (validate_count) printf("Harmonic Mean TEPS (Billion): %g\n", validate_count / inv_sum);

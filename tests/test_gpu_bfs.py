@@ -209,3 +209,15 @@ def test_cli_end_to_end(eb, orc, tmp_path):
     assert "Final Average TEPS (Billion):" in r.stdout
     assert r.stdout.count("BFS result validation: CORRECT") + r.stdout.count("Traverse depth is") == 8
     assert "WRONG" not in r.stdout
+    # --batch: the same sources as bitwise batches of 3; same per-source edges and reach
+    jb = tmp_path / "batch.jsonl"
+    r = subprocess.run([eb.CLI_PATH, bp, cp, "--sources", "8", "--batch", "3", "--json", str(jb)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "WRONG" not in r.stdout and "Final Average TEPS (Billion):" in r.stdout
+    import json
+    one = [json.loads(x) for x in js.read_text().splitlines()]
+    bat = [json.loads(x) for x in jb.read_text().splitlines()]
+    assert [(x["source"], x["edges"], x["reached"], x["levels"]) for x in one] == \
+           [(x["source"], x["edges"], x["reached"], x["levels"]) for x in bat]
+    assert all(x["batched"] for x in bat) and not any(x["batched"] for x in one)
