@@ -25,9 +25,15 @@
 //    single-source traversal runs its small frontiers inside one
 //    thread-block cluster, so several queries proceed side by side on
 //    different SMs and each finishes as soon as its own traversal does.
-//  * Batched slots run on the highest stream priority and single-source slots
-//    on the lowest, so that the block scheduler hands freed SMs to batch
-//    kernels before the next cluster of a deep graph's traversal.
+//  * Every other graph also has fast_slots single-source slots, listed before
+//    its batched slots. They take the graph's queries while at most
+//    fast_max_waiting wait: one direction-optimising traversal per query ends
+//    sooner than a bitwise batch of a few, whose levels each sweep every
+//    vertex. When more wait, the batched slots take them.
+//  * Batched and fast slots run on the highest stream priority and the
+//    single-source slots of deep graphs on the lowest, so that the block
+//    scheduler hands freed SMs to them before the next cluster of a deep
+//    graph's traversal.
 //  * Latency = submit to the scheduler observing completion (poll granularity
 //    tens of microseconds); queue time = submit to launch.
 #include <algorithm>
@@ -66,6 +72,7 @@ struct Slot {
   int32_t* row_map_dev = nullptr;
   std::vector<int64_t> qids;
   bool busy = false;
+  bool fast = false;                   // single-source slot of a shallow graph
 };
 
 struct GraphState {
@@ -170,6 +177,8 @@ bool launch(ent_server* s) {
       {
         std::lock_guard<std::mutex> lk(s->mu);
         if (g.pending.empty() || g.free_rows.empty()) break;
+        // a fast slot takes queries only while few wait; else the batched slots do
+        if (sl.fast && g.pending.size() > (size_t)s->opts.fast_max_waiting) continue;
         const int cap = sl.sws ? 1 : batch_max_sources(sl.ws);
         const int take = (int)std::min<size_t>({(size_t)s->opts.max_batch, (size_t)cap, g.pending.size(),
                                                 g.free_rows.size()});
@@ -188,6 +197,7 @@ bool launch(ent_server* s) {
         }
         s->ctr.batches += 1;
         s->ctr.launched += take;
+        if (sl.fast) s->ctr.fast_launches += take;
         if (take > s->ctr.max_batch_seen) s->ctr.max_batch_seen = take;
       }
       const int n = (int)src.size();
@@ -252,6 +262,8 @@ void ent_server_opts_default(ent_server_opts* o) {
   o->hbm_budget_bytes = 0;
   o->single_source_levels = 64;
   o->single_slots = 8;
+  o->fast_slots = 2;
+  o->fast_max_waiting = 2;
 }
 
 // Depth of one traversal of g from its first non-isolated vertex (0 if the
@@ -285,6 +297,8 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
   if (o.max_pending < 1) return fail(ENT_ERR_INVALID_ARG, "max_pending must be >= 1");
   if (o.single_source_levels < 0) return fail(ENT_ERR_INVALID_ARG, "single_source_levels must be >= 0");
   if (o.single_slots < 1 || o.single_slots > 64) return fail(ENT_ERR_INVALID_ARG, "single_slots must be 1..64");
+  if (o.fast_slots < 0 || o.fast_slots > 16) return fail(ENT_ERR_INVALID_ARG, "fast_slots must be 0..16");
+  if (o.fast_max_waiting < 1) return fail(ENT_ERR_INVALID_ARG, "fast_max_waiting must be >= 1");
   const int dev = graphs[0]->device;
   for (int k = 0; k < n_graphs; ++k)
     if (!graphs[k] || graphs[k]->device != dev) return fail(ENT_ERR_INVALID_ARG, "all graphs must be on one GPU");
@@ -344,8 +358,27 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
       }
       continue;
     }
-    g.slots.resize(o.slots_per_graph);
-    for (Slot& sl : g.slots) {
+    g.slots.resize((size_t)o.fast_slots + o.slots_per_graph);
+    for (int f = 0; f < o.fast_slots; ++f) {
+      Slot& sl = g.slots[f];
+      sl.fast = true;
+      int rc;
+      {
+        std::lock_guard<std::mutex> lk(g.g->mu);
+        rc = create_bfs_workspace(g.g, &sl.sws);
+      }
+      if (rc == ENT_OK) {
+        cudaError_t e2 = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio_high);
+        if (e2 == cudaSuccess) e2 = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+        if (e2 != cudaSuccess) rc = fail(ENT_ERR_CUDA, "slot setup: %s", cudaGetErrorString(e2));
+      }
+      if (rc != ENT_OK) {
+        free_server(s);
+        return rc;
+      }
+    }
+    for (size_t b = (size_t)o.fast_slots; b < g.slots.size(); ++b) {
+      Slot& sl = g.slots[b];
       int rc = create_batch_workspace(g.g, o.max_batch, &sl.ws);
       if (rc == ENT_OK) {
         cudaError_t e2 = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio_high);

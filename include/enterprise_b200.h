@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define ENT_ABI_VERSION 3
+#define ENT_ABI_VERSION 4
 
 enum ent_status {
   ENT_OK = 0,
@@ -350,6 +350,12 @@ typedef struct ent_server_opts {
                                    source per launch (default 64, 0 = never)    */
   int32_t single_slots;     /* concurrent single-source traversals per such graph,
                                1..64 (default 8)                                 */
+  int32_t fast_slots;       /* single-source slots of every other graph, 0..16
+                               (default 2, 0 = none): they take the graph's
+                               queries while at most fast_max_waiting wait, where
+                               one direction-optimising traversal per query beats
+                               a bitwise batch of a few                          */
+  int32_t fast_max_waiting; /* default 2                                          */
 } ent_server_opts;
 typedef struct ent_query_result {
   int64_t query_id;
@@ -366,6 +372,7 @@ typedef struct ent_server_counters {
   int64_t submitted, rejected, completed, released, batches, launched, pending, rows_total, rows_free;
   int32_t max_batch_seen;
   int32_t single_graphs;    /* graphs served one source per launch */
+  int64_t fast_launches;    /* queries run on the fast single-source slots of the other graphs */
 } ent_server_counters;
 void ent_server_opts_default(ent_server_opts* opts);
 int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_server_opts* opts,

@@ -210,3 +210,31 @@ def test_single_source_slots_admission_by_memory(eb, orc):
                 break
         assert got == len(ids)
     g.close()
+
+
+def test_fast_slots_take_lone_queries(eb, orc):
+    """On a shallow graph, queries that arrive one at a time run on the fast
+    single-source slots; a burst goes to the batched slots; the depths are the
+    same either way, and with fast_slots=0 every query is batched."""
+    csr = eb.Csr.rmat(12, 16, seed=91)
+    g = eb.Graph.from_csr(csr)
+    srcs = [int(s) for s in eb.pick_sources(csr.beg_pos, 92, 24)]
+    for fast in (2, 0):
+        with eb.Server([g], max_batch=16, slots_per_graph=1, fast_slots=fast, fast_max_waiting=2) as srv:
+            for s in srcs[:6]:  # one at a time
+                q = srv.submit(0, s)
+                (r,) = _drain(srv, 1)
+                assert r["query_id"] == q and r["status"] == 0
+                np.testing.assert_array_equal(srv.depth(q), orc.bfs(csr.beg_pos, csr.csr, s)[0])
+                srv.release(q)
+            ids = {srv.submit(0, s): s for s in srcs[6:]}  # a burst
+            for r in _drain(srv, len(ids)):
+                np.testing.assert_array_equal(srv.depth(r["query_id"]),
+                                              orc.bfs(csr.beg_pos, csr.csr, ids[r["query_id"]])[0])
+                srv.release(r["query_id"])
+            c = srv.counters()
+            if fast:
+                assert c["fast_launches"] >= 6 and c["max_batch_seen"] > 1
+            else:
+                assert c["fast_launches"] == 0
+    g.close()
