@@ -548,7 +548,8 @@ def run_serving(args):
     sample_every = max(1, n_q // 40)
     checks, bad_status, mismatches = 0, 0, []
     graph_of = {}
-    with eb.Server(graphs, max_batch=args.serve_batch, slots_per_graph=args.serve_slots) as srv:
+    with eb.Server(graphs, max_batch=args.serve_batch, slots_per_graph=args.serve_slots,
+                   single_cluster=args.serve_cluster) as srv:
         t0 = time.perf_counter()
         i = 0
         while done < n_q:
@@ -594,7 +595,7 @@ def run_serving(args):
             "batches": c["batches"], "mean_batch": round(c["launched"] / max(1, c["batches"]), 2),
             "max_batch_seen": c["max_batch_seen"], "samples_checked": checks,
             "sampled_exact": not mismatches and bad_status == 0, "bad_status": bad_status,
-            "mismatches": mismatches[:5], "max_batch": args.serve_batch, "slots_per_graph": args.serve_slots,
+            "mismatches": mismatches[:5], "max_batch": args.serve_batch, "slots_per_graph": args.serve_slots, "single_cluster": args.serve_cluster,
             "single_source_graphs": c["single_graphs"],
             "by_class": {k: {"queries": len(v),
                              "p50_ms": round(float(np.percentile(v, 50)), 3) if v else None,
@@ -708,6 +709,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--serve-slots", type=int, default=1)
+    ap.add_argument("--serve-cluster", type=int, default=8,
+                    help="CTAs per small-frontier cluster of the deep graphs' single-source slots")
     ap.add_argument("--deep-graphs", default="grid,er", help="graphs of the high-diameter/uniform leg")
     ap.add_argument("--deep-sources", type=int, default=32)
     ap.add_argument("--ingest-scale", type=int, default=24)

@@ -18,7 +18,8 @@ int batch_max_sources(const BatchWorkspace* w);
 
 // Single-source traversal state with its own instantiated CUDA graph
 // (independent of the graph's own workspace, so several run concurrently).
-int create_bfs_workspace(ent_graph* g, BfsWorkspace** out);
+// cluster > 0 sets the CTAs of its small-frontier cluster (else the graph's option).
+int create_bfs_workspace(ent_graph* g, BfsWorkspace** out, int32_t cluster = 0);
 // Launches one traversal from src writing depth_dev (V int32) on stream s; async.
 int launch_bfs_single(BfsWorkspace* w, int32_t src, int32_t* depth_dev, cudaStream_t s);
 // Statistics of w's last traversal once it finished (copies on s, synchronises).

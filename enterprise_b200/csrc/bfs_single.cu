@@ -1253,7 +1253,7 @@ static int pick_narrow_cluster(int limit, size_t smem) {
   return 0;
 }
 
-static int create_workspace(ent_graph* g, BfsWorkspace** out, bool force_graph = false) {
+static int create_workspace(ent_graph* g, BfsWorkspace** out, bool force_graph = false, int32_t cluster = 0) {
   BfsWorkspace* w = new BfsWorkspace();
   w->device = g->device;
   w->V = g->V;
@@ -1330,7 +1330,8 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out, bool force_graph =
   w->grid_inspect = g->num_sms * std::min(occ_i, 4);
   w->grid_reset = g->num_sms * 4;
   w->smem_narrow = 2 * NQCAP * sizeof(int4);
-  w->narrow_nc = o.narrow_max_frontier > 0 ? pick_narrow_cluster(o.narrow_cluster, w->smem_narrow) : 0;
+  w->narrow_nc =
+      o.narrow_max_frontier > 0 ? pick_narrow_cluster(cluster > 0 ? cluster : o.narrow_cluster, w->smem_narrow) : 0;
   if (w->narrow_nc > 0) {
     a.narrow_f = std::min(o.narrow_max_frontier, w->narrow_nc * NQCAP / 2);
     a.exit_f = 2 * a.narrow_f;
@@ -1346,7 +1347,9 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out, bool force_graph =
   return ENT_OK;
 }
 
-int create_bfs_workspace(ent_graph* g, BfsWorkspace** out) { return create_workspace(g, out, true); }
+int create_bfs_workspace(ent_graph* g, BfsWorkspace** out, int32_t cluster) {
+  return create_workspace(g, out, true, cluster);
+}
 
 static void fill_stats(const BfsCtl& h, float ms, ent_stats* stats) {
   stats->reached_vertices = h.n_vis;

@@ -30,6 +30,10 @@
 //    fast_max_waiting wait: one direction-optimising traversal per query ends
 //    sooner than a bitwise batch of a few, whose levels each sweep every
 //    vertex. When more wait, the batched slots take them.
+//  * The single-source slots of deep graphs run their small frontiers in
+//    clusters of single_cluster CTAs (8 by default, where a lone traversal
+//    would take the largest cluster, 16): with several deep queries in
+//    flight, smaller clusters leave SMs to the others and to the batches.
 //  * Batched and fast slots run on the highest stream priority and the
 //    single-source slots of deep graphs on the lowest, so that the block
 //    scheduler hands freed SMs to them before the next cluster of a deep
@@ -264,6 +268,8 @@ void ent_server_opts_default(ent_server_opts* o) {
   o->single_slots = 8;
   o->fast_slots = 2;
   o->fast_max_waiting = 2;
+  o->single_cluster = 8;
+  o->pad = 0;
 }
 
 // Depth of one traversal of g from its first non-isolated vertex (0 if the
@@ -299,6 +305,7 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
   if (o.single_slots < 1 || o.single_slots > 64) return fail(ENT_ERR_INVALID_ARG, "single_slots must be 1..64");
   if (o.fast_slots < 0 || o.fast_slots > 16) return fail(ENT_ERR_INVALID_ARG, "fast_slots must be 0..16");
   if (o.fast_max_waiting < 1) return fail(ENT_ERR_INVALID_ARG, "fast_max_waiting must be >= 1");
+  if (o.single_cluster < 0 || o.single_cluster > 16) return fail(ENT_ERR_INVALID_ARG, "single_cluster must be 0..16");
   const int dev = graphs[0]->device;
   for (int k = 0; k < n_graphs; ++k)
     if (!graphs[k] || graphs[k]->device != dev) return fail(ENT_ERR_INVALID_ARG, "all graphs must be on one GPU");
@@ -344,7 +351,7 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
         int rc;
         {
           std::lock_guard<std::mutex> lk(g.g->mu);
-          rc = create_bfs_workspace(g.g, &sl.sws);
+          rc = create_bfs_workspace(g.g, &sl.sws, o.single_cluster);
         }
         if (rc == ENT_OK) {
           cudaError_t e2 = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio_low);

@@ -356,6 +356,10 @@ typedef struct ent_server_opts {
                                one direction-optimising traversal per query beats
                                a bitwise batch of a few                          */
   int32_t fast_max_waiting; /* default 2                                          */
+  int32_t single_cluster;   /* CTAs per small-frontier cluster of the deep graphs'
+                               single-source slots, 0..16 (default 8; 0 = each
+                               graph's own narrow_cluster option)                */
+  int32_t pad;
 } ent_server_opts;
 typedef struct ent_query_result {
   int64_t query_id;

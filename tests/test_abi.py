@@ -41,7 +41,7 @@ def test_struct_layout_matches_header(eb):
     import ctypes
     assert ctypes.sizeof(eb._Opts) == 4 + 4 + 8 * 3 + 4 * 5 + 4 + 8 + 4 * 8
     assert ctypes.sizeof(eb._Stats) == 8 + 8 + 4 * 4 + 8 + 4 * 2
-    assert ctypes.sizeof(eb._ServerOpts) == 4 * 4 + 8 + 4 * 4
+    assert ctypes.sizeof(eb._ServerOpts) == 4 * 4 + 8 + 4 * 6
     assert ctypes.sizeof(eb._ServerCounters) == 8 * 9 + 4 * 2 + 8
 
 
@@ -50,7 +50,7 @@ def test_server_option_defaults(eb):
     c = eb._ServerOpts()
     eb.lib().ent_server_opts_default(ctypes.byref(c))
     assert (c.max_batch, c.slots_per_graph, c.single_source_levels, c.single_slots) == (64, 2, 64, 8)
-    assert (c.fast_slots, c.fast_max_waiting) == (2, 2)
+    assert (c.fast_slots, c.fast_max_waiting, c.single_cluster) == (2, 2, 8)
 
 
 def test_invalid_arguments_return_status(eb):
