@@ -1115,6 +1115,8 @@ struct BfsWorkspace {
   cudaStream_t copy_stream = nullptr;
   BfsCtl* many_ctl_h = nullptr;
   int32_t many_cap = 0;
+  std::vector<cudaEvent_t> many_ev;          // [2i], [2i+1] bracket traversal i
+  cudaEvent_t many_sync[3] = {nullptr, nullptr, nullptr};  // buffer 0 / 1 copied, row packed
 };
 
 void destroy_bfs_workspace(BfsWorkspace* w) {
@@ -1133,6 +1135,9 @@ void destroy_bfs_workspace(BfsWorkspace* w) {
     if (w->depth8[i]) cudaFree(w->depth8[i]);
   if (w->copy_stream) cudaStreamDestroy(w->copy_stream);
   if (w->many_ctl_h) cudaFreeHost(w->many_ctl_h);
+  for (cudaEvent_t e : w->many_ev) cudaEventDestroy(e);
+  for (cudaEvent_t e : w->many_sync)
+    if (e) cudaEventDestroy(e);
   delete w;
 }
 
@@ -1610,24 +1615,22 @@ static int bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, void* const
     w->many_cap = n_src;
   }
   const cudaStream_t s = g->stream, cs = w->copy_stream;
-  // events: [2i] / [2i+1] bracket traversal i; the next two mark each depth
-  // buffer's latest copy as done, the last one that a byte row is packed
-  std::vector<cudaEvent_t> ev(2 * (size_t)n_src + 3, nullptr);
-  const auto destroy_events = [&]() {
-    for (cudaEvent_t e : ev)
-      if (e) cudaEventDestroy(e);
-  };
-  for (size_t k = 0; k < ev.size(); ++k) {
-    const unsigned flags = k < 2 * (size_t)n_src ? cudaEventDefault : cudaEventDisableTiming;
-    if (cudaEventCreateWithFlags(&ev[k], flags) != cudaSuccess) {
-      ev[k] = nullptr;
-      destroy_events();
+  // events (kept in the workspace): two per traversal for its time, and three
+  // to order the streams: each depth buffer's latest copy done, a row packed
+  while (w->many_ev.size() < 2 * (size_t)n_src) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return fail(ENT_ERR_CUDA, "event creation failed");
+    w->many_ev.push_back(e);
+  }
+  for (cudaEvent_t& e : w->many_sync)
+    if (!e && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+      e = nullptr;
       return fail(ENT_ERR_CUDA, "event creation failed");
     }
-  }
+  const std::vector<cudaEvent_t>& ev = w->many_ev;
   int32_t* buf[2] = {w->depth, w->depth_b};
-  cudaEvent_t freed[2] = {ev[2 * (size_t)n_src], ev[2 * (size_t)n_src + 1]};
-  const cudaEvent_t packed = ev[2 * (size_t)n_src + 2];
+  cudaEvent_t freed[2] = {w->many_sync[0], w->many_sync[1]};
+  const cudaEvent_t packed = w->many_sync[2];
   bool copied[2] = {false, false};
   const size_t row_bytes = (bytes ? 1 : sizeof(int32_t)) * g->V;
   const unsigned pack_grid = (unsigned)((g->V + 16 * 256 - 1) / (16 * 256));
@@ -1665,10 +1668,7 @@ static int bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, void* const
   const cudaError_t se = cudaStreamSynchronize(s);
   const cudaError_t sc = cudaStreamSynchronize(cs);
   if (rc == ENT_OK && ce == cudaSuccess) ce = se != cudaSuccess ? se : sc;
-  if (rc == ENT_OK && ce != cudaSuccess) {
-    destroy_events();
-    return fail(ENT_ERR_CUDA, "pipelined traversals: %s", cudaGetErrorString(ce));
-  }
+  if (rc == ENT_OK && ce != cudaSuccess) return fail(ENT_ERR_CUDA, "pipelined traversals: %s", cudaGetErrorString(ce));
   int first_bad = -1, first_deep = -1;
   for (int32_t i = 0; i < done; ++i) {
     const BfsCtl& h = w->many_ctl_h[i];
@@ -1681,7 +1681,6 @@ static int bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, void* const
     if (h.err && first_bad < 0) first_bad = i;
     if (bytes && st.levels > 255 && first_deep < 0) first_deep = i;
   }
-  destroy_events();
   if (rc != ENT_OK) return rc;
   if (first_bad >= 0)
     return fail(ENT_ERR_TIMEOUT, "traversal %d (source %d) reported error flags 0x%x", first_bad, src[first_bad],

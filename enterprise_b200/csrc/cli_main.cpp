@@ -15,7 +15,8 @@
 //   --loop L        graph | host
 //   --gpu G         device id (default 0, as main.cu:49)
 //   --batch [N]     run the sources as bitwise multi-source batches of up to N
-//                   (default 64) sources, one launch per batch
+//                   (default 64) sources, one launch per batch; a batch's depth
+//                   rows (N x V int32) are held in host memory for the checks
 // The csr file may hold int64 (the reference's format) or int32 ids: the
 // width follows from its size against beg_pos[V].
 #include <stdio.h>
