@@ -705,7 +705,7 @@ def main():
     ap.add_argument("--batch-scale", type=int, default=22)
     ap.add_argument("--batch-sizes", default="64,256,1024", help="sources per batch in the batched leg")
     ap.add_argument("--no-multi", action="store_true", help="skip the 48-graph launch of the batched leg")
-    ap.add_argument("--serve-seconds", type=float, default=10.0, help="serving run length (config: 60)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving run length (the configuration's 60 s)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--serve-slots", type=int, default=1)
