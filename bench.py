@@ -149,7 +149,7 @@ def run_ours(args, rank, world, dist):
         t0 = time.time()
         tune_srcs = eb.pick_sources(beg, source_seed(args.scale, rank) + 0x7E57, 16)  # disjoint from the timed set
         opts, ms, hit = tune.autotune(g, tune_srcs, "single", reps=2, label="rmat", device=local)
-        tuned = {"opts": {k: v for k, v in vars(opts).items() if k != "pad"}, "cached": hit,
+        tuned = {"opts": {k: v for k, v in vars(opts).items() if k != "fault_inject"}, "cached": hit,
                  "search_s": round(time.time() - t0, 2)}
 
     if args.loop != "graph":
@@ -437,7 +437,7 @@ def run_deep(args):
             t0 = time.time()
             tsrc = eb.pick_sources(beg, 0x50C0C3 + len(name) + 0x7E57, 8)
             opts, _, hit = tune.autotune(g, tsrc, "single", reps=1, label="er")
-            tuned = {"opts": {k: v for k, v in vars(opts).items() if k != "pad"}, "cached": hit,
+            tuned = {"opts": {k: v for k, v in vars(opts).items() if k != "fault_inject"}, "cached": hit,
                      "search_s": round(time.time() - t0, 2)}
         V = g.vert_count
         depth = torch.empty(V, dtype=torch.int32, device="cuda")

@@ -51,7 +51,7 @@ class _Opts(C.Structure):
         ("hub_slots", C.c_int32), ("chunk_edges", C.c_int32), ("blocks_per_sm", C.c_int32),
         ("batch_alpha", C.c_double), ("batch_small_max", C.c_int32), ("batch_large_min", C.c_int32),
         ("batch_heavy", C.c_int32), ("narrow_max_frontier", C.c_int32), ("narrow_max_edges", C.c_int32),
-        ("narrow_max_degree", C.c_int32), ("narrow_cluster", C.c_int32), ("pad", C.c_int32),
+        ("narrow_max_degree", C.c_int32), ("narrow_cluster", C.c_int32), ("fault_inject", C.c_int32),
     ]
 
 
@@ -112,7 +112,7 @@ class BfsOpts:
     narrow_max_edges: int = 131072
     narrow_max_degree: int = 256
     narrow_cluster: int = 0
-    pad: int = 0
+    fault_inject: int = 0  # test hook: 1 makes a bounded device wait run out (ENT_ERR_TIMEOUT)
 
     def _c(self) -> _Opts:
         return _Opts(**{f.name: getattr(self, f.name) for f in fields(self)})

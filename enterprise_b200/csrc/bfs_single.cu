@@ -127,6 +127,7 @@ struct LevelArgs {
   // small-frontier mode: enter at <= narrow_f vertices, <= narrow_m edges and
   // no degree above narrow_deg; leave above exit_f vertices or exit_m edges.
   int32_t narrow_f, exit_f, narrow_deg;
+  int32_t fault_inject;  // test hook (ent_bfs_opts::fault_inject)
   int64_t narrow_m, exit_m;
 };
 
@@ -591,7 +592,7 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
       }
       uint32_t pre[4] = {cnt[0], cnt[1], cnt[2], cnt[3]}, agg[4], excl[4];
       block_excl_scan<4>(pre, agg, s_scan);
-      lookback<4, KS>(a.tiles, tile, epoch, agg, excl, s_excl, err);
+      lookback<4, KS>(a.tiles, tile, epoch, agg, excl, s_excl, err, a.fault_inject != 0);
       uint32_t pos[4];
 #pragma unroll
       for (int k = 0; k < 4; ++k) pos[k] = excl[k] + pre[k];
@@ -644,7 +645,7 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
         }
         uint32_t pre[4] = {cnt[0], cnt[1], cnt[2], cnt[3]}, agg[4], excl[4];
         block_excl_scan<4>(pre, agg, s_scan);
-        lookback<4, KS>(a.tiles, tile, epoch, agg, excl, s_excl, err);
+        lookback<4, KS>(a.tiles, tile, epoch, agg, excl, s_excl, err, a.fault_inject != 0);
         uint32_t pos[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) pos[k] = excl[k] + pre[k];
@@ -718,6 +719,10 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
     err1 |= 8;
     done = 1;
   }
+  // A look-back wait ran out (bit 2): the positions of this classification
+  // came from partial prefixes, so its queues and chunk offsets are not
+  // consistent. Stop here: no kernel may expand them.
+  if (err1 & 2) done = 1;
   // Small-frontier mode for the next level (top-down only).
   const int narrow = !done && next_dir == TD && a.narrow_f > 0 && n_next <= a.narrow_f &&
                      m_next <= a.narrow_m && (int64_t)maxd <= a.narrow_deg;
@@ -1323,6 +1328,7 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out, bool force_graph =
   a.alpha = o.alpha;
   a.beta = o.beta;
   a.ref_ratio = o.ref_ratio;
+  a.fault_inject = o.fault_inject;
   a.max_levels = (int32_t)std::min<int64_t>(V + 2, 0x7ffffff0);
   w->smem_expand = sizeof(int32_t) * (hub > 0 ? hub : 1);
   int occ_e = 0, occ_i = 0;

@@ -40,8 +40,11 @@ __device__ __forceinline__ unsigned long long lb_flag(unsigned long long w, uint
 }
 
 // Spin limit for any wait in these kernels: a wait that exceeds it records
-// an error bit and gives up, so a bug can never hang the GPU.
-constexpr int SPIN_LIMIT = 1 << 22;
+// an error bit and gives up, so a bug can never hang the GPU. An iteration
+// (an acquire load, a load of the error word, a short sleep) takes about a
+// microsecond, so a wait gives up after roughly a second; a predecessor
+// tile is always held by a running CTA and publishes within microseconds.
+constexpr int SPIN_LIMIT = 1 << 20;
 
 // Inclusive warp scan of K lanes' values (each lane holds v[k]).
 template <int K>
@@ -97,12 +100,14 @@ __device__ __forceinline__ void block_excl_scan(uint32_t (&v)[K], uint32_t (&tot
 // prefix of chain k. *err gets bit 1 set if a wait timed out.
 template <int K, int KS>
 __device__ void lookback(unsigned long long* status, uint32_t tile, uint32_t epoch, const uint32_t (&agg)[K],
-                         uint32_t (&excl)[K], uint32_t* s_excl, int* err) {
+                         uint32_t (&excl)[K], uint32_t* s_excl, int* err, bool hold_first = false) {
   const int lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     if (tile == 0) {
+      if (!hold_first) {  // fault-injection hook: tile 0 never publishes, the others time out
 #pragma unroll
-      for (int k = 0; k < K; ++k) st_release(status + k, lb_pack(epoch, LB_PREFIX, agg[k]));
+        for (int k = 0; k < K; ++k) st_release(status + k, lb_pack(epoch, LB_PREFIX, agg[k]));
+      }
     } else {
 #pragma unroll
       for (int k = 0; k < K; ++k) st_release(status + (size_t)tile * KS + k, lb_pack(epoch, LB_AGG, agg[k]));

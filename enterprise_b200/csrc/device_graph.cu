@@ -334,7 +334,7 @@ void ent_bfs_opts_default(ent_bfs_opts* o) {
   o->narrow_max_edges = 131072;
   o->narrow_max_degree = 256;
   o->narrow_cluster = 0;
-  o->pad = 0;
+  o->fault_inject = 0;
 }
 
 int ent_graph_create(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E, int32_t gpu, ent_graph** out) {
@@ -526,6 +526,7 @@ int ent_graph_set_opts(ent_graph* g, const ent_bfs_opts* o) {
   if (o->narrow_max_edges < 0 || o->narrow_max_degree < 1 || o->narrow_max_degree > (1 << 20))
     return fail(ENT_ERR_INVALID_ARG, "need narrow_max_edges >= 0 and 1 <= narrow_max_degree <= 2^20");
   if (o->narrow_cluster < 0 || o->narrow_cluster > 16) return fail(ENT_ERR_INVALID_ARG, "narrow_cluster must be in [0, 16]");
+  if (o->fault_inject < 0 || o->fault_inject > 1) return fail(ENT_ERR_INVALID_ARG, "fault_inject must be 0 or 1");
   std::lock_guard<std::mutex> lk(g->mu);
   g->opts = *o;
   if (g->ws || g->bws) {  // workspaces were built and captured with the old options

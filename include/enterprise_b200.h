@@ -94,7 +94,11 @@ typedef struct ent_bfs_opts {
   int32_t narrow_max_edges;
   int32_t narrow_max_degree;
   int32_t narrow_cluster;  /* CTAs in the cluster (1..16), 0 = largest that fits */
-  int32_t pad;
+  int32_t fault_inject;    /* test hook, 0 in use. 1: the first tile of each frontier
+                              classification never publishes its prefix, so the
+                              tiles that wait for it run out their bounded spin
+                              (a few seconds) and the traversal returns
+                              ENT_ERR_TIMEOUT with the context still usable */
 } ent_bfs_opts;
 
 typedef struct ent_stats {
