@@ -1375,6 +1375,7 @@ extern "C" {
 
 int ent_bfs_batch_device(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, void* stream,
                          ent_stats* stats) {
+  ent::NvtxRange nvtx_range("ent_bfs_batch_device");
   clear_error();
   if (!g || !src || !depth_dev || n_src < 1) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
   if (n_src > MAX_BATCH) return fail(ENT_ERR_UNSUPPORTED, "at most %d sources per batch", MAX_BATCH);
@@ -1384,6 +1385,7 @@ int ent_bfs_batch_device(ent_graph* g, const int32_t* src, int32_t n_src, int32_
 }
 
 int ent_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_out, ent_stats* stats) {
+  ent::NvtxRange nvtx_range("ent_bfs_batch");
   clear_error();
   if (!g || !src || n_src < 1) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
   if (n_src > MAX_BATCH) return fail(ENT_ERR_UNSUPPORTED, "at most %d sources per batch", MAX_BATCH);
@@ -1571,6 +1573,7 @@ int ent_multi_create(ent_graph* const* graphs, int32_t n_graphs, const int32_t* 
 }
 
 int ent_multi_run(ent_multi* m, double* device_ms) {
+  ent::NvtxRange nvtx_range("ent_multi_run");
   clear_error();
   if (!m) return fail(ENT_ERR_INVALID_ARG, "null plan");
   DeviceGuard dg(m->device);
@@ -1615,6 +1618,7 @@ int ent_multi_destroy(ent_multi* m) {
 
 int ent_bfs_multi(ent_graph* const* graphs, int32_t n_graphs, const int32_t* src, const int32_t* n_src,
                   int32_t* const* depth_out) {
+  ent::NvtxRange nvtx_range("ent_bfs_multi");
   ent_multi* m = nullptr;
   int rc = ent_multi_create(graphs, n_graphs, src, n_src, &m);
   if (rc != ENT_OK) return rc;

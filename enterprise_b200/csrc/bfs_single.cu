@@ -1464,6 +1464,7 @@ using namespace ent;
 extern "C" {
 
 int ent_bfs_device(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* parent_dev, void* stream, ent_stats* stats) {
+  ent::NvtxRange nvtx_range("ent_bfs_device");
   clear_error();
   if (!g || !depth_dev) return fail(ENT_ERR_INVALID_ARG, "null argument");
   if (src < 0 || src >= g->V) return fail(ENT_ERR_INVALID_ARG, "source %d out of range [0,%lld)", src, (long long)g->V);
@@ -1474,6 +1475,7 @@ int ent_bfs_device(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* paren
 
 int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_levels, int32_t* n_levels,
                   ent_stats* stats) {
+  ent::NvtxRange nvtx_range("ent_bfs_trace");
   clear_error();
   if (!g || !out || !n_levels || max_levels < 1) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
   if (src < 0 || src >= g->V) return fail(ENT_ERR_INVALID_ARG, "source %d out of range", src);
@@ -1557,6 +1559,7 @@ int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_l
 }
 
 int ent_bfs(ent_graph* g, int32_t src, int32_t* depth_out, int32_t* parent_out, ent_stats* stats) {
+  ent::NvtxRange nvtx_range("ent_bfs");
   clear_error();
   if (!g) return fail(ENT_ERR_INVALID_ARG, "null graph");
   if (src < 0 || src >= g->V) return fail(ENT_ERR_INVALID_ARG, "source %d out of range [0,%lld)", src, (long long)g->V);
@@ -1585,6 +1588,7 @@ int ent_bfs(ent_graph* g, int32_t src, int32_t* depth_out, int32_t* parent_out, 
 // copy of source i overlaps the traversal of source i+1.
 static int bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, void* const* depth_out, bool bytes,
                     ent_stats* stats) {
+  ent::NvtxRange nvtx_range("ent_bfs_many");
   clear_error();
   if (!g) return fail(ENT_ERR_INVALID_ARG, "null graph");
   if (n_src < 0) return fail(ENT_ERR_INVALID_ARG, "negative source count %d", n_src);

@@ -130,6 +130,7 @@ using namespace ent;
 
 extern "C" int ent_validate(ent_graph* g, int32_t src, const int32_t* depth_dev, const int32_t* parent_dev,
                             int32_t* depth_code, int64_t* depth_bad, int32_t* parent_code, int64_t* parent_bad) {
+  ent::NvtxRange nvtx_range("ent_validate");
   clear_error();
   if (!g || !depth_dev || !depth_code || !depth_bad) return fail(ENT_ERR_INVALID_ARG, "null argument");
   if (parent_dev && (!parent_code || !parent_bad)) return fail(ENT_ERR_INVALID_ARG, "null parent result");

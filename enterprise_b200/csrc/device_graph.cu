@@ -338,6 +338,7 @@ void ent_bfs_opts_default(ent_bfs_opts* o) {
 }
 
 int ent_graph_create(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E, int32_t gpu, ent_graph** out) {
+  ent::NvtxRange nvtx_range("ent_graph_create");
   clear_error();
   if (!beg || (!csr && E > 0) || !out || V < 1 || E < 0) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
   *out = nullptr;
@@ -394,6 +395,7 @@ static int check_gpu(int gpu) {
 
 int ent_graph_gen_rmat(int32_t scale, int32_t ef, double a, double b, double c, uint64_t seed, int32_t gpu,
                        ent_graph** out) {
+  ent::NvtxRange nvtx_range("ent_graph_gen_rmat");
   clear_error();
   if (!out || scale < 1 || scale > 30 || ef < 1 || a < 0 || b < 0 || c < 0 || a + b + c > 1.0)
     return fail(ENT_ERR_INVALID_ARG, "bad R-MAT parameters");
@@ -443,6 +445,7 @@ __global__ void k_first_bad_edge(const int64_t* __restrict__ src, const int64_t*
 
 int ent_graph_from_edges(const int64_t* src, const int64_t* dst, int64_t n, int64_t V, int32_t gpu,
                          ent_graph** out) {
+  ent::NvtxRange nvtx_range("ent_graph_from_edges");
   clear_error();
   if ((!src || !dst) && n > 0) return fail(ENT_ERR_INVALID_ARG, "null edge arrays");
   if (!out || V < 1 || n < 0) return fail(ENT_ERR_INVALID_ARG, "bad arguments");

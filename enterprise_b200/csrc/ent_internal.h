@@ -4,9 +4,19 @@
 #include <stdarg.h>
 #include <vector>
 #include <atomic>
+#include <nvtx3/nvToolsExt.h>
 #include "../../include/enterprise_b200.h"
 
 namespace ent {
+
+// NVTX range over a host entry point, so a timeline profiler shows which
+// call issued which kernels (header-only NVTX v3: a no-op without a tool).
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Records a thread-local error message and returns `code` so call sites can
 // write `return fail(ENT_ERR_IO, "...")`.

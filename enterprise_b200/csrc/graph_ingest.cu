@@ -83,6 +83,7 @@ struct Fd {
 using namespace ent;
 
 extern "C" int ent_graph_load(const char* beg_path, const char* csr_path, int32_t gpu, ent_graph** out) {
+  ent::NvtxRange nvtx_range("ent_graph_load");
   clear_error();
   if (!beg_path || !csr_path || !out) return fail(ENT_ERR_INVALID_ARG, "null argument");
   *out = nullptr;

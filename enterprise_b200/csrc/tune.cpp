@@ -59,6 +59,7 @@ double score(ent_graph* g, const int32_t* src, int32_t n, int mode, int reps) {
 
 extern "C" int ent_autotune(ent_graph* g, const int32_t* src, int32_t n_src, int32_t mode, int32_t reps,
                             ent_bfs_opts* best_out, double* best_ms_out) {
+  ent::NvtxRange nvtx_range("ent_autotune");
   ent::clear_error();
   if (!g || !src || n_src < 1 || (mode != 0 && mode != 1) || reps < 1)
     return ent::fail(ENT_ERR_INVALID_ARG, "bad arguments");
