@@ -16,12 +16,16 @@
 //   jfb  bit per vertex    [2] joint-frontier membership of levels L and L+1:
 //                          dedups top-down claims and lets bottom-up skip the
 //                          frontier-word gather of neighbours outside the frontier
-// A level is top-down (frontier-driven, atomicOr of new bits, then a commit
-// pass) or bottom-up (every unfinished vertex ORs its neighbours' frontier
-// words, stopping once all its missing bits are covered). Depths are never
-// scattered during the traversal: a flush kernel turns the log into the
-// source-major int32 depth rows, 32 vertices x 64 sources per warp, with
-// coalesced 128-byte row writes.
+//   act  uint64[2][W]      sources with a non-empty frontier at L (and at L+1,
+//                          being collected): only their bits are ever needed
+// A level is top-down (frontier-driven ORs of new bits, then a commit pass;
+// with many frontier edges the ORs are no-return atomics and the commit
+// rebuilds the frontier from its bitmap) or bottom-up (every unfinished
+// vertex ORs its neighbours' frontier words, stopping once all bits of the
+// active sources it lacks are covered; light, mid and large degree tiers).
+// Depths are never scattered during the traversal: a flush kernel decodes the
+// log into a byte tile per span of vertices and writes the source-major int32
+// depth rows with coalesced 128-byte stores.
 #include <algorithm>
 #include <string.h>
 #include <vector>
