@@ -522,6 +522,20 @@ def run_ingest(args):
         same = bool(np.array_equal(g1.download().csr, g2.download().csr))
         g1.close()
         g2.close()
+        torch.cuda.empty_cache()
+        # the drop-in command line end to end on the same files: load, the
+        # reference's 64 glibc rand() sources, validation, its stdout lines
+        cli = {}
+        for name, extra in (("streamed_gpu_certified", []), ("host_load_sampled_checks", ["--host-load"])):
+            t0 = time.perf_counter()
+            r = subprocess.run([eb.CLI_PATH, b, c] + extra, capture_output=True, text=True, timeout=900)
+            wall = time.perf_counter() - t0
+            line = [x for x in r.stdout.splitlines() if x.startswith("Final Average TEPS (Billion):")]
+            cli[name] = {"wall_s": round(wall, 3), "exit": r.returncode,
+                         "correct": r.stdout.count("BFS result validation: CORRECT"),
+                         "wrong": r.stdout.count("WRONG"),
+                         "final_average_teps": float(line[0].split(":")[1]) if line else None}
+        out["cli_64_sources"] = cli
     del host
     torch.cuda.empty_cache()
     out.update({"host_path_s": round(t_host, 3), "host_path_gbs": round(nbytes / t_host / 1e9, 2),

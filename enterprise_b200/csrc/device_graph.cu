@@ -493,6 +493,27 @@ int64_t ent_graph_vert_count(const ent_graph* g) { return g ? g->V : -1; }
 int64_t ent_graph_edge_count(const ent_graph* g) { return g ? g->E : -1; }
 int32_t ent_graph_device(const ent_graph* g) { return g ? g->device : -1; }
 
+int ent_device_alloc(int32_t gpu, size_t bytes, void** out) {
+  clear_error();
+  if (!out) return fail(ENT_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || gpu < 0 || gpu >= n)
+    return fail(ENT_ERR_INVALID_ARG, "no GPU %d (%d present)", gpu, n);
+  DeviceGuard dg(gpu);
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes ? bytes : 1) != cudaSuccess)
+    return fail(ENT_ERR_OOM, "device allocation of %zu bytes on GPU %d failed", bytes, gpu);
+  *out = p;
+  return ENT_OK;
+}
+
+int ent_device_free(void* p) {
+  clear_error();
+  if (p && cudaFree(p) != cudaSuccess) return fail(ENT_ERR_CUDA, "device free failed");
+  return ENT_OK;
+}
+
 int ent_graph_download(const ent_graph* g, int64_t* beg, int32_t* csr) {
   clear_error();
   if (!g || !beg || (!csr && g->E > 0)) return fail(ENT_ERR_INVALID_ARG, "null argument");

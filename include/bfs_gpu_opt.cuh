@@ -60,38 +60,23 @@ inline int local_check(const int64_t* off, const int32_t* adj, const int32_t* de
   return 0;
 }
 
-inline int run(const int32_t* src_list, const int64_t* beg_pos, const int32_t* csr, int64_t vert_count,
-               int64_t edge_count, int gpu_id, const RunOptions& ro) {
-  ent_graph* g = nullptr;
-  if (ent_graph_create(beg_pos, csr, vert_count, edge_count, gpu_id, &g) != ENT_OK) {
-    printf("Graph upload failed: %s\n", ent_last_error());
-    return 1;
-  }
-  if (ro.opts && ent_graph_set_opts(g, ro.opts) != ENT_OK) {
-    printf("Bad options: %s\n", ent_last_error());
-    ent_graph_destroy(g);
-    return 1;
-  }
-  printf("In gpu bfs\n");
+/* The reference's per-source output block (bfs_gpu_opt.cuh:372-431) and its
+ * closing lines, shared by both runners. `check` is called only for sources
+ * whose traversal has more than 2 levels, as the reference validates only
+ * those; it returns 0 when the depths pass, else the broken rule. */
+struct Report {
+  const RunOptions& ro;
   double average_teps = 0.0, inv_sum = 0.0;
   int64_t validate_count = 0;
   int failures = 0;
-  uint64_t rng = 0x9E3779B97F4A7C15ull;
-  /* the reference's per-source block (bfs_gpu_opt.cuh:372-431) for source i */
-  const auto report = [&](int i, const ent_stats& st, const int32_t* depth, double tm) {
+  explicit Report(const RunOptions& r) : ro(r) {}
+  template <class Check>
+  void source(int i, int32_t src, const ent_stats& st, double tm, Check check) {
     printf("Test %d\n", i + 1);
-    printf("Started from: %d\n", src_list[i]);
+    printf("Started from: %d\n", src);
     if (st.levels > 2) {
       ++validate_count;
-      /* sampled local checks on reached vertices */
-      int ret = 0;
-      for (int k = 0; k < ro.check_samples && ret == 0; ++k) {
-        for (int tries = 0; tries < 1000; ++tries) {
-          rng ^= rng << 13; rng ^= rng >> 7; rng ^= rng << 17;
-          int64_t b = (int64_t)(rng % (uint64_t)vert_count);
-          if (depth[b] >= 0) { ret = local_check(beg_pos, csr, depth, b); break; }
-        }
-      }
+      const int ret = check();
       if (ret != 0) ++failures;
       printf("\nBFS result validation: %s\n", ret == 0 ? "CORRECT" : "WRONG");
       const double curr_teps = (double)st.traversed_edges / (1e9 * tm);
@@ -105,12 +90,47 @@ inline int run(const int32_t* src_list, const int64_t* beg_pos, const int32_t* c
         fprintf(ro.json,
                 "{\"source\": %d, \"levels\": %d, \"td_levels\": %d, \"bu_levels\": %d, \"reached\": %lld, "
                 "\"edges\": %lld, \"ms\": %.6f, \"gteps\": %.6f, \"check\": %d, \"batched\": %s}\n",
-                src_list[i], st.levels, st.td_levels, st.bu_levels, (long long)st.reached_vertices,
+                src, st.levels, st.td_levels, st.bu_levels, (long long)st.reached_vertices,
                 (long long)st.traversed_edges, tm * 1e3, curr_teps, ret, ro.batch > 0 ? "true" : "false");
     } else {
       printf("Traverse depth is %d\n", st.levels);
     }
     printf("\n====================================\n");
+  }
+  int finish() {
+    printf("Final Average TEPS (Billion): %g\n", average_teps);
+    if (validate_count) printf("Harmonic Mean TEPS (Billion): %g\n", validate_count / inv_sum);
+    return failures ? 2 : 0;
+  }
+};
+
+/* Host CSR in hand (the reference's setting): upload it, traverse into host
+ * depth arrays, check sampled reached vertices with local_check. */
+inline int run(const int32_t* src_list, const int64_t* beg_pos, const int32_t* csr, int64_t vert_count,
+               int64_t edge_count, int gpu_id, const RunOptions& ro) {
+  ent_graph* g = nullptr;
+  if (ent_graph_create(beg_pos, csr, vert_count, edge_count, gpu_id, &g) != ENT_OK) {
+    printf("Graph upload failed: %s\n", ent_last_error());
+    return 1;
+  }
+  if (ro.opts && ent_graph_set_opts(g, ro.opts) != ENT_OK) {
+    printf("Bad options: %s\n", ent_last_error());
+    ent_graph_destroy(g);
+    return 1;
+  }
+  printf("In gpu bfs\n");
+  Report rep(ro);
+  uint64_t rng = 0x9E3779B97F4A7C15ull;
+  const auto sampled_checks = [&](const int32_t* depth) {
+    int ret = 0;
+    for (int k = 0; k < ro.check_samples && ret == 0; ++k) {
+      for (int tries = 0; tries < 1000; ++tries) {
+        rng ^= rng << 13; rng ^= rng >> 7; rng ^= rng << 17;
+        int64_t b = (int64_t)(rng % (uint64_t)vert_count);
+        if (depth[b] >= 0) { ret = local_check(beg_pos, csr, depth, b); break; }
+      }
+    }
+    return ret;
   };
   if (ro.batch > 0) {
     for (int first = 0; first < ro.n_sources; first += ro.batch) {
@@ -123,7 +143,10 @@ inline int run(const int32_t* src_list, const int64_t* beg_pos, const int32_t* c
         return 1;
       }
       const double tm = st[0].device_ms * 1e-3 / k;  /* the batch's time, shared by its sources */
-      for (int j = 0; j < k; ++j) report(first + j, st[j], rows.data() + (size_t)j * (size_t)vert_count, tm);
+      for (int j = 0; j < k; ++j) {
+        const int32_t* row = rows.data() + (size_t)j * (size_t)vert_count;
+        rep.source(first + j, src_list[first + j], st[j], tm, [&] { return sampled_checks(row); });
+      }
     }
   } else {
     std::vector<int32_t> depth((size_t)vert_count);
@@ -136,13 +159,57 @@ inline int run(const int32_t* src_list, const int64_t* beg_pos, const int32_t* c
         ent_graph_destroy(g);
         return 1;
       }
-      report(i, st, depth.data(), st.device_ms * 1e-3);
+      rep.source(i, src_list[i], st, st.device_ms * 1e-3, [&] { return sampled_checks(depth.data()); });
     }
   }
-  printf("Final Average TEPS (Billion): %g\n", average_teps);
-  if (validate_count) printf("Harmonic Mean TEPS (Billion): %g\n", validate_count / inv_sum);
   ent_graph_destroy(g);
-  return failures ? 2 : 0;
+  return rep.finish();
+}
+
+/* Graph already on the GPU (ent_graph_load): traverse into device buffers
+ * and validate every result completely on the GPU (ent_validate: the depth
+ * certificate over every vertex and edge), so no host copy of the CSR or of
+ * the depths is needed. The caller keeps ownership of g. */
+inline int run_loaded(ent_graph* g, const int32_t* src_list, const RunOptions& ro) {
+  if (ro.opts && ent_graph_set_opts(g, ro.opts) != ENT_OK) {
+    printf("Bad options: %s\n", ent_last_error());
+    return 1;
+  }
+  const int64_t V = ent_graph_vert_count(g);
+  const int width = ro.batch > 0 ? ro.batch : 1;
+  void* buf = nullptr;
+  if (ent_device_alloc(ent_graph_device(g), sizeof(int32_t) * (size_t)V * (size_t)width, &buf) != ENT_OK) {
+    printf("Device buffer failed: %s\n", ent_last_error());
+    return 1;
+  }
+  int32_t* rows = static_cast<int32_t*>(buf);
+  printf("In gpu bfs\n");
+  Report rep(ro);
+  int rc = 0;
+  const auto certify = [&](int32_t src, const int32_t* depth_dev) {
+    int32_t dc = 0, pc = 0;
+    int64_t db = -1, pb = -1;
+    if (ent_validate(g, src, depth_dev, nullptr, &dc, &db, &pc, &pb) != ENT_OK) return -100;
+    return (int)dc;
+  };
+  for (int first = 0; first < ro.n_sources && rc == 0; first += width) {
+    const int k = ro.n_sources - first < width ? ro.n_sources - first : width;
+    std::vector<ent_stats> st((size_t)k);
+    const int e = ro.batch > 0 ? ent_bfs_batch_device(g, src_list + first, k, rows, nullptr, st.data())
+                               : ent_bfs_device(g, src_list[first], rows, nullptr, nullptr, st.data());
+    if (e != ENT_OK) {
+      printf("BFS failed: %s\n", ent_last_error());
+      rc = 1;
+      break;
+    }
+    const double tm = st[0].device_ms * 1e-3 / k;
+    for (int j = 0; j < k; ++j) {
+      const int32_t* row = rows + (size_t)j * (size_t)V;
+      rep.source(first + j, src_list[first + j], st[j], tm, [&] { return certify(src_list[first + j], row); });
+    }
+  }
+  ent_device_free(buf);
+  return rc ? rc : rep.finish();
 }
 
 }  // namespace ent_compat

@@ -194,6 +194,11 @@ int ent_graph_from_edges(const int64_t* src, const int64_t* dst, int64_t n_edges
 int64_t ent_graph_vert_count(const ent_graph* g);
 int64_t ent_graph_edge_count(const ent_graph* g);
 int32_t ent_graph_device(const ent_graph* g);  /* the graph's GPU */
+/* Device buffers for callers without a CUDA runtime of their own (a
+ * foreign-function binding, the command line): bytes on GPU gpu, for the
+ * *_device calls and ent_validate. Free with ent_device_free. */
+int ent_device_alloc(int32_t gpu, size_t bytes, void** out);
+int ent_device_free(void* ptr);
 /* Copies the device CSR to caller host arrays (V+1 and E entries). */
 int ent_graph_download(const ent_graph* g, int64_t* beg_pos, int32_t* csr);
 /* Device pointers of the resident CSR (for callers that keep work on GPU). */

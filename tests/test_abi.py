@@ -86,3 +86,15 @@ def test_no_cpu_fallback_without_gpu(eb):
     with pytest.raises(eb.EntError) as ei:
         eb.Graph.from_csr(g)
     assert ei.value.code == 2
+
+
+def test_device_alloc_without_a_gpu_is_a_status(eb):
+    """ent_device_alloc reports a missing GPU as a status, not a crash."""
+    import ctypes
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    p = ctypes.c_void_p(1)
+    rc = eb.lib().ent_device_alloc(0, 1024, ctypes.byref(p))
+    assert rc != 0 and not p.value
+    assert eb.lib().ent_device_free(None) == 0

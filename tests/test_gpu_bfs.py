@@ -198,26 +198,28 @@ def test_repeated_traversals_are_independent(eb, orc):
 
 
 def test_cli_end_to_end(eb, orc, tmp_path):
+    """enterprise.bin on the reference's files: the default route (files
+    streamed to the GPU, every result certified there), the reference's route
+    (--host-load: host CSR, sampled local checks) and --batch in both give the
+    same per-source reach, edges and levels, all validated."""
+    import json
     import subprocess
     csr = eb.Csr.rmat(12, 16, seed=99)
     bp, cp = str(tmp_path / "g_beg_pos.bin"), str(tmp_path / "g_csr.bin")
     csr.save(bp, cp)
-    js = tmp_path / "out.jsonl"
-    r = subprocess.run([eb.CLI_PATH, bp, cp, "--sources", "8", "--json", str(js)], capture_output=True, text=True,
-                       timeout=300)
-    assert r.returncode == 0, r.stdout + r.stderr
-    assert "Final Average TEPS (Billion):" in r.stdout
-    assert r.stdout.count("BFS result validation: CORRECT") + r.stdout.count("Traverse depth is") == 8
-    assert "WRONG" not in r.stdout
-    # --batch: the same sources as bitwise batches of 3; same per-source edges and reach
-    jb = tmp_path / "batch.jsonl"
-    r = subprocess.run([eb.CLI_PATH, bp, cp, "--sources", "8", "--batch", "3", "--json", str(jb)],
-                       capture_output=True, text=True, timeout=300)
-    assert r.returncode == 0, r.stdout + r.stderr
-    assert "WRONG" not in r.stdout and "Final Average TEPS (Billion):" in r.stdout
-    import json
-    one = [json.loads(x) for x in js.read_text().splitlines()]
-    bat = [json.loads(x) for x in jb.read_text().splitlines()]
-    assert [(x["source"], x["edges"], x["reached"], x["levels"]) for x in one] == \
-           [(x["source"], x["edges"], x["reached"], x["levels"]) for x in bat]
-    assert all(x["batched"] for x in bat) and not any(x["batched"] for x in one)
+    runs = {}
+    for name, extra in (("gpu", []), ("host", ["--host-load"]), ("gpu_batch", ["--batch", "3"]),
+                        ("host_batch", ["--host-load", "--batch", "3"])):
+        js = tmp_path / f"{name}.jsonl"
+        r = subprocess.run([eb.CLI_PATH, bp, cp, "--sources", "8", "--json", str(js)] + extra,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, name + ": " + r.stdout + r.stderr
+        assert "Final Average TEPS (Billion):" in r.stdout and "WRONG" not in r.stdout, name
+        assert r.stdout.count("BFS result validation: CORRECT") + r.stdout.count("Traverse depth is") == 8, name
+        lines = [json.loads(x) for x in js.read_text().splitlines()]
+        assert all(x["check"] == 0 for x in lines) and all(x["batched"] == ("batch" in name) for x in lines)
+        runs[name] = [(x["source"], x["edges"], x["reached"], x["levels"]) for x in lines]
+    assert runs["gpu"] == runs["host"] == runs["gpu_batch"] == runs["host_batch"]
+    for src, edges, reached, levels in runs["gpu"]:
+        exp, _ = orc.bfs(csr.beg_pos, csr.csr, src)
+        assert (edges, reached) == orc.report(csr.beg_pos, exp) and levels == int(exp.max()) + 1
