@@ -526,7 +526,7 @@ def run_ingest(args):
         # the drop-in command line end to end on the same files: load, the
         # reference's 64 glibc rand() sources, validation, its stdout lines
         cli = {}
-        for name, extra in (("streamed_gpu_certified", []), ("host_load_sampled_checks", ["--host-load"])):
+        for name, extra in (("streamed_gpu_certified", []), ("host_load_gpu_certified", ["--host-load"])):
             t0 = time.perf_counter()
             r = subprocess.run([eb.CLI_PATH, b, c] + extra, capture_output=True, text=True, timeout=900)
             wall = time.perf_counter() - t0

@@ -10,8 +10,8 @@
 // streamed straight to the GPU (ent_graph_load: the CSR never sits in host
 // memory; only beg_pos is read on the host, for the source draw), and every
 // traversal is validated on the GPU against the whole graph (ent_validate).
-// --host-load takes the reference's route instead: the CSR loaded into host
-// memory, uploaded, depths copied back and checked on sampled vertices.
+// --host-load takes the reference's route to the GPU instead: the CSR loaded
+// into host memory and uploaded from there.
 // Options (only after the two paths):
 //   --seed S        seeded sources (hash draw) instead of rand()
 //   --sources N     number of sources (default 64)
@@ -21,9 +21,8 @@
 //   --gpu G         device id (default 0, as main.cu:49)
 //   --batch [N]     run the sources as bitwise multi-source batches of up to N
 //                   (default 64) sources, one launch per batch; a batch's depth
-//                   rows (N x V int32) are held in GPU memory (host memory
-//                   with --host-load)
-//   --host-load     load through host memory and check sampled vertices
+//                   rows (N x V int32) are held in GPU memory
+//   --host-load     load through host memory, then upload
 // The csr file may hold int64 (the reference's format) or int32 ids: the
 // width follows from its size against beg_pos[V].
 #include <stdio.h>

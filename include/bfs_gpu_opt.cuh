@@ -12,9 +12,10 @@
  * block and "Final Average TEPS (Billion)" line (bfs_gpu_opt.cuh:372-445).
  * The body forwards to the C ABI in enterprise_b200.h. Differences, by design:
  *  - errors return non-zero instead of exit() (reference comm.h:34-45);
- *  - the validation line reports the real outcome of a local depth check on
- *    sampled reached vertices (the reference prints CORRECT on both branches,
- *    bfs_gpu_opt.cuh:424-426);
+ *  - the validation line reports the real outcome of a complete depth
+ *    certificate computed on the GPU over every vertex and edge (ent_validate;
+ *    the reference spot-checks one random vertex, validate.h:34-103, and
+ *    prints CORRECT on both branches, bfs_gpu_opt.cuh:424-426);
  *  - time is the traversal's CUDA-event time (the reference used gettimeofday
  *    around a host-driven loop, bfs_gpu_opt.cuh:381-411).
  * Plain C++: include it from a .cpp or .cu file and link libenterprise_b200.
@@ -34,31 +35,10 @@ struct RunOptions {
   int n_sources = 64;          /* the reference hard-codes 64 (bfs_gpu_opt.cuh:370) */
   const ent_bfs_opts* opts = nullptr;
   FILE* json = nullptr;        /* optional machine-readable per-source lines */
-  int check_samples = 64;      /* reached vertices checked per source */
   int batch = 0;               /* > 0: run the sources as bitwise batches of up to this many
                                   (ent_bfs_batch, one launch per batch); each source's time
                                   line shows its batch's time divided by the batch's sources */
 };
-
-/* Local depth rule on one reached vertex b: every neighbour c has
- * |d(c)-d(b)| <= 1 and, beyond b, neighbours of c keep the ordering the
- * reference's validate() checks (validate.h:57-99). Returns 0 or -1..-4. */
-inline int local_check(const int64_t* off, const int32_t* adj, const int32_t* depth, int64_t b) {
-  const int32_t db = depth[b];
-  for (int64_t i = off[b]; i < off[b + 1]; ++i) {
-    const int32_t c = adj[i];
-    const int32_t dc = depth[c];
-    if (dc < 0 || dc > db + 1 || dc < db - 1) return -1;
-    for (int64_t j = off[c]; j < off[c + 1]; ++j) {
-      const int32_t dx = depth[adj[j]];
-      if (dx < 0) return -4;
-      if (dc < db && dx > db) return -2;
-      if (dc > db && dx < db) return -3;
-      if (dc == db && (dx > db + 1 || dx < db - 1)) return -4;
-    }
-  }
-  return 0;
-}
 
 /* The reference's per-source output block (bfs_gpu_opt.cuh:372-431) and its
  * closing lines, shared by both runners. `check` is called only for sources
@@ -104,8 +84,9 @@ struct Report {
   }
 };
 
-/* Host CSR in hand (the reference's setting): upload it, traverse into host
- * depth arrays, check sampled reached vertices with local_check. */
+/* Host CSR in hand (the reference's setting): upload it, then run as
+ * run_loaded does. */
+inline int run_loaded(ent_graph* g, const int32_t* src_list, const RunOptions& ro);
 inline int run(const int32_t* src_list, const int64_t* beg_pos, const int32_t* csr, int64_t vert_count,
                int64_t edge_count, int gpu_id, const RunOptions& ro) {
   ent_graph* g = nullptr;
@@ -113,57 +94,9 @@ inline int run(const int32_t* src_list, const int64_t* beg_pos, const int32_t* c
     printf("Graph upload failed: %s\n", ent_last_error());
     return 1;
   }
-  if (ro.opts && ent_graph_set_opts(g, ro.opts) != ENT_OK) {
-    printf("Bad options: %s\n", ent_last_error());
-    ent_graph_destroy(g);
-    return 1;
-  }
-  printf("In gpu bfs\n");
-  Report rep(ro);
-  uint64_t rng = 0x9E3779B97F4A7C15ull;
-  const auto sampled_checks = [&](const int32_t* depth) {
-    int ret = 0;
-    for (int k = 0; k < ro.check_samples && ret == 0; ++k) {
-      for (int tries = 0; tries < 1000; ++tries) {
-        rng ^= rng << 13; rng ^= rng >> 7; rng ^= rng << 17;
-        int64_t b = (int64_t)(rng % (uint64_t)vert_count);
-        if (depth[b] >= 0) { ret = local_check(beg_pos, csr, depth, b); break; }
-      }
-    }
-    return ret;
-  };
-  if (ro.batch > 0) {
-    for (int first = 0; first < ro.n_sources; first += ro.batch) {
-      const int k = ro.n_sources - first < ro.batch ? ro.n_sources - first : ro.batch;
-      std::vector<int32_t> rows((size_t)k * (size_t)vert_count);
-      std::vector<ent_stats> st((size_t)k);
-      if (ent_bfs_batch(g, src_list + first, k, rows.data(), st.data()) != ENT_OK) {
-        printf("BFS failed: %s\n", ent_last_error());
-        ent_graph_destroy(g);
-        return 1;
-      }
-      const double tm = st[0].device_ms * 1e-3 / k;  /* the batch's time, shared by its sources */
-      for (int j = 0; j < k; ++j) {
-        const int32_t* row = rows.data() + (size_t)j * (size_t)vert_count;
-        rep.source(first + j, src_list[first + j], st[j], tm, [&] { return sampled_checks(row); });
-      }
-    }
-  } else {
-    std::vector<int32_t> depth((size_t)vert_count);
-    for (int i = 0; i < ro.n_sources; ++i) {
-      ent_stats st;
-      if (ent_bfs(g, src_list[i], depth.data(), nullptr, &st) != ENT_OK) {
-        printf("Test %d\n", i + 1);
-        printf("Started from: %d\n", src_list[i]);
-        printf("BFS failed: %s\n", ent_last_error());
-        ent_graph_destroy(g);
-        return 1;
-      }
-      rep.source(i, src_list[i], st, st.device_ms * 1e-3, [&] { return sampled_checks(depth.data()); });
-    }
-  }
+  const int rc = run_loaded(g, src_list, ro);
   ent_graph_destroy(g);
-  return rep.finish();
+  return rc;
 }
 
 /* Graph already on the GPU (ent_graph_load): traverse into device buffers

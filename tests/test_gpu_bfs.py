@@ -200,7 +200,7 @@ def test_repeated_traversals_are_independent(eb, orc):
 def test_cli_end_to_end(eb, orc, tmp_path):
     """enterprise.bin on the reference's files: the default route (files
     streamed to the GPU, every result certified there), the reference's route
-    (--host-load: host CSR, sampled local checks) and --batch in both give the
+    (--host-load: host CSR, then upload) and --batch in both give the
     same per-source reach, edges and levels, all validated."""
     import json
     import subprocess
