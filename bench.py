@@ -384,6 +384,18 @@ def run_batched(args):
         torch.cuda.empty_cache()
     if "batch_256" in out:
         out["batch_256_vs_sequential_256"] = round(out["sequential_256"]["ms"] / out["batch_256"]["ms"], 3)
+        # the same batch writing the reference's byte depths (a quarter of the row bytes)
+        d8 = torch.empty((256, V), dtype=torch.uint8, device="cuda")
+        t8 = []
+        for rep in range(4):
+            st8 = g.bfs_batch_device_u8(srcs[:256], d8.data_ptr())
+            if rep:
+                t8.append(st8[0].device_ms)
+        chk = d8[0].cpu().numpy()
+        ref0 = g.bfs(int(srcs[0]))[0]
+        out["batch_256_byte_rows"] = {"ms": round(min(t8), 3),
+                                      "row_checked_exact": bool(np.array_equal(chk, np.where(ref0 < 0, 255, ref0)))}
+        del d8
     g.close()
     if args.no_multi:
         torch.cuda.empty_cache()

@@ -208,6 +208,8 @@ def lib() -> C.CDLL:
         "ent_validate": (C.c_int, [_P, C.c_int32, _P, _P, _I32P, _I64P, _I32P, _I64P]),
         "ent_bfs_batch": (C.c_int, [_P, _I32P, C.c_int32, _I32P, C.POINTER(_Stats)]),
         "ent_bfs_batch_device": (C.c_int, [_P, _I32P, C.c_int32, _P, _P, C.POINTER(_Stats)]),
+        "ent_bfs_batch_u8": (C.c_int, [_P, _I32P, C.c_int32, _P, C.POINTER(_Stats)]),
+        "ent_bfs_batch_device_u8": (C.c_int, [_P, _I32P, C.c_int32, _P, _P, C.POINTER(_Stats)]),
         "ent_bfs_multi": (C.c_int, [C.POINTER(_P), C.c_int32, _I32P, _I32P, C.POINTER(_I32P)]),
         "ent_bfs_batch_trace": (C.c_int, [_P, _I32P, C.c_int32, _P, C.POINTER(_Trace), C.c_int32, _I32P]),
         "ent_multi_create": (C.c_int, [C.POINTER(_P), C.c_int32, _I32P, _I32P, C.POINTER(_P)]),
@@ -543,6 +545,26 @@ class Graph:
         st = (_Stats * max(n, 1))()
         _check(lib().ent_bfs_batch_device(self.handle, _i32p(src), n, C.c_void_p(depth_ptr),
                                           C.c_void_p(stream or None), st if stats else None))
+        return [Stats._from_c(st[i]) for i in range(n)] if stats else None
+
+    def bfs_batch_u8(self, sources, depth_out: Optional[np.ndarray] = None):
+        """bfs_batch with the reference's byte depths (uint8[n_src, V], 255 =
+        unreached); depths above 254 raise ENT_ERR_UNSUPPORTED."""
+        src = np.ascontiguousarray(list(sources) if not isinstance(sources, np.ndarray) else sources,
+                                   dtype=np.int32)
+        n = len(src)
+        depth = depth_out if depth_out is not None else np.empty((n, self.vert_count), dtype=np.uint8)
+        st = (_Stats * max(n, 1))()
+        _check(lib().ent_bfs_batch_u8(self.handle, _i32p(src), n, C.c_void_p(depth.ctypes.data), st))
+        return depth, [Stats._from_c(st[i]) for i in range(n)]
+
+    def bfs_batch_device_u8(self, sources, depth_ptr: int, stream: int = 0, stats: bool = True):
+        """bfs_batch_device writing n_src x V bytes (255 = unreached)."""
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        n = len(src)
+        st = (_Stats * max(n, 1))()
+        _check(lib().ent_bfs_batch_device_u8(self.handle, _i32p(src), n, C.c_void_p(depth_ptr),
+                                             C.c_void_p(stream or None), st if stats else None))
         return [Stats._from_c(st[i]) for i in range(n)] if stats else None
 
     def close(self) -> None:

@@ -11,8 +11,10 @@ int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out);
 int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream_t cap_stream);
 // Uploads sources and output location for the next launch of w's branch.
 // With row_map_dev (device, n_src entries) source s writes depth row row_map[s].
+// bytes: the rows are uint8 (255 = unreached) instead of int32; depth_dev then
+// points at n_src x V bytes.
 int stage_request(ent_graph* g, BatchWorkspace* w, const int32_t* src, int32_t n_src, int32_t* depth_dev,
-                  cudaStream_t s, const int32_t* row_map_dev);
+                  cudaStream_t s, const int32_t* row_map_dev, bool bytes = false);
 int batch_source_stats(BatchWorkspace* w, int32_t n_src, cudaStream_t s, ent_stats* stats);
 int batch_max_sources(const BatchWorkspace* w);
 

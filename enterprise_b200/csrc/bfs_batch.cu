@@ -58,7 +58,7 @@ struct BatchCtl {
   unsigned long long acc_m, acc_mdone;
   int64_t m_f, m_done;
   uint32_t finished;
-  uint32_t pad2;
+  int32_t out_bytes;  // depth rows are uint8 (the reference's depth type, 255 = unreached), not int32
 };
 
 struct BatchArgs {
@@ -837,10 +837,10 @@ __device__ __forceinline__ uint32_t spread4(uint32_t n, int sh) {
   return ((n * 0x00204081u) & 0x01010101u) << sh;
 }
 
-template <int CG>
+template <int CG, bool BYTES>
 __device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, int last, int base, int windows,
-                           int nsrc, int32_t* depth, const int32_t* row_map, uint32_t* tile, const int* s_deg,
-                           unsigned* s_cnt, int* s_maxd, unsigned long long* s_edg) {
+                           int nsrc, int32_t* depth, const int32_t* row_map, uint32_t* tile,
+                           const int* s_deg, unsigned* s_cnt, int* s_maxd, unsigned long long* s_edg) {
   constexpr int VS = 1024 / CG;  // vertices per pass
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool four_planes = last >= 8;
@@ -901,13 +901,14 @@ __device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, in
       for (int r0 = warp * 4; r0 < 64 * CG; r0 += BB / 32 * 4) {
         const int s0 = cg * 64 + r0;
         if (s0 >= nsrc) break;
-        int32_t* out[4];
+        size_t ofs[4];  // element offset of each row's segment (int32 or byte rows)
         bool rv[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           rv[j] = s0 + j < nsrc;
-          out[j] = rv[j] ? depth + (size_t)(row_map ? row_map[s0 + j] : s0 + j) * a.V + v0 + sub : depth;
+          ofs[j] = rv[j] ? (size_t)(row_map ? row_map[s0 + j] : s0 + j) * a.V + v0 + sub : 0;
         }
+        bool deep = false;  // a depth above 254 met in byte rows
         unsigned cnt[4] = {0, 0, 0, 0};
         unsigned long long edg[4] = {0, 0, 0, 0};
         int mx[4] = {-1, -1, -1, -1};
@@ -919,7 +920,14 @@ __device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, in
             int d = (int)(signed char)(uint8_t)(wv >> (8 * j));
             if (d >= 0) d += base;
             if (rv[j]) {
-              if (windows == 0 || d >= 0) out[j][vi] = d;
+              if (windows == 0 || d >= 0) {
+                if constexpr (BYTES) {
+                  reinterpret_cast<uint8_t*>(depth)[ofs[j] + vi] = d < 0 ? (uint8_t)255 : (uint8_t)d;
+                  deep |= d > 254;
+                } else {
+                  depth[ofs[j] + vi] = d;
+                }
+              }
               if (d >= 0) {
                 ++cnt[j];
                 edg[j] += (unsigned long long)dg;
@@ -928,6 +936,8 @@ __device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, in
             }
           }
         }
+        if constexpr (BYTES)
+          if (__any_sync(FULL, deep) && lane == 0) atomicOr(&a.ctl->err, 16);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
 #pragma unroll
@@ -965,6 +975,7 @@ __global__ void __launch_bounds__(BB, 3) k_b_flush(BatchArgs a, int final_flush)
   unsigned long long* s_edg = reinterpret_cast<unsigned long long*>(s_maxd + NSRC);
   for (int i = threadIdx.x; i < NSRC; i += BB) { s_cnt[i] = 0; s_maxd[i] = -1; s_edg[i] = 0; }
   int32_t* depth = c->depth;
+  const bool bytes = c->out_bytes != 0;
   const int64_t units = (a.V + 1023) / 1024;
   for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
     const int64_t v0 = u * 1024;
@@ -973,9 +984,17 @@ __global__ void __launch_bounds__(BB, 3) k_b_flush(BatchArgs a, int final_flush)
     for (int i = threadIdx.x; i < 1024; i += BB) s_deg[i] = i < nv ? a.deg[v0 + i] : 0;
     __syncthreads();
     const int32_t* row_map = c->row_map;
-    if (a.W == 1) flush_span<1>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, tile, s_deg, s_cnt, s_maxd, s_edg);
-    else if (a.W == 2) flush_span<2>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, tile, s_deg, s_cnt, s_maxd, s_edg);
-    else flush_span<4>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, tile, s_deg, s_cnt, s_maxd, s_edg);
+#define ENT_FLUSH(CG, B) flush_span<CG, B>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, tile, s_deg, s_cnt, s_maxd, s_edg)
+    if (bytes) {
+      if (a.W == 1) ENT_FLUSH(1, true);
+      else if (a.W == 2) ENT_FLUSH(2, true);
+      else ENT_FLUSH(4, true);
+    } else {
+      if (a.W == 1) ENT_FLUSH(1, false);
+      else if (a.W == 2) ENT_FLUSH(2, false);
+      else ENT_FLUSH(4, false);
+    }
+#undef ENT_FLUSH
   }
   __syncthreads();
   for (int s = threadIdx.x; s < nsrc; s += BB) {
@@ -1291,7 +1310,7 @@ static int ensure_batch(ent_graph* g, int n_src) {
 // Uploads sources, mask and the output pointer (the kernels read them from
 // device memory, so one instantiated graph serves every batch).
 int stage_request(ent_graph*, BatchWorkspace* w, const int32_t* src, int32_t n_src, int32_t* depth_dev,
-                  cudaStream_t s, const int32_t* row_map_dev) {
+                  cudaStream_t s, const int32_t* row_map_dev, bool bytes) {
   std::vector<unsigned long long> mask(w->W, 0);
   for (int i = 0; i < n_src; ++i) mask[i >> 6] |= 1ull << (i & 63);
   ENT_CUDA(cudaMemcpyAsync((void*)w->args.mask, mask.data(), sizeof(unsigned long long) * w->W, cudaMemcpyHostToDevice, s));
@@ -1300,7 +1319,16 @@ int stage_request(ent_graph*, BatchWorkspace* w, const int32_t* src, int32_t n_s
   init.n_src = n_src;
   init.depth = depth_dev;
   init.row_map = row_map_dev;
+  init.out_bytes = bytes ? 1 : 0;
   ENT_CUDA(cudaMemcpyAsync(w->ctl, &init, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
+  return ENT_OK;
+}
+
+// Status of a finished batch from its device error word: bit 16 = a depth
+// above 254 met while writing byte rows (those rows hold its low byte).
+static int batch_status(int32_t err) {
+  if (err & 16) return fail(ENT_ERR_UNSUPPORTED, "a source reaches a depth above 254; byte depths hold 0..254");
+  if (err) return fail(ENT_ERR_TIMEOUT, "batched traversal reported error flags 0x%x", err);
   return ENT_OK;
 }
 
@@ -1324,8 +1352,7 @@ static int read_batch_stats(ent_graph* g, BatchWorkspace* w, int32_t n_src, cuda
     stats[i].launches = 3 + 4 * w->ctl_h->level;  // shared by the batch
   }
   g_kernel_launches += 3 + 4 * (int64_t)w->ctl_h->level;
-  if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "batched traversal reported error flags 0x%x", w->ctl_h->err);
-  return ENT_OK;
+  return batch_status(w->ctl_h->err);
 }
 
 // Per-source statistics of a finished run of workspace w (the caller has
@@ -1348,20 +1375,20 @@ int batch_source_stats(BatchWorkspace* w, int32_t n_src, cudaStream_t s, ent_sta
     stats[i].launches = 3 + 4 * w->ctl_h->level;  // shared by the batch
   }
   g_kernel_launches += 3 + 4 * (int64_t)w->ctl_h->level;
-  return w->ctl_h->err ? fail(ENT_ERR_TIMEOUT, "batched traversal error flags 0x%x", w->ctl_h->err) : ENT_OK;
+  return batch_status(w->ctl_h->err);
 }
 
 int batch_max_sources(const BatchWorkspace* w) { return w->cap_src; }
 
 int run_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, cudaStream_t stream,
-                  ent_stats* stats) {
+                  ent_stats* stats, bool bytes) {
   for (int i = 0; i < n_src; ++i)
     if (src[i] < 0 || src[i] >= g->V) return fail(ENT_ERR_INVALID_ARG, "source %d out of range", src[i]);
   int rc = ensure_batch(g, n_src);
   if (rc != ENT_OK) return rc;
   BatchWorkspace* w = g->bws;
   cudaStream_t s = stream ? stream : g->stream;
-  rc = stage_request(g, w, src, n_src, depth_dev, s, nullptr);
+  rc = stage_request(g, w, src, n_src, depth_dev, s, nullptr, bytes);
   if (rc != ENT_OK) return rc;
   ENT_CUDA(cudaEventRecord(w->ev0, s));
   ENT_CUDA(cudaGraphLaunch(w->exec, s));
@@ -1388,8 +1415,21 @@ int ent_bfs_batch_device(ent_graph* g, const int32_t* src, int32_t n_src, int32_
   return run_bfs_batch(g, src, n_src, depth_dev, (cudaStream_t)stream, stats);
 }
 
-int ent_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_out, ent_stats* stats) {
-  ent::NvtxRange nvtx_range("ent_bfs_batch");
+int ent_bfs_batch_device_u8(ent_graph* g, const int32_t* src, int32_t n_src, uint8_t* depth_dev, void* stream,
+                            ent_stats* stats) {
+  ent::NvtxRange nvtx_range("ent_bfs_batch_device_u8");
+  clear_error();
+  if (!g || !src || !depth_dev || n_src < 1) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
+  if (n_src > MAX_BATCH) return fail(ENT_ERR_UNSUPPORTED, "at most %d sources per batch", MAX_BATCH);
+  std::lock_guard<std::mutex> lk(g->mu);
+  DeviceGuard dg(g->device);
+  return run_bfs_batch(g, src, n_src, reinterpret_cast<int32_t*>(depth_dev), (cudaStream_t)stream, stats, true);
+}
+
+// Host rows of either type: the batch writes them into the workspace's
+// device buffer, then one copy brings them back.
+static int batch_to_host(ent_graph* g, const int32_t* src, int32_t n_src, void* depth_out, bool bytes,
+                         ent_stats* stats) {
   clear_error();
   if (!g || !src || n_src < 1) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
   if (n_src > MAX_BATCH) return fail(ENT_ERR_UNSUPPORTED, "at most %d sources per batch", MAX_BATCH);
@@ -1398,7 +1438,7 @@ int ent_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* dept
   int rc = ensure_batch(g, n_src);
   if (rc != ENT_OK) return rc;
   BatchWorkspace* w = g->bws;
-  const size_t need = sizeof(int32_t) * (size_t)n_src * g->V;
+  const size_t need = (bytes ? 1 : sizeof(int32_t)) * (size_t)n_src * g->V;
   if (w->depth_cap < need) {
     if (w->depth) cudaFree(w->depth);
     w->depth = nullptr;
@@ -1407,11 +1447,22 @@ int ent_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* dept
     w->depth_cap = need;
   }
   std::vector<ent_stats> local(stats ? 0 : n_src);
-  rc = run_bfs_batch(g, src, n_src, w->depth, g->stream, stats ? stats : local.data());
-  if (rc != ENT_OK) return rc;
+  rc = run_bfs_batch(g, src, n_src, w->depth, g->stream, stats ? stats : local.data(), bytes);
+  // a byte row past depth 254 still holds the other sources' complete rows
+  if (rc != ENT_OK && !(bytes && rc == ENT_ERR_UNSUPPORTED)) return rc;
   if (depth_out) ENT_CUDA(cudaMemcpyAsync(depth_out, w->depth, need, cudaMemcpyDeviceToHost, g->stream));
   ENT_CUDA(cudaStreamSynchronize(g->stream));
-  return ENT_OK;
+  return rc;
+}
+
+int ent_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_out, ent_stats* stats) {
+  ent::NvtxRange nvtx_range("ent_bfs_batch");
+  return batch_to_host(g, src, n_src, depth_out, false, stats);
+}
+
+int ent_bfs_batch_u8(ent_graph* g, const int32_t* src, int32_t n_src, uint8_t* depth_out, ent_stats* stats) {
+  ent::NvtxRange nvtx_range("ent_bfs_batch_u8");
+  return batch_to_host(g, src, n_src, depth_out, true, stats);
 }
 
 // Host-driven run of a batch with CUDA events per level (tracing aid; same
@@ -1430,7 +1481,7 @@ int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t
   if (rc != ENT_OK) return rc;
   BatchWorkspace* w = g->bws;
   cudaStream_t s = g->stream;
-  rc = stage_request(g, w, src, n_src, depth_dev, s, nullptr);
+  rc = stage_request(g, w, src, n_src, depth_dev, s, nullptr, false);
   if (rc != ENT_OK) return rc;
   ENT_CUDA(cudaMemsetAsync(w->x_ptr, 0, w->x_bytes, s));
   ENT_CUDA(cudaMemsetAsync(w->small_ptr, 0, w->small_bytes, s));
@@ -1587,7 +1638,7 @@ int ent_multi_run(ent_multi* m, double* device_ms) {
   std::vector<std::unique_lock<std::mutex>> locks;
   for (ent_graph* g : order) locks.emplace_back(g->mu);
   for (size_t k = 0; k < m->graphs.size(); ++k) {
-    int rc = stage_request(m->graphs[k], m->ws[k], m->src[k].data(), m->n_src[k], m->depth[k], m->stream, nullptr);
+    int rc = stage_request(m->graphs[k], m->ws[k], m->src[k].data(), m->n_src[k], m->depth[k], m->stream, nullptr, false);
     if (rc != ENT_OK) return rc;
   }
   ENT_CUDA(cudaEventRecord(m->ev0, m->stream));

@@ -72,6 +72,6 @@ int graph_finish(ent_graph* g);  // computes deg, creates stream
 int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* parent_dev, cudaStream_t stream,
                    ent_stats* stats);
 int run_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, cudaStream_t stream,
-                  ent_stats* stats);
+                  ent_stats* stats, bool bytes = false);
 
 }  // namespace ent

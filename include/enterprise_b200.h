@@ -297,6 +297,16 @@ int ent_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* dept
 /* Batched traversal with device-resident output (n_src x V int32 on the GPU). */
 int ent_bfs_batch_device(ent_graph* g, const int32_t* src, int32_t n_src,
                          int32_t* depth_dev, void* stream, ent_stats* stats);
+/* The same two calls with the reference's own depth type: rows of n_src x V
+ * bytes (depth_t = unsigned char, comm.h:69; 255 = unreached, comm.h:131), a
+ * quarter of the bytes to write and to copy. A source whose traversal goes
+ * deeper than 254 levels makes the call return ENT_ERR_UNSUPPORTED (its row
+ * holds the low byte of each depth; the other rows are complete), where the
+ * reference wraps around. */
+int ent_bfs_batch_u8(ent_graph* g, const int32_t* src, int32_t n_src, uint8_t* depth_out,
+                     ent_stats* stats);
+int ent_bfs_batch_device_u8(ent_graph* g, const int32_t* src, int32_t n_src,
+                            uint8_t* depth_dev, void* stream, ent_stats* stats);
 
 /* Host-driven batched run with CUDA events per level (tracing aid). Entry
  * n-1 with level == -1 times the final depth flush. */

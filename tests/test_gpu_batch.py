@@ -156,3 +156,38 @@ def test_sources_in_small_components(eb, orc, n):
             np.testing.assert_array_equal(depth[i], exp, err_msg=f"row {i} (source {srcs[i]})")
             assert stats[i].reached_vertices == (exp >= 0).sum()
             assert stats[i].levels == int(exp.max()) + 1
+
+
+@pytest.mark.parametrize("n", [5, 70, 300])
+def test_byte_rows_match_int32_rows(eb, orc, n):
+    """ent_bfs_batch_u8: the reference's byte depths equal the int32 rows with
+    -1 read as 255, for 1, 2 and 8 words per vertex; the device variant too."""
+    import torch
+    csr = eb.Csr.rmat(13, 16, seed=700 + n)
+    srcs = [int(s) for s in eb.pick_sources(csr.beg_pos, 701 + n, n)]
+    with eb.Graph.from_csr(csr) as g:
+        d32, st32 = g.bfs_batch(srcs)
+        d8, st8 = g.bfs_batch_u8(srcs)
+        np.testing.assert_array_equal(d8, np.where(d32 < 0, 255, d32).astype(np.uint8))
+        assert [s.traversed_edges for s in st8] == [s.traversed_edges for s in st32]
+        dev = torch.empty((n, g.vert_count), dtype=torch.uint8, device="cuda")
+        g.bfs_batch_device_u8(srcs, dev.data_ptr())
+        np.testing.assert_array_equal(dev.cpu().numpy(), d8)
+        for i in range(0, n, max(1, n // 6)):
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, srcs[i])
+            np.testing.assert_array_equal(d8[i], np.where(exp < 0, 255, exp).astype(np.uint8))
+
+
+def test_byte_rows_refuse_depths_above_254(eb, orc):
+    """A 300-vertex path (depths up to 299, several flush windows): the call
+    reports ENT_ERR_UNSUPPORTED; the row of a source whose depths stay below
+    255 is still complete."""
+    n = 300
+    csr = eb.Csr.from_edges(np.arange(n - 1), np.arange(1, n), n)
+    with eb.Graph.from_csr(csr) as g:
+        out = np.zeros((2, n), dtype=np.uint8)
+        with pytest.raises(eb.EntError, match="byte depths") as ei:
+            g.bfs_batch_u8([150, 0], depth_out=out)
+        assert ei.value.code == 8
+        exp, _ = orc.bfs(csr.beg_pos, csr.csr, 150)
+        np.testing.assert_array_equal(out[0], exp.astype(np.uint8))
