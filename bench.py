@@ -342,7 +342,15 @@ def run_batched(args):
     g = eb.Graph.rmat(scale, 16, seed=graph_seed(scale), **RMAT)
     beg = g.download().beg_pos
     srcs = eb.pick_sources(beg, source_seed(scale), 1024)
+    tune_srcs = eb.pick_sources(beg, source_seed(scale) + 0x7E57, 1024)  # disjoint from the timed sources
     V = g.vert_count
+    tuned = {}
+    if not args.no_tune:
+        # the sequential baseline runs with single-source options tuned for this graph too
+        from enterprise_b200 import tune
+        o1, _, hit = tune.autotune(g, tune_srcs[:16], "single", reps=2, label="rmat")
+        tuned["single"] = {"alpha": o1.alpha, "beta": o1.beta, "small_max": o1.small_max,
+                           "large_min": o1.large_min, "chunk_edges": o1.chunk_edges, "cached": hit}
     d1 = torch.empty(V, dtype=torch.int32, device="cuda")
     st = [g.bfs_device(int(s), d1.data_ptr()) for s in srcs[:256]]
     m = np.array([x.traversed_edges for x in st], dtype=np.float64)
@@ -361,14 +369,13 @@ def run_batched(args):
     out = {"graph": f"rmat s{scale} ef16", "vertices": V, "directed_entries": g.edge_count,
            "sequential_256": {"ms": round(seq_ms, 3), "gteps": round(m.sum() / seq_ms / 1e6, 2),
                               "kind": "256 direction-optimizing single-source runs, back to back"}}
-    tuned = None
-    if not args.no_tune:
-        from enterprise_b200 import tune
-        opts, _, hit = tune.autotune(g, srcs[:256], "batch", reps=1, label="rmat")
-        tuned = {"batch_alpha": opts.batch_alpha, "batch_small_max": opts.batch_small_max,
-                 "batch_large_min": opts.batch_large_min, "batch_heavy": opts.batch_heavy, "cached": hit}
-        out["autotuned"] = tuned
     for n in [int(x) for x in args.batch_sizes.split(",")]:
+        if not args.no_tune:
+            # each batch width gets its own search, on sources disjoint from the timed ones
+            ob, _, hit = tune.autotune(g, tune_srcs[:n], "batch", reps=1, label=f"rmat-batch{n}")
+            tuned[f"batch_{n}"] = {"batch_alpha": ob.batch_alpha, "batch_small_max": ob.batch_small_max,
+                                   "batch_large_min": ob.batch_large_min, "batch_heavy": ob.batch_heavy,
+                                   "cached": hit}
         dd = torch.empty((n, V), dtype=torch.int32, device="cuda")
         times, edges = [], 0
         for rep in range(4):
@@ -382,9 +389,13 @@ def run_batched(args):
                             "levels": stb[0].td_levels + stb[0].bu_levels}
         del dd
         torch.cuda.empty_cache()
+    if tuned:
+        out["autotuned"] = tuned
     if "batch_256" in out:
         out["batch_256_vs_sequential_256"] = round(out["sequential_256"]["ms"] / out["batch_256"]["ms"], 3)
         # the same batch writing the reference's byte depths (a quarter of the row bytes)
+        if not args.no_tune:
+            tune.autotune(g, tune_srcs[:256], "batch", reps=1, label="rmat-batch256")  # its options again
         d8 = torch.empty((256, V), dtype=torch.uint8, device="cuda")
         t8 = []
         for rep in range(4):
