@@ -379,10 +379,17 @@ def run_batched(args):
         dd = torch.empty((n, V), dtype=torch.int32, device="cuda")
         times, edges = [], 0
         for rep in range(4):
-            stb = g.bfs_batch_device(srcs[:n], dd.data_ptr())
-            if rep:
-                times.append(stb[0].device_ms)
-            edges = sum(x.traversed_edges for x in stb)
+            if args.batch_loop == "host":  # same kernels, launched per level (for profilers)
+                rows = g.trace_batch([int(x) for x in srcs[:n]], dd.data_ptr())
+                if rep:
+                    times.append(sum(r["expand_ms"] + r["inspect_ms"] for r in rows))
+                stb = g.bfs_batch_device(srcs[:n], dd.data_ptr()) if rep == 3 else None
+            else:
+                stb = g.bfs_batch_device(srcs[:n], dd.data_ptr())
+                if rep:
+                    times.append(stb[0].device_ms)
+            if stb:
+                edges = sum(x.traversed_edges for x in stb)
         ms = min(times)
         ok = all(np.array_equal(dd[i].cpu().numpy(), g.bfs(int(srcs[i]))[0]) for i in (0, n // 2, n - 1))
         out[f"batch_{n}"] = {"ms": round(ms, 3), "gteps": round(edges / ms / 1e6, 2), "rows_checked_exact": ok,
@@ -751,6 +758,8 @@ def main():
     ap.add_argument("--batch-scale", type=int, default=22)
     ap.add_argument("--batch-sizes", default="64,256,1024", help="sources per batch in the batched leg")
     ap.add_argument("--no-multi", action="store_true", help="skip the 48-graph launch of the batched leg")
+    ap.add_argument("--batch-loop", choices=["graph", "host"], default="graph",
+                    help="host: drive each batch level by level from the host (kernels visible to ncu)")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving run length (the configuration's 60 s)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-batch", type=int, default=64)
