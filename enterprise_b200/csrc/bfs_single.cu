@@ -21,7 +21,9 @@
 //    shared-memory hub cache of the frontier's highest-degree vertices
 //    (reference K5-K7, expander.cuh:431-819; hub cache comm.h:172-177).
 //    Rows are ordered by descending neighbour degree, so the first check
-//    usually meets a hub.
+//    usually meets a hub; each vertex's first four neighbours are also kept
+//    in a `lead` array read coalesced beside its row offsets, so that check
+//    costs no scattered row read.
 //  * The inspector (reference K8/K9/K11, inspector.cuh:36-432) classifies the
 //    next frontier into small/mid/large queues with one single-pass
 //    decoupled look-back scan, order-preserving: from the raw discovery queue
@@ -41,7 +43,9 @@
 //    status probe and one claim on its critical path.
 //  * The whole traversal is one CUDA graph: a reset kernel, then a while node
 //    whose body is [expand, inspect, if(narrow){narrow}]; the inspector sets
-//    both conditions.
+//    both conditions. The look-back wait is the only spin: it is bounded, and
+//    a classification whose wait ran out ends the traversal with an error
+//    bit instead of handing on inconsistent queues.
 #include <algorithm>
 #include <vector>
 #include <string.h>
