@@ -223,3 +223,49 @@ def test_cli_end_to_end(eb, orc, tmp_path):
     for src, edges, reached, levels in runs["gpu"]:
         exp, _ = orc.bfs(csr.beg_pos, csr.csr, src)
         assert (edges, reached) == orc.report(csr.beg_pos, exp) and levels == int(exp.max()) + 1
+
+@pytest.mark.parametrize("policy", POLICIES)
+def test_raw_csr_with_duplicates_and_self_loops(eb, orc, policy):
+    """Files from the reference's own edge-list converter keep duplicate edges
+    and self loops and need not sort rows. Such a (symmetric) CSR taken as it
+    is: depths equal the oracle's on the same arrays, report() counts every
+    listed entry, and the batched path and the GPU certificates agree."""
+    import torch
+    base = eb.Csr.rmat(12, 8, seed=888)
+    V = base.vert_count
+    rng = np.random.default_rng(889)
+    rows = []
+    for v in range(V):
+        r = list(base.csr[base.beg_pos[v]:base.beg_pos[v + 1]])
+        if r and rng.random() < 0.3:
+            r += r[: max(1, len(r) // 3)]          # duplicates (each mirrored below)
+        if rng.random() < 0.1:
+            r.append(v)                            # self loop
+        rows.append(r)
+    # keep the adjacency symmetric: mirror every duplicate
+    extra = [[] for _ in range(V)]
+    for v, r in enumerate(rows):
+        seen = {}
+        for u in r:
+            seen[u] = seen.get(u, 0) + 1
+        for u, k in seen.items():
+            if u != v and k > 1:
+                extra[u] += [v] * (k - 1)
+    adj_rows = [np.array(r + e, dtype=np.int32) for r, e in zip(rows, extra)]
+    for r in adj_rows:
+        rng.shuffle(r)
+    beg = np.zeros(V + 1, dtype=np.int64)
+    beg[1:] = np.cumsum([len(r) for r in adj_rows])
+    adj = np.concatenate(adj_rows).astype(np.int32)
+    srcs = [int(s) for s in eb.pick_sources(beg, 890, 6)]
+    with _graph(eb, eb.Csr(beg, adj), policy=policy) as g:
+        for s in srcs:
+            exp, _ = orc.bfs(beg, adj, s)
+            d, p, st = g.bfs(s, parents=True)
+            np.testing.assert_array_equal(d, exp)
+            assert (st.traversed_edges, st.reached_vertices) == orc.report(beg, exp)
+            (dc, db), (pc, pb) = g.validate(s, d, p)
+            assert (dc, pc) == (0, 0), (dc, db, pc, pb)
+        rows_b, _ = g.bfs_batch(srcs)
+        for i, s in enumerate(srcs):
+            np.testing.assert_array_equal(rows_b[i], orc.bfs(beg, adj, s)[0])
