@@ -191,3 +191,27 @@ def test_byte_rows_refuse_depths_above_254(eb, orc):
         assert ei.value.code == 8
         exp, _ = orc.bfs(csr.beg_pos, csr.csr, 150)
         np.testing.assert_array_equal(out[0], exp.astype(np.uint8))
+
+
+def test_widest_batch_and_one_more(eb, orc):
+    """2048 sources (32 words per vertex, the most one launch takes): eight
+    lanes share a neighbour's words in the heavy tiers and the flush walks
+    eight column groups; every tier is forced with small thresholds. 2049
+    sources are refused."""
+    csr = eb.Csr.rmat(12, 16, seed=2048)
+    base = [int(s) for s in eb.pick_sources(csr.beg_pos, 2049, 1500)]
+    srcs = (base * 2)[:2048]  # repeats are allowed and give the same rows
+    with eb.Graph.from_csr(csr) as g:
+        o = g.opts
+        o.batch_small_max = 8
+        o.batch_large_min = 64
+        g.opts = o
+        depth, stats = g.bfs_batch(srcs)
+        for i in list(range(0, 2048, 97)) + [2047]:
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, srcs[i])
+            np.testing.assert_array_equal(depth[i], exp, err_msg=f"row {i}")
+            assert stats[i].traversed_edges == orc.report(csr.beg_pos, exp)[0]
+        np.testing.assert_array_equal(depth[0], depth[len(base)])  # the same source twice
+        with pytest.raises(eb.EntError) as ei:
+            g.bfs_batch(srcs + [srcs[0]])
+        assert ei.value.code == 8
