@@ -269,3 +269,30 @@ def test_raw_csr_with_duplicates_and_self_loops(eb, orc, policy):
         rows_b, _ = g.bfs_batch(srcs)
         for i, s in enumerate(srcs):
             np.testing.assert_array_equal(rows_b[i], orc.bfs(beg, adj, s)[0])
+
+
+@pytest.mark.parametrize("V", [1, 5, 37])
+def test_edgeless_graphs(eb, orc, V):
+    """No edges at all (and a single vertex): every entry point returns the
+    source at depth 0 and -1 (255 in bytes) elsewhere, with exact statistics."""
+    empty = np.zeros(0, dtype=np.int64)
+    csr = eb.Csr.from_edges(empty, empty, V)
+    assert csr.edge_count == 0
+    srcs = [0, V - 1]
+    with eb.Graph.from_csr(csr) as g:
+        for s in srcs:
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, s)
+            d, p, st = g.bfs(s, parents=True)
+            np.testing.assert_array_equal(d, exp)
+            assert (st.reached_vertices, st.traversed_edges, st.levels) == (1, 0, 1)
+            assert p[s] == s and (p >= 0).sum() == 1
+            (dc, _), (pc, _) = g.validate(s, d, p)
+            assert (dc, pc) == (0, 0)
+        rows, stats = g.bfs_batch(srcs)
+        for i, s in enumerate(srcs):
+            np.testing.assert_array_equal(rows[i], orc.bfs(csr.beg_pos, csr.csr, s)[0])
+            assert stats[i].reached_vertices == 1
+        outs = [np.zeros(V, dtype=np.uint8) for _ in srcs]
+        g.bfs_many(srcs, outs)
+        for s, o in zip(srcs, outs):
+            np.testing.assert_array_equal(o, np.where(np.arange(V) == s, 0, 255).astype(np.uint8))
