@@ -109,13 +109,13 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(name: str):
-    """Per-BFS DRAM bytes from the committed ncu summary (profiles/<name>)."""
+def profiled_traffic(name: str, key: str = "dram_bytes_per_bfs"):
+    """A `key: value` figure from a committed ncu summary (profiles/<name>)."""
     p = os.path.join(ROOT, "profiles", name)
     try:
         with open(p) as f:
             for ln in f:
-                if ln.startswith("dram_bytes_per_bfs:"):
+                if ln.startswith(key + ":"):
                     return float(ln.split(":", 1)[1].split()[0])
     except OSError:
         pass
@@ -400,6 +400,19 @@ def run_batched(args):
         out["autotuned"] = tuned
     if "batch_256" in out:
         out["batch_256_vs_sequential_256"] = round(out["sequential_256"]["ms"] / out["batch_256"]["ms"], 3)
+        # roofline of the batch from ncu-measured DRAM bytes (algorithmic sums would count the
+        # shared CSR reads once per source), scaled from the profiled graph by directed entries
+        prof = "bfs_batch_rmat_s21_256_graph.md"
+        tb, e_prof = profiled_traffic(prof, "dram_bytes_per_batch"), profiled_traffic(prof, "directed_entries")
+        if tb and e_prof:
+            traffic = tb * g.edge_count / e_prof
+            peak, peak_kind = measured_peak()
+            gbs = traffic / (out["batch_256"]["ms"] * 1e-3) / 1e9
+            out["batch_256_roofline"] = {
+                "bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(gbs / peak, 4), "peak_kind": peak_kind, "traffic": round(traffic),
+                "basis": f"ncu DRAM bytes of whole 256-source batches (profiles/{prof}), "
+                         "scaled to this graph by directed entries"}
         # the same batch writing the reference's byte depths (a quarter of the row bytes)
         if not args.no_tune:
             tune.autotune(g, tune_srcs[:256], "batch", reps=1, label="rmat-batch256")  # its options again
