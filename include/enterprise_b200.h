@@ -378,7 +378,7 @@ typedef struct ent_server_opts {
   int32_t single_cluster;   /* CTAs per small-frontier cluster of the deep graphs'
                                single-source slots, 0..16 (default 8; 0 = each
                                graph's own narrow_cluster option)                */
-  int32_t pad;
+  int32_t pad;              /* reserved, 0                                        */
 } ent_server_opts;
 typedef struct ent_query_result {
   int64_t query_id;
@@ -401,7 +401,9 @@ void ent_server_opts_default(ent_server_opts* opts);
 int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_server_opts* opts,
                       ent_server** out);
 int ent_server_submit(ent_server* s, int32_t graph, int32_t src, int64_t* query_id);
-/* Completed queries (up to max_results); waits up to wait_us if none is ready. */
+/* Completed queries (up to max_results); waits up to wait_us if none is ready.
+ * A query's depths stay readable (ent_server_depth, _device) until it is
+ * released, which frees its depth row for the next query. */
 int ent_server_poll(ent_server* s, ent_query_result* out, int32_t max_results, int32_t* n_out,
                     int32_t wait_us);
 int ent_server_depth(ent_server* s, int64_t query_id, int32_t* depth_out);
