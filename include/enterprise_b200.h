@@ -97,7 +97,7 @@ typedef struct ent_bfs_opts {
   int32_t fault_inject;    /* test hook, 0 in use. 1: the first tile of each frontier
                               classification never publishes its prefix, so the
                               tiles that wait for it run out their bounded spin
-                              (a few seconds) and the traversal returns
+                              (about a second) and the traversal returns
                               ENT_ERR_TIMEOUT with the context still usable */
 } ent_bfs_opts;
 
