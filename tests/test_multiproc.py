@@ -141,3 +141,9 @@ def test_bench_reference_arm_torchrun_world2():
     assert line["value"] > 0 and line["unit"] == "GTEPS"
     assert line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] == "port"
+    # the rest of the line's contract
+    assert line["metric"].startswith("GTEPS, R-MAT s24 ef16") and line["higher_is_better"] is True
+    assert (line["steps"], line["warmup"], line["scaling"]) == (3, 3, "weak")
+    assert line["e2e"]["value"] == line["value"] and line["cpu_baseline"]["value"] == line["value"]
+    assert line["cpu_baseline"]["cores"] >= 1 and line["cpu_baseline"]["sample"]
+    assert "workload" in line["config"] and line["dtype"] == "int32"
