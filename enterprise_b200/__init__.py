@@ -9,6 +9,12 @@ gpu_id)`` (reference bfs_gpu_opt.cuh:293-300) and its CSR loader
 The native library is mandatory: importing this package on a machine where
 ``lib/libenterprise_b200.so`` is missing raises, and every traversal runs on
 the GPU through that library. There is no CPU fallback.
+
+Main types: ``Csr`` (a host CSR: load, save, generate, build from edges),
+``Graph`` (a device-resident graph: single-source traversals, the pipelined
+source loop, bitwise batches, validation, tracing), ``MultiPlan`` /
+``bfs_multi`` (many graphs in one launch) and ``Server`` (the continuous-
+batching query loop).
 """
 from __future__ import annotations
 
@@ -20,8 +26,9 @@ from typing import Iterable, Optional, Sequence
 import numpy as np
 
 __all__ = [
-    "EntError", "BfsOpts", "Stats", "Csr", "Graph", "lib", "pick_sources", "pick_sources_compat",
-    "kernel_launch_count", "POLICY", "LOOP", "host_register", "host_unregister",
+    "EntError", "BfsOpts", "Stats", "Csr", "Graph", "MultiPlan", "Server", "bfs_multi", "lib",
+    "pick_sources", "pick_sources_compat", "kernel_launch_count", "POLICY", "LOOP", "host_register",
+    "host_unregister",
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
