@@ -69,7 +69,7 @@ constexpr int NROUND = 4;        // rounds of 32 edges a warp keeps in flight to
 constexpr int NC_MAX = 16;       // CTAs per cluster, at most
 constexpr int NQCAP = 4096;      // small-frontier entries per CTA and buffer
 constexpr uint32_t NF_HEAVY = 1, NF_SPILL = 2;
-constexpr int BU_ILP = 4;        // bottom-up light path: neighbours checked per step
+constexpr int BU_ILP = 2;        // bottom-up light path: neighbours checked per step (2 beat 4 and 8)
 
 // Device-resident loop state. Written only by the reset kernel's and the
 // inspector's last CTA (plus atomics on the acc_* counters and n_raw); read
