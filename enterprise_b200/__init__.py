@@ -198,6 +198,7 @@ def lib() -> C.CDLL:
         "ent_graph_vert_count": (C.c_int64, [_P]),
         "ent_graph_edge_count": (C.c_int64, [_P]),
         "ent_graph_device": (C.c_int32, [_P]),
+        "ent_graph_device_bytes": (C.c_int64, [_P]),
         "ent_device_alloc": (C.c_int, [C.c_int32, C.c_size_t, C.POINTER(_P)]),
         "ent_device_free": (C.c_int, [_P]),
         "ent_graph_from_edges": (C.c_int, [_I64P, _I64P, C.c_int64, C.c_int64, C.c_int32, C.POINTER(_P)]),

@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 #include <mutex>
 #include <stdint.h>
+#include <vector>
 
 #include "ent_internal.h"
 
@@ -116,25 +117,51 @@ __global__ void k_na_expand(unsigned char* scratch, const int64_t* __restrict__ 
   }
 }
 
-// Device address of the scratch array, looked up once per device with that
-// device current (in host code the symbol's name is only a stand-in).
+// Device address of the scratch array, looked up once per device and CUDA
+// context with that device current (in host code the symbol's name is only a
+// stand-in). An address is valid only in the context it was looked up in, so
+// a caller that switches between the runtime's primary context and a context
+// of its own (a driver-API plug-in) gets one lookup in each.
+typedef int (*CtxGetCurrentFn)(void**);  // cuCtxGetCurrent, from the driver
+struct NaEntry {
+  int dev;
+  void* ctx;
+  unsigned char* ptr;
+};
 static std::mutex g_na_mu;
-static unsigned char* g_na_ptr[128];
+static std::vector<NaEntry> g_na_cache;
+static CtxGetCurrentFn g_ctx_get = nullptr;
 
 static int na_scratch_for_current_device(unsigned char** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(ENT_ERR_CUDA, "cudaGetDevice failed: %s", cudaGetErrorString(e));
-  if (dev < 0 || dev >= 128) return fail(ENT_ERR_UNSUPPORTED, "device id %d out of range", dev);
   std::lock_guard<std::mutex> lk(g_na_mu);
-  if (!g_na_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return fail(ENT_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed on device %d: %s", dev, cudaGetErrorString(e));
-    g_na_ptr[dev] = static_cast<unsigned char*>(p);
+  if (!g_ctx_get) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+      return fail(ENT_ERR_CUDA, "driver entry point cuCtxGetCurrent unavailable: %s", cudaGetErrorString(e));
+    g_ctx_get = reinterpret_cast<CtxGetCurrentFn>(fn);
   }
-  *out = g_na_ptr[dev];
+  void* ctx = nullptr;
+  if (g_ctx_get(&ctx) != 0) return fail(ENT_ERR_CUDA, "cuCtxGetCurrent failed on device %d", dev);
+  if (ctx)
+    for (const NaEntry& n : g_na_cache)
+      if (n.dev == dev && n.ctx == ctx) {
+        *out = n.ptr;
+        return ENT_OK;
+      }
+  // Not seen in this context (or no context is bound to this thread yet: the
+  // lookup binds the device's primary context, as any runtime call does).
+  void* p = nullptr;
+  e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(ENT_ERR_CUDA, "cudaGetSymbolAddress(scratch) failed on device %d: %s", dev, cudaGetErrorString(e));
+  if (!ctx && (g_ctx_get(&ctx) != 0 || !ctx)) return fail(ENT_ERR_CUDA, "no current CUDA context on device %d", dev);
+  g_na_cache.push_back(NaEntry{dev, ctx, static_cast<unsigned char*>(p)});
+  *out = static_cast<unsigned char*>(p);
   return ENT_OK;
 }
 

@@ -492,6 +492,13 @@ int ent_graph_from_edges(const int64_t* src, const int64_t* dst, int64_t n, int6
 int64_t ent_graph_vert_count(const ent_graph* g) { return g ? g->V : -1; }
 int64_t ent_graph_edge_count(const ent_graph* g) { return g ? g->E : -1; }
 int32_t ent_graph_device(const ent_graph* g) { return g ? g->device : -1; }
+int64_t ent_graph_device_bytes(const ent_graph* g) {
+  if (!g) return -1;
+  const int64_t V = g->V, E = g->E, W = (V + 31) >> 5;
+  int64_t b = 8 * (V + 1) + 4 * std::max<int64_t>(E, 1) + 4 * V + 4 * (W + 1) + 16 * std::max<int64_t>(V, 1);
+  if (g->trav && g->trav != g->adj) b += 4 * E;
+  return b;
+}
 
 int ent_device_alloc(int32_t gpu, size_t bytes, void** out) {
   clear_error();

@@ -38,6 +38,8 @@ struct RunOptions {
   int batch = 0;               /* > 0: run the sources as bitwise batches of up to this many
                                   (ent_bfs_batch, one launch per batch); each source's time
                                   line shows its batch's time divided by the batch's sources */
+  int64_t cpu_bytes = 0;       /* host bytes the caller holds for the graph, printed as the
+                                  reference's "CPU alloc space" line (allocator.cuh:150) */
 };
 
 /* The reference's per-source output block (bfs_gpu_opt.cuh:372-431) and its
@@ -116,6 +118,10 @@ inline int run_loaded(ent_graph* g, const int32_t* src_list, const RunOptions& r
     return 1;
   }
   int32_t* rows = static_cast<int32_t*>(buf);
+  /* the reference's allocation lines (allocator.cuh:149-150), then its banner */
+  printf("GPU alloc space: %lld bytes\n",
+         (long long)(ent_graph_device_bytes(g) + (int64_t)sizeof(int32_t) * V * width));
+  printf("CPU alloc space: %lld bytes\n", (long long)ro.cpu_bytes);
   printf("In gpu bfs\n");
   Report rep(ro);
   int rc = 0;
@@ -157,6 +163,7 @@ int bfs_gpu_coalescing_mem(vertex_t* src_list, index_t* beg_pos, vertex_t* csr, 
   std::vector<int32_t> src(64);
   for (int i = 0; i < 64; ++i) src[i] = (int32_t)src_list[i];
   ent_compat::RunOptions ro;
+  ro.cpu_bytes = (int64_t)(sizeof(int64_t) * off.size() + sizeof(int32_t) * adj.size() + sizeof(int32_t) * src.size());
   return ent_compat::run(src.data(), off.data(), adj.data(), (int64_t)vert_count, (int64_t)edge_count,
                          (int)gpu_id, ro);
 }

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define ENT_ABI_VERSION 4
+#define ENT_ABI_VERSION 5
 
 enum ent_status {
   ENT_OK = 0,
@@ -194,6 +194,11 @@ int ent_graph_from_edges(const int64_t* src, const int64_t* dst, int64_t n_edges
 int64_t ent_graph_vert_count(const ent_graph* g);
 int64_t ent_graph_edge_count(const ent_graph* g);
 int32_t ent_graph_device(const ent_graph* g);  /* the graph's GPU */
+/* Device bytes held by the graph's resident arrays (offsets, the two column
+ * arrays, degrees, the active bitmap and the lead entries; traversal
+ * workspaces come on top). The reference prints its allocation total as
+ * "GPU alloc space: N bytes" (allocator.cuh:149). */
+int64_t ent_graph_device_bytes(const ent_graph* g);
 /* Device buffers for callers without a CUDA runtime of their own (a
  * foreign-function binding, the command line): bytes on GPU gpu, for the
  * *_device calls and ent_validate. Free with ent_device_free. */
@@ -266,6 +271,13 @@ int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_l
  * loads it (about 8.5 MB) and limits V to ENT_NOALLOC_MAX_VERTICES; larger
  * graphs return ENT_ERR_INVALID_ARG. The first call on a device looks up the
  * array's device address, so make that first call before any stream capture.
+ * That first call may also be when CUDA loads this library's GPU code onto the
+ * device (modules load lazily by default), which places the array there and
+ * so takes its 8.5 MB of device memory, and fails if that memory is not free:
+ * make one call while the process initialises, before it enters the code that
+ * may not allocate. The address is valid only in the CUDA context it was
+ * looked up in; a caller that also calls from a context of its own (a
+ * driver-API plug-in) gets one more lookup, once, in that context.
  * All calls share the array: calls whose work overlaps on one GPU race and
  * give wrong results, so serialise them. Synchronous on `stream` (NULL = the
  * default stream). */

@@ -29,7 +29,7 @@ def test_library_exports_every_declared_symbol(eb):
 
 
 def test_abi_version_and_defaults(eb):
-    assert eb.lib().ent_abi_version() == 4
+    assert eb.lib().ent_abi_version() == 5
     o = eb.BfsOpts()
     import ctypes
     c = eb._Opts()

@@ -5,7 +5,7 @@ paths where cudaMalloc can synchronise the device, plug-ins whose process
 memory belongs to another allocator or a fixed budget). The test calls it
 through the C ABI, twice in a row on the same device (the second call reuses
 the static scratch the first left behind), and checks each result bit-exact
-against the existing ent_bfs entry point. This file is collected last so a
+against the existing ent_bfs entry point and the CPU oracle. This file is collected last so a
 run that stops at the first failure has already run every other test.
 """
 import ctypes as C
@@ -31,7 +31,7 @@ def _run(eb, g, src, out):
 
 
 @pytest.mark.parametrize("kind", ["rmat", "grid", "hand"])
-def test_noalloc_matches_ent_bfs_twice(eb, kind):
+def test_noalloc_matches_ent_bfs_twice(eb, orc, kind):
     import torch
     if kind == "rmat":
         csr = eb.Csr.rmat(15, 16, seed=404)
@@ -42,11 +42,16 @@ def test_noalloc_matches_ent_bfs_twice(eb, kind):
     with eb.Graph.from_csr(csr) as g:
         out = torch.full((g.vert_count,), 7, dtype=torch.int32, device="cuda")
         srcs = eb.pick_sources(csr.beg_pos, 1, 2) if kind != "hand" else [0, 4]
-        for src in list(srcs) + [srcs[0]]:  # two different calls, then a repeat
+        # two different sources, a repeat, and (hand graph) an isolated source
+        order = list(srcs) + [srcs[0]] + ([7] if kind == "hand" else [])
+        for src in order:
             _run(eb, g, src, out)
             torch.cuda.synchronize()
+            got = out.cpu().numpy()
             ref, _, _ = g.bfs(int(src))
-            np.testing.assert_array_equal(out.cpu().numpy(), ref)
+            np.testing.assert_array_equal(got, ref)  # the existing entry point
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, int(src))
+            np.testing.assert_array_equal(got, exp)  # and the CPU oracle
 
 
 def test_noalloc_rejects_too_large_and_bad_source(eb):
