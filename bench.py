@@ -40,9 +40,25 @@ def graph_seed(scale):
     return 0x5EED0000 + scale
 
 
+# Seed of rank `rank`'s source set (enterprise_b200.replicas.source_seed, kept
+# here as well so that the CPU arm imports no product code; a test keeps the
+# two equal).
+SOURCE_SEED_BASE = 0x50C0000
+
+
 def source_seed(scale, rank=0):
-    from enterprise_b200.replicas import source_seed as seed
-    return seed(scale, rank)
+    return SOURCE_SEED_BASE + scale + 1000 * rank
+
+
+def headline_config(args, V, E):
+    """The workload both arms run, named the same way in both JSON lines."""
+    return {
+        "workload": f"direction-optimizing single-source BFS, R-MAT scale {args.scale} edge factor {args.ef}, "
+                    f"{args.sources} seeded sources per step",
+        "graph": {"vertices": int(V), "directed_entries": int(E), "generator_seed": graph_seed(args.scale),
+                  "source_seed": source_seed(args.scale)},
+        "l2": "inputs larger than L2 (CSR %.2f GB)" % (4 * E / 1e9),
+    }
 
 
 # ----------------------------------------------------------------- clocks --
@@ -152,10 +168,16 @@ def run_ours(args, rank, world, dist):
         tuned = {"opts": {k: v for k, v in vars(opts).items() if k != "fault_inject"}, "cached": hit,
                  "search_s": round(time.time() - t0, 2)}
 
+    if args.opts:  # explicit traversal options (on top of the tuner's or the defaults)
+        o = g.opts
+        for k, v in json.loads(args.opts).items():
+            setattr(o, k, type(getattr(o, k))(v))
+        g.opts = o
     if args.loop != "graph":
         o = g.opts
         o.loop = eb.LOOP[args.loop]
         g.opts = o
+    run_opts = {k: v for k, v in vars(g.opts).items() if k not in ("fault_inject", "loop")}
 
     stream = torch.cuda.Stream(device=local)
     sptr = stream.cuda_stream
@@ -227,7 +249,7 @@ def run_ours(args, rank, world, dist):
     # Each source's depths land in their own pinned host row; the copy of one
     # source overlaps the next traversal.
     src_list = [int(s) for s in srcs]
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = args.steps  # the same number of steps as the device-timed figure
 
     def e2e_run(dtype):
         rows = len(src_list)
@@ -279,14 +301,10 @@ def run_ours(args, rank, world, dist):
         "vs_baseline": None,
         "dtype": "int32",
         "data": "synthetic: seeded Graph500-parameter R-MAT generated on the GPU (no dataset)",
-        "config": {
-            "workload": f"direction-optimizing single-source BFS, R-MAT scale {args.scale} edge factor {args.ef}, "
-                        f"{args.sources} seeded sources per step",
-            "graph": {"vertices": V, "directed_entries": E, "generator_seed": graph_seed(args.scale)},
-            "parallelism": f"replicas x{world} (sources independent, no collective on the data path)",
-            "l2": "inputs larger than L2 (CSR %.2f GB) and a 256 MB L2 flush before every step" % (4 * E / 1e9),
-            "graph_gen_s": round(gen_s, 2),
-        },
+        "config": headline_config(args, V, E),
+        "parallelism": f"replicas x{world} (sources independent, no collective on the data path)",
+        "l2_flush": "a 256 MB buffer written before every step, besides inputs larger than L2",
+        "graph_gen_s": round(gen_s, 2),
         "gteps_harmonic_mean": round(hmean, 3),
         "gteps_reference_convention": {
             "value": round(amean_ref, 3) if amean_ref is not None else None,
@@ -320,7 +338,7 @@ def run_ours(args, rank, world, dist):
     if cpu:
         line["cpu_baseline"] = cpu
     if tuned:
-        line["config"]["autotuned"] = tuned
+        line["autotuned"] = tuned
     if world == 1 and not args.no_extras:
         g.close()
         del depth, flush
@@ -340,7 +358,8 @@ def run_batched(args):
     import enterprise_b200 as eb
     scale = args.batch_scale
     g = eb.Graph.rmat(scale, 16, seed=graph_seed(scale), **RMAT)
-    beg = g.download().beg_pos
+    host = g.download()  # the CSR the oracle checks rows against
+    beg = host.beg_pos
     srcs = eb.pick_sources(beg, source_seed(scale), 1024)
     tune_srcs = eb.pick_sources(beg, source_seed(scale) + 0x7E57, 1024)  # disjoint from the timed sources
     V = g.vert_count
@@ -391,8 +410,11 @@ def run_batched(args):
             if stb:
                 edges = sum(x.traversed_edges for x in stb)
         ms = min(times)
-        ok = all(np.array_equal(dd[i].cpu().numpy(), g.bfs(int(srcs[i]))[0]) for i in (0, n // 2, n - 1))
-        out[f"batch_{n}"] = {"ms": round(ms, 3), "gteps": round(edges / ms / 1e6, 2), "rows_checked_exact": ok,
+        # rows against the CPU oracle: every row of the 256-source batch, 16 spread rows of the others
+        check = range(n) if n == 256 else sorted(set(np.linspace(0, n - 1, 16).astype(int).tolist()))
+        bad = oracle_rows(host, [int(srcs[i]) for i in check], lambda j, _c=list(check): dd[_c[j]].cpu().numpy())
+        out[f"batch_{n}"] = {"ms": round(ms, 3), "gteps": round(edges / ms / 1e6, 2),
+                            "oracle_checked": len(check), "oracle_mismatches": bad,
                             "levels": stb[0].td_levels + stb[0].bu_levels}
         del dd
         torch.cuda.empty_cache()
@@ -422,10 +444,10 @@ def run_batched(args):
             st8 = g.bfs_batch_device_u8(srcs[:256], d8.data_ptr())
             if rep:
                 t8.append(st8[0].device_ms)
-        chk = d8[0].cpu().numpy()
-        ref0 = g.bfs(int(srcs[0]))[0]
-        out["batch_256_byte_rows"] = {"ms": round(min(t8), 3),
-                                      "row_checked_exact": bool(np.array_equal(chk, np.where(ref0 < 0, 255, ref0)))}
+        chk8 = [0, 128, 255]
+        bad8 = oracle_rows(host, [int(srcs[i]) for i in chk8], lambda j: d8[chk8[j]].cpu().numpy(), as_bytes=True)
+        out["batch_256_byte_rows"] = {"ms": round(min(t8), 3), "oracle_checked": len(chk8),
+                                      "oracle_mismatches": bad8}
         del d8
     g.close()
     if args.no_multi:
@@ -433,14 +455,15 @@ def run_batched(args):
         return out
     # 48 graphs of uneven sizes, 64 sources each, one launch
     rng = np.random.default_rng(0x48)
-    graphs, sources, total_v = [], [], 0
+    graphs, sources, hosts, total_v = [], [], [], 0
     for k in range(48):
         sc = int(rng.integers(12, 21))
         ef = int(rng.choice([8, 16, 32]))
         gk = eb.Graph.rmat(sc, ef, seed=0xC4000 + k, **RMAT)
-        bk = gk.download().beg_pos
+        hk = gk.download()
         graphs.append(gk)
-        sources.append(eb.pick_sources(bk, 0xC4100 + k, 64))
+        hosts.append(hk)
+        sources.append(eb.pick_sources(hk.beg_pos, 0xC4100 + k, 64))
         total_v += gk.vert_count
     plan = eb.MultiPlan(graphs, sources)
     mts = [plan.run() for _ in range(4)][1:]
@@ -451,10 +474,14 @@ def run_batched(args):
         dd = torch.empty((len(sk), gk.vert_count), dtype=torch.int32, device="cuda")
         edges += sum(x.traversed_edges for x in gk.bfs_batch_device(sk, dd.data_ptr()))
         del dd
-    d_last = plan.depths(47)
-    ok = np.array_equal(d_last[0], graphs[47].bfs(int(sources[47][0]))[0])
+    # the first and the last row of every graph against the CPU oracle
+    bad = []
+    for k in range(48):
+        dk = plan.depths(k)
+        bad += [dict(m, graph=k) for m in
+                oracle_rows(hosts[k], [int(sources[k][0]), int(sources[k][63])], lambda j: dk[0 if j == 0 else 63])]
     out["multi_graph_48"] = {"ms": round(ms, 3), "graphs": 48, "sources_per_graph": 64, "vertices_total": total_v,
-                             "gteps": round(edges / ms / 1e6, 2), "row_checked_exact": ok,
+                             "gteps": round(edges / ms / 1e6, 2), "oracle_checked": 96, "oracle_mismatches": bad,
                              "launches": "one CUDA graph launch, one branch per graph"}
     plan.close()
     for gk in graphs:
@@ -507,13 +534,17 @@ def run_deep(args):
         m = np.array([x.traversed_edges for x in st], dtype=np.float64)
         lv = np.array([x.levels for x in st])
         nl = np.array([x.narrow_levels for x in st])
-        # cross-check one source against the grid-wide path
-        on = g.bfs(int(srcs[0]))[0]
+        # two sources against the CPU oracle, one of them also against the grid-wide path alone
+        rows = [g.bfs(int(s))[0] for s in srcs[:2]]
         o = g.opts
         o.narrow_max_frontier = 0
         g.opts = o
         off = g.bfs(int(srcs[0]))[0]
+        on = rows[0]
+        host = g.download()
         g.close()
+        bad = oracle_rows(host, [int(s) for s in srcs[:2]], lambda j: rows[j])
+        del host
         out[name] = {"vertices": V, "sources": len(srcs), "ms_per_bfs_mean": round(float(ms.mean()), 3),
                      "gteps_harmonic": round(len(m) / float(np.sum(ms * 1e-3 / m)) / 1e9, 3),
                      "gteps_total": round(float(m.sum() / ms.sum() / 1e6), 3),
@@ -521,6 +552,7 @@ def run_deep(args):
                      "small_frontier_levels_mean": round(float(nl.mean()), 1),
                      "us_per_level": round(float((ms / lv).mean() * 1e3), 3),
                      "same_depths_with_small_frontier_mode_off": bool(np.array_equal(on, off)),
+                     "oracle_checked": 2, "oracle_mismatches": bad,
                      "autotuned": tuned}
         del depth
         torch.cuda.empty_cache()
@@ -595,13 +627,14 @@ def run_serving(args):
     import torch
     import enterprise_b200 as eb
     rmat_scales = [14, 15, 16, 17, 18, 18, 19, 19, 20, 20, 21, 22]
-    graphs, begs = [], []
+    graphs, begs, hosts = [], [], []
     for k, sc in enumerate(rmat_scales):
         graphs.append(eb.Graph.rmat(sc, 16, seed=0xC5000 + k, **RMAT))
     for k, w in enumerate([1024, 1448, 1774, 2048]):
         graphs.append(eb.Graph.grid(w, w, 0.1, seed=0xC5100 + k))
     for gk in graphs:
-        begs.append(gk.download().beg_pos)
+        hosts.append(gk.download())  # for the oracle's check of the sampled queries
+        begs.append(hosts[-1].beg_pos)
     pools = [eb.pick_sources(b, 0xC5200 + k, 512) for k, b in enumerate(begs)]
     rng = np.random.default_rng(0xC5)
     duration, rate = args.serve_seconds, args.serve_rate
@@ -612,7 +645,7 @@ def run_serving(args):
     lat, qwait, edges, done = [], [], 0, 0
     lat_cls = {"rmat": [], "grid": []}
     sample_every = max(1, n_q // 40)
-    checks, bad_status, mismatches = 0, 0, []
+    checks, bad_status, mismatches, samples = 0, 0, [], []
     graph_of = {}
     with eb.Server(graphs, max_batch=args.serve_batch, slots_per_graph=args.serve_slots,
                    single_cluster=args.serve_cluster) as srv:
@@ -634,13 +667,7 @@ def run_serving(args):
                 if r["status"] != 0:
                     bad_status += 1
                 if sample and r["status"] == 0:
-                    d = srv.depth(r["query_id"])
-                    ref = graphs[gi].bfs(src)[0]
-                    if not np.array_equal(d, ref):
-                        diff = np.flatnonzero(d != ref)
-                        mismatches.append({"graph": gi, "src": src, "n_diff": int(len(diff)), "at": int(diff[0]),
-                                           "got": int(d[diff[0]]), "want": int(ref[diff[0]])})
-                    checks += 1
+                    samples.append((gi, src, srv.depth(r["query_id"])))  # checked after the run
                 srv.release(r["query_id"])
             if time.perf_counter() - t0 > duration * 3 + 60:
                 break
@@ -649,6 +676,9 @@ def run_serving(args):
     for gk in graphs:
         gk.close()
     torch.cuda.empty_cache()
+    for gi, src, d in samples:
+        mismatches += [dict(m, graph=gi) for m in oracle_rows(hosts[gi], [src], lambda j: d)]
+    checks = len(samples)
     lat = np.array(lat)
     return {"graphs": "12 R-MAT s14-22 ef16 + 4 grids 1024^2,1448^2,1774^2,2048^2 (10% edges dropped)",
             "arrival": f"Poisson {rate}/s for {duration} s ({n_q} queries, seeded)",
@@ -659,7 +689,7 @@ def run_serving(args):
             "p999_ms": round(float(np.percentile(lat, 99.9)), 3) if len(lat) else None,
             "queue_p50_ms": round(float(np.percentile(qwait, 50)), 3) if len(qwait) else None,
             "batches": c["batches"], "mean_batch": round(c["launched"] / max(1, c["batches"]), 2),
-            "max_batch_seen": c["max_batch_seen"], "samples_checked": checks,
+            "max_batch_seen": c["max_batch_seen"], "oracle_checked": checks,
             "sampled_exact": not mismatches and bad_status == 0, "bad_status": bad_status,
             "mismatches": mismatches[:5], "max_batch": args.serve_batch, "slots_per_graph": args.serve_slots, "single_cluster": args.serve_cluster,
             "single_source_graphs": c["single_graphs"],
@@ -667,6 +697,27 @@ def run_serving(args):
                              "p50_ms": round(float(np.percentile(v, 50)), 3) if v else None,
                              "p99_ms": round(float(np.percentile(v, 99)), 3) if v else None}
                          for k, v in lat_cls.items()}}
+
+
+def oracle_rows(host, srcs, get_row, as_bytes=False):
+    """Checker for the extra legs (outside every timed region): the depth rows
+    the GPU produced for `srcs` (get_row(j) -> row j, host numpy) against the
+    CPU oracle's direction-optimising BFS on all host threads. Returns the
+    mismatches (at most 5 described), empty when every row is bit-exact."""
+    import oracle
+    bad = []
+    for j, s in enumerate(srcs):
+        exp = oracle.bfs_omp_do(host.beg_pos, host.csr, int(s))
+        if as_bytes:
+            exp = np.where(exp < 0, 255, exp).astype(np.uint8)
+        got = np.asarray(get_row(j))
+        if not np.array_equal(got, exp):
+            diff = np.flatnonzero(got != exp)
+            if len(bad) < 5:
+                bad.append({"src": int(s), "n_diff": int(len(diff)), "at": int(diff[0]) if len(diff) else -1})
+            else:
+                bad.append({"src": int(s)})
+    return bad
 
 
 def cpu_baseline(beg, csr, srcs, args, g, depth):
@@ -703,28 +754,34 @@ def cpu_baseline(beg, csr, srcs, args, g, depth):
 
 # ----------------------------------------------------------- reference ----
 def run_reference(args, rank, world):
-    """CPU BFS (oracle port; the reference has no CPU BFS) on all host threads,
-    same graph and sources; each step is a bounded sample (one source)."""
+    """The CPU arm: the oracle's direction-optimising OpenMP BFS (the reference
+    has no CPU BFS of its own; validate.h holds only a spot check) on all host
+    threads, over the GPU arm's workload: the same seeded R-MAT, rebuilt on the
+    host by the oracle's generator (the same CSR, bit for bit), and the same
+    seeded sources, all of them in every step. Loads no product code."""
     if rank != 0:
         return None
-    import enterprise_b200 as eb
     import oracle
     t0 = time.time()
-    csr = eb.Csr.rmat(args.scale, args.ef, seed=graph_seed(args.scale), **RMAT)
+    beg, adj = oracle.gen_rmat(args.scale, args.ef, seed=graph_seed(args.scale), **RMAT)
     gen_s = time.time() - t0
-    srcs = eb.pick_sources(csr.beg_pos, source_seed(args.scale), args.sources)
+    srcs = [int(s) for s in oracle.pick_sources(beg, source_seed(args.scale), args.sources)]
     threads = oracle.max_threads()
-    def one(i):
-        s = int(srcs[i % len(srcs)])
-        t = time.perf_counter()
-        d = oracle.bfs_omp_do(csr.beg_pos, csr.csr, s, threads=threads)
-        dt = time.perf_counter() - t
-        return oracle.report(csr.beg_pos, d)[0], dt
-    for i in range(args.warmup):
-        one(i)
+
+    def step():
+        edges, secs = 0.0, 0.0
+        for s in srcs:
+            t = time.perf_counter()
+            d = oracle.bfs_omp_do(beg, adj, s, threads=threads)
+            secs += time.perf_counter() - t
+            edges += oracle.report(beg, d)[0]
+        return edges, secs
+
+    for _ in range(args.warmup):
+        step()
     edges, secs = 0.0, 0.0
-    for i in range(args.steps):
-        e, dt = one(args.warmup + i)
+    for _ in range(args.steps):
+        e, dt = step()
         edges += e
         secs += dt
     value = edges / secs / 1e9
@@ -741,14 +798,15 @@ def run_reference(args, rank, world):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "int32",
-        "data": "synthetic: seeded Graph500-parameter R-MAT built on the host (same CSR as the GPU arm)",
-        "config": {"workload": f"direction-optimizing single-source BFS, R-MAT scale {args.scale} edge factor "
-                               f"{args.ef}, {args.sources} seeded sources",
-                   "graph": {"vertices": csr.vert_count, "directed_entries": csr.edge_count},
-                   "graph_gen_s": round(gen_s, 2)},
+        "data": "synthetic: seeded Graph500-parameter R-MAT built on the host by the oracle's generator "
+                "(the GPU arm's CSR, bit for bit)",
+        "config": headline_config(args, len(beg) - 1, len(adj)),
+        "parallelism": f"{threads} host threads (OpenMP)",
+        "graph_gen_s": round(gen_s, 2),
         "cpu_baseline": {"value": round(value, 4), "unit": "GTEPS", "cores": threads, "kind": "port",
-                         "sample": f"one source per step ({args.steps} timed, {args.warmup} warm-up), "
-                                   "direction-optimizing OpenMP CPU BFS (oracle port; the reference has no CPU BFS)"},
+                         "sample": f"all {len(srcs)} sources in every step ({args.steps} timed, {args.warmup} "
+                                   "warm-up), direction-optimizing OpenMP CPU BFS (oracle port; the reference "
+                                   "has no CPU BFS)"},
         "e2e": {"value": round(value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -765,6 +823,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner")
+    ap.add_argument("--opts", default="",
+                    help="JSON object of traversal options (BfsOpts fields) applied to the headline graph")
     ap.add_argument("--loop", choices=["graph", "host"], default="graph",
                     help="level loop driver; host launches each kernel (profilers can see them)")
     ap.add_argument("--no-extras", action="store_true", help="skip the batched and serving measurements")

@@ -41,6 +41,11 @@ def lib() -> C.CDLL:
         L.oracle_check_depths.argtypes = [C.c_int64, _I64P, _I32P, C.c_int32, _I32P, _I64P]
         L.oracle_check_parents.argtypes = [C.c_int64, _I64P, _I32P, C.c_int32, _I32P, _I32P, _I64P]
         L.oracle_max_threads.restype = C.c_int
+        L.oracle_gen_rmat.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64,
+                                      C.POINTER(_I64P), C.POINTER(_I32P), _I64P, _I64P]
+        L.oracle_pick_sources.argtypes = [_I64P, C.c_int64, C.c_uint64, C.c_int32, _I32P]
+        L.oracle_free.argtypes = [C.c_void_p]
+        L.oracle_free.restype = None
         _lib = L
     return _lib
 
@@ -132,6 +137,36 @@ def check_parents(beg_pos, csr, src, depth, parent) -> tuple[int, int]:
 
 def max_threads() -> int:
     return int(lib().oracle_max_threads())
+
+
+def gen_rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             seed: int = 0):
+    """Seeded R-MAT as (beg_pos int64[V+1], csr int32[E]): the CSR the product's
+    generator builds for the same arguments (graph_oracle.c)."""
+    po, pa = _I64P(), _I32P()
+    V, E = C.c_int64(), C.c_int64()
+    rc = lib().oracle_gen_rmat(scale, edge_factor, a, b, c, seed, C.byref(po), C.byref(pa), C.byref(V),
+                               C.byref(E))
+    if rc:
+        raise ValueError(f"oracle_gen_rmat failed ({rc})")
+    try:
+        beg = np.ctypeslib.as_array(po, shape=(V.value + 1,)).copy()
+        adj = np.ctypeslib.as_array(pa, shape=(max(E.value, 1),))[: E.value].copy()
+    finally:
+        lib().oracle_free(C.cast(po, C.c_void_p))
+        lib().oracle_free(C.cast(pa, C.c_void_p))
+    return beg, adj
+
+
+def pick_sources(beg_pos, seed: int, count: int) -> np.ndarray:
+    """The product's seeded source rule: first `count` distinct non-isolated
+    vertices of the hash draw."""
+    beg = np.ascontiguousarray(beg_pos, dtype=np.int64)
+    out = np.empty(count, dtype=np.int32)
+    rc = lib().oracle_pick_sources(_p64(beg), len(beg) - 1, seed, count, _p32(out))
+    if rc:
+        raise ValueError(f"oracle_pick_sources failed ({rc})")
+    return out
 
 
 def ref_validate(beg_pos, csr, depth, times: int = 1) -> int:

@@ -58,6 +58,18 @@ int oracle_check_parents(int64_t V, const int64_t* off, const int32_t* adj, int3
 /* Maximum OpenMP threads on this host. */
 int oracle_max_threads(void);
 
+/* Seeded Graph500-parameter R-MAT graph as an undirected CSR (both directions,
+ * self loops and duplicates dropped, rows ascending, ids scrambled by a seeded
+ * bijection): the same CSR as the product's generator for the same arguments,
+ * so the benchmark's CPU arm needs no product code (graph_oracle.c). *off_out
+ * (V+1) and *adj_out (E) are malloc'ed; release with oracle_free. */
+int oracle_gen_rmat(int32_t scale, int32_t edge_factor, double a, double b, double c, uint64_t seed,
+                    int64_t** off_out, int32_t** adj_out, int64_t* vert_count, int64_t* edge_count);
+/* The first `count` distinct non-isolated vertices of the seeded hash draw
+ * (the product's seeded source rule). */
+int oracle_pick_sources(const int64_t* off, int64_t V, uint64_t seed, int32_t count, int32_t* out);
+void oracle_free(void* p);
+
 #ifdef __cplusplus
 }
 #endif

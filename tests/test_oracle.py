@@ -60,6 +60,20 @@ def test_oracle_known_answers(eb, orc):
     assert orc.report(g.beg_pos, d) == (4, 3)
 
 
+@pytest.mark.parametrize("scale,ef,abc,seed", [(10, 16, (0.57, 0.19, 0.19), 1), (14, 16, (0.57, 0.19, 0.19), 0x5EED000E),
+                                               (13, 8, (0.45, 0.15, 0.15), 77)])
+def test_oracle_generator_is_the_products(eb, orc, scale, ef, abc, seed):
+    """The benchmark's CPU arm rebuilds the GPU arm's graph and sources with the
+    oracle's own generator: same CSR and same seeded sources, bit for bit."""
+    a, b, c = abc
+    beg, adj = orc.gen_rmat(scale, ef, a, b, c, seed=seed)
+    csr = eb.Csr.rmat(scale, ef, a=a, b=b, c=c, seed=seed)
+    np.testing.assert_array_equal(beg, csr.beg_pos)
+    np.testing.assert_array_equal(adj, csr.csr)
+    for s in (0, 5, 0x50C0018):
+        np.testing.assert_array_equal(orc.pick_sources(beg, s, 64), eb.pick_sources(csr.beg_pos, s, 64))
+
+
 def test_oracle_variants_agree_rmat(eb, orc):
     g = eb.Csr.rmat(12, 16, seed=11)
     for s in eb.pick_sources(g.beg_pos, 5, 8):
