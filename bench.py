@@ -138,6 +138,37 @@ def profiled_traffic(name: str, key: str = "dram_bytes_per_bfs"):
     return None
 
 
+def profiled_options(name: str):
+    """The traversal options an ncu summary was captured with (its `options:` line)."""
+    p = os.path.join(ROOT, "profiles", name)
+    try:
+        with open(p) as f:
+            for ln in f:
+                if ln.startswith("options:"):
+                    return json.loads(ln.split(":", 1)[1])
+    except (OSError, ValueError):
+        pass
+    return None
+
+
+TRAFFIC_PROFILE = "bfs_rmat_s22_traffic.md"
+
+
+def headline_traffic(run_opts: dict, E: int):
+    """(DRAM bytes per traversal, basis) for the headline's roofline: the ncu
+    capture's bytes scaled to this graph by directed entries, and only when
+    this run traverses with the options the capture used."""
+    want = profiled_options(TRAFFIC_PROFILE)
+    per, e_prof = profiled_traffic(TRAFFIC_PROFILE), profiled_traffic(TRAFFIC_PROFILE, "directed_entries")
+    if not want or not per or not e_prof:
+        return None, f"no capture summary (profiles/{TRAFFIC_PROFILE})"
+    differ = {k: (v, run_opts.get(k)) for k, v in want.items() if run_opts.get(k) != v}
+    if differ:
+        return None, f"this run's options differ from the capture's: {differ}"
+    return per * E / e_prof, (f"ncu DRAM bytes per traversal (profiles/{TRAFFIC_PROFILE}, R-MAT s22, same "
+                              f"options) x {E / e_prof:.3f} directed entries")
+
+
 # --------------------------------------------------------------- ours -----
 def run_ours(args, rank, world, dist):
     import torch
@@ -240,7 +271,8 @@ def run_ours(args, rank, world, dist):
     amean_ref = float(np.mean(gteps_src[deep])) if deep.any() else None
     peak, peak_kind = measured_peak()
     achieved = float(b_alg.mean() / (mean_per_src.mean() * 1e-3) / 1e9)
-    traffic = profiled_traffic("bfs_rmat_s24_traffic.txt") if args.scale == 24 else None  # bytes per traversal
+    traffic, traffic_basis = headline_traffic(run_opts, E)  # DRAM bytes per traversal (ncu) or None
+    physical = traffic / (mean_per_src.mean() * 1e-3) / 1e9 if traffic else None  # GB/s
 
     # ------------------------------------------------ e2e through the C ABI
     # The reference's per-source loop (traverse, copy the depths to the host)
@@ -321,9 +353,13 @@ def run_ours(args, rank, world, dist):
             "unit": "GB/s",
             "frac": round(achieved / peak, 4),
             "peak_kind": peak_kind,
-            "traffic": traffic,
+            "traffic": round(traffic) if traffic else None,
+            "traffic_basis": traffic_basis,
+            "physical_gbs": round(physical, 1) if physical else None,
+            "physical_frac": round(physical / peak, 4) if physical else None,
             "unit_of_work": "one BFS (one CUDA-graph launch: reset + [expand, inspect] x levels); "
-                            "algorithmic bytes 4*m_c + 8*n_c + 4*V",
+                            "algorithmic bytes 4*m_c + 8*n_c + 4*V; physical = ncu DRAM bytes per traversal "
+                            "over the same mean traversal time",
         },
         "e2e": {"value": round(e2e_value, 3), "unit": "GTEPS", "h2d_bytes_per_step": 4 * len(srcs),
                 "d2h_bytes_per_step": V * len(srcs),
@@ -347,10 +383,68 @@ def run_ours(args, rank, world, dist):
         line["high_diameter_and_uniform"] = run_deep(args)
         line["ingest"] = run_ingest(args)
         line["serving"] = run_serving(args)
+    elif not args.no_extras:
+        g.close()
+        del depth, flush
+        torch.cuda.empty_cache()
+        extras = run_extras_multi(args, rank, world, dist)
+        if rank == 0:
+            line.update(extras)
     return line
 
 
-def run_batched(args):
+def run_extras_multi(args, rank, world, dist):
+    """The batched and serving legs with one replica per rank (weak scaling:
+    every rank runs the single-GPU leg's work on its own GPU with its own
+    seeded sources or query stream). Each rank computes its leg without any
+    collective, then one all_gather_object on every rank, failed or not,
+    brings the results to rank 0, which sums the work and takes the slowest
+    rank's time."""
+    local = {}
+    for name, fn in (("batched", lambda: run_batched(args, rank, no_multi=True)),
+                     ("serving", lambda: run_serving(args, rank, seconds=args.serve_seconds_multi, raw=True))):
+        try:
+            local[name] = fn()
+        except Exception as e:  # noqa: BLE001 - reported in the line, the collective below still runs
+            local[name] = {"error": f"{type(e).__name__}: {e}"}
+    every = [None] * world
+    dist.all_gather_object(every, local)
+    if rank != 0:
+        return {}
+    out = {}
+    errs = [e["batched"]["error"] for e in every if "error" in e["batched"]]
+    if errs:
+        out["batched"] = {"error": errs[0], "ranks": world}
+    else:
+        b = {"ranks": world, "graph": every[0]["batched"]["graph"],
+             "kind": "replicas: every rank runs each batch width on its own seeded sources"}
+        for key in [k for k in every[0]["batched"] if k.startswith("batch_") and isinstance(every[0]["batched"][k], dict)
+                    and "edges" in every[0]["batched"][k]]:
+            ms = max(e["batched"][key]["ms"] for e in every)
+            edges = sum(e["batched"][key]["edges"] for e in every)
+            b[key] = {"ms_max_over_ranks": ms, "gteps_aggregate": round(edges / ms / 1e6, 2),
+                      "oracle_mismatches": sum(len(e["batched"][key]["oracle_mismatches"]) for e in every)}
+        out["batched"] = b
+    errs = [e["serving"]["error"] for e in every if "error" in e["serving"]]
+    if errs:
+        out["serving"] = {"error": errs[0], "ranks": world}
+    else:
+        lat = np.concatenate([np.asarray(e["serving"].pop("latencies_ms")) for e in every])
+        s = {"ranks": world, "kind": "one server per rank, each with its own seeded Poisson stream",
+             "completed": sum(e["serving"]["completed"] for e in every),
+             "throughput_qps": round(sum(e["serving"]["throughput_qps"] for e in every), 1),
+             "gteps": round(sum(e["serving"]["gteps"] for e in every), 2),
+             "p50_ms": round(float(np.percentile(lat, 50)), 3) if len(lat) else None,
+             "p99_ms": round(float(np.percentile(lat, 99)), 3) if len(lat) else None,
+             "p999_ms": round(float(np.percentile(lat, 99.9)), 3) if len(lat) else None,
+             "sampled_exact": all(e["serving"]["sampled_exact"] for e in every),
+             "per_rank": [{k: e["serving"][k] for k in ("completed", "throughput_qps", "mean_batch", "p99_ms")}
+                          for e in every]}
+        out["serving"] = s
+    return out
+
+
+def run_batched(args, rank=0, no_multi=False):
     """Bitwise multi-source BFS on R-MAT s22 ef16: batches of 64/256/1024
     sources against 256 sequential single-source runs of the same sources,
     plus 48 R-MAT graphs of scales 12-20, edge factors 8-32, in one launch."""
@@ -360,8 +454,8 @@ def run_batched(args):
     g = eb.Graph.rmat(scale, 16, seed=graph_seed(scale), **RMAT)
     host = g.download()  # the CSR the oracle checks rows against
     beg = host.beg_pos
-    srcs = eb.pick_sources(beg, source_seed(scale), 1024)
-    tune_srcs = eb.pick_sources(beg, source_seed(scale) + 0x7E57, 1024)  # disjoint from the timed sources
+    srcs = eb.pick_sources(beg, source_seed(scale, rank), 1024)
+    tune_srcs = eb.pick_sources(beg, source_seed(scale, rank) + 0x7E57, 1024)  # disjoint from the timed sources
     V = g.vert_count
     tuned = {}
     if not args.no_tune:
@@ -413,7 +507,7 @@ def run_batched(args):
         # rows against the CPU oracle: every row of the 256-source batch, 16 spread rows of the others
         check = range(n) if n == 256 else sorted(set(np.linspace(0, n - 1, 16).astype(int).tolist()))
         bad = oracle_rows(host, [int(srcs[i]) for i in check], lambda j, _c=list(check): dd[_c[j]].cpu().numpy())
-        out[f"batch_{n}"] = {"ms": round(ms, 3), "gteps": round(edges / ms / 1e6, 2),
+        out[f"batch_{n}"] = {"ms": round(ms, 3), "gteps": round(edges / ms / 1e6, 2), "edges": int(edges),
                             "oracle_checked": len(check), "oracle_mismatches": bad,
                             "levels": stb[0].td_levels + stb[0].bu_levels}
         del dd
@@ -430,11 +524,17 @@ def run_batched(args):
             traffic = tb * g.edge_count / e_prof
             peak, peak_kind = measured_peak()
             gbs = traffic / (out["batch_256"]["ms"] * 1e-3) / 1e9
+            # in-run lower bound: the output rows written once plus one read of the CSR
+            min_bytes = 4.0 * 256 * V + 4.0 * g.edge_count + 8.0 * V
+            min_gbs = min_bytes / (out["batch_256"]["ms"] * 1e-3) / 1e9
             out["batch_256_roofline"] = {
                 "bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(gbs / peak, 4), "peak_kind": peak_kind, "traffic": round(traffic),
-                "basis": f"ncu DRAM bytes of whole 256-source batches (profiles/{prof}), "
-                         "scaled to this graph by directed entries"}
+                "basis": f"scaled estimate: ncu DRAM bytes of whole 256-source batches on R-MAT s21 "
+                         f"(profiles/{prof}), scaled to this graph by directed entries",
+                "min_bytes": round(min_bytes), "min_bytes_gbs": round(min_gbs, 1),
+                "min_bytes_frac": round(min_gbs / peak, 4),
+                "min_bytes_rule": "in-run lower bound: 4*n_src*V of int32 rows written + 4*E + 8*V of CSR read once"}
         # the same batch writing the reference's byte depths (a quarter of the row bytes)
         if not args.no_tune:
             tune.autotune(g, tune_srcs[:256], "batch", reps=1, label="rmat-batch256")  # its options again
@@ -450,7 +550,7 @@ def run_batched(args):
                                       "oracle_mismatches": bad8}
         del d8
     g.close()
-    if args.no_multi:
+    if args.no_multi or no_multi:
         torch.cuda.empty_cache()
         return out
     # 48 graphs of uneven sizes, 64 sources each, one launch
@@ -620,10 +720,11 @@ def run_ingest(args):
     return out
 
 
-def run_serving(args):
+def run_serving(args, rank=0, seconds=None, raw=False):
     """Poisson stream of BFS queries against 16 device-resident graphs (12
     R-MAT s14-22 ef16, 4 grids 1024^2..2048^2 with 10% of edges dropped):
-    continuous batching, admission by HBM depth rows, latency percentiles."""
+    continuous batching, admission by HBM depth rows, latency percentiles.
+    rank > 0 draws its own query stream (replicas); raw adds the latencies."""
     import torch
     import enterprise_b200 as eb
     rmat_scales = [14, 15, 16, 17, 18, 18, 19, 19, 20, 20, 21, 22]
@@ -635,9 +736,9 @@ def run_serving(args):
     for gk in graphs:
         hosts.append(gk.download())  # for the oracle's check of the sampled queries
         begs.append(hosts[-1].beg_pos)
-    pools = [eb.pick_sources(b, 0xC5200 + k, 512) for k, b in enumerate(begs)]
-    rng = np.random.default_rng(0xC5)
-    duration, rate = args.serve_seconds, args.serve_rate
+    pools = [eb.pick_sources(b, 0xC5200 + k + 1000 * rank, 512) for k, b in enumerate(begs)]
+    rng = np.random.default_rng(0xC5 + 1000 * rank)
+    duration, rate = (args.serve_seconds if seconds is None else seconds), args.serve_rate
     n_q = int(rng.poisson(rate * duration))
     arrivals = np.sort(rng.uniform(0, duration, n_q))
     which = rng.integers(0, len(graphs), n_q)
@@ -680,7 +781,8 @@ def run_serving(args):
         mismatches += [dict(m, graph=gi) for m in oracle_rows(hosts[gi], [src], lambda j: d)]
     checks = len(samples)
     lat = np.array(lat)
-    return {"graphs": "12 R-MAT s14-22 ef16 + 4 grids 1024^2,1448^2,1774^2,2048^2 (10% edges dropped)",
+    extra = {"latencies_ms": [float(x) for x in lat]} if raw else {}
+    return {**extra, "graphs": "12 R-MAT s14-22 ef16 + 4 grids 1024^2,1448^2,1774^2,2048^2 (10% edges dropped)",
             "arrival": f"Poisson {rate}/s for {duration} s ({n_q} queries, seeded)",
             "completed": int(done), "wall_s": round(wall, 2), "throughput_qps": round(done / wall, 1),
             "gteps": round(edges / wall / 1e9, 2),
@@ -834,6 +936,8 @@ def main():
     ap.add_argument("--batch-loop", choices=["graph", "host"], default="graph",
                     help="host: drive each batch level by level from the host (kernels visible to ncu)")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving run length (the configuration's 60 s)")
+    ap.add_argument("--serve-seconds-multi", type=float, default=20.0,
+                    help="serving run length per rank when --gpus N > 1 (replicas, one stream each)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-batch", type=int, default=64)
     ap.add_argument("--serve-slots", type=int, default=1)

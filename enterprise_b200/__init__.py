@@ -13,7 +13,8 @@ the GPU through that library. There is no CPU fallback.
 Main types: ``Csr`` (a host CSR: load, save, generate, build from edges),
 ``Graph`` (a device-resident graph: single-source traversals, the pipelined
 source loop, bitwise batches, validation, tracing), ``MultiPlan`` /
-``bfs_multi`` (many graphs in one launch) and ``Server`` (the continuous-
+``bfs_multi`` (many graphs in one launch), ``Replicas`` (one graph on several
+GPUs, many-source requests spread over them) and ``Server`` (the continuous-
 batching query loop).
 """
 from __future__ import annotations
@@ -26,9 +27,9 @@ from typing import Iterable, Optional, Sequence
 import numpy as np
 
 __all__ = [
-    "EntError", "BfsOpts", "Stats", "Csr", "Graph", "MultiPlan", "Server", "bfs_multi", "lib",
+    "EntError", "BfsOpts", "Stats", "Csr", "Graph", "MultiPlan", "Server", "Replicas", "bfs_multi", "lib",
     "pick_sources", "pick_sources_compat", "kernel_launch_count", "POLICY", "LOOP", "host_register",
-    "host_unregister",
+    "host_unregister", "replicas_plan",
 ]
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -59,6 +60,7 @@ class _Opts(C.Structure):
         ("batch_alpha", C.c_double), ("batch_small_max", C.c_int32), ("batch_large_min", C.c_int32),
         ("batch_heavy", C.c_int32), ("narrow_max_frontier", C.c_int32), ("narrow_max_edges", C.c_int32),
         ("narrow_max_degree", C.c_int32), ("narrow_cluster", C.c_int32), ("fault_inject", C.c_int32),
+        ("batch_narrow", C.c_int32), ("batch_narrow_levels", C.c_int32),
     ]
 
 
@@ -120,6 +122,8 @@ class BfsOpts:
     narrow_max_degree: int = 256
     narrow_cluster: int = 0
     fault_inject: int = 0  # test hook: 1 makes a bounded device wait run out (ENT_ERR_TIMEOUT)
+    batch_narrow: int = 1  # batched small-frontier mode: 0 off, 1 auto (deep graphs), 2 on
+    batch_narrow_levels: int = 64
 
     def _c(self) -> _Opts:
         return _Opts(**{f.name: getattr(self, f.name) for f in fields(self)})
@@ -224,6 +228,13 @@ def lib() -> C.CDLL:
         "ent_multi_run": (C.c_int, [_P, C.POINTER(C.c_double)]),
         "ent_multi_depths": (C.c_int, [_P, C.c_int32, _I32P]),
         "ent_multi_destroy": (C.c_int, [_P]),
+        "ent_replicas_plan": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _I32P, _I32P]),
+        "ent_replicas_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_P)]),
+        "ent_replicas_set_max_batch": (C.c_int, [_P, C.c_int32]),
+        "ent_replicas_bfs_batch": (C.c_int, [_P, _I32P, C.c_int32, _P, _P]),
+        "ent_replicas_bfs_batch_u8": (C.c_int, [_P, _I32P, C.c_int32, _P, _P]),
+        "ent_replicas_sources_run": (C.c_int, [_P, _I64P]),
+        "ent_replicas_destroy": (C.c_int, [_P]),
         "ent_autotune": (C.c_int, [_P, _I32P, C.c_int32, C.c_int32, C.c_int32, C.POINTER(_Opts),
                                    C.POINTER(C.c_double)]),
         "ent_server_opts_default": (None, [C.POINTER(_ServerOpts)]),
@@ -620,6 +631,72 @@ class MultiPlan:
         if self._h is not None:
             lib().ent_multi_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def replicas_plan(n_src: int, n_replicas: int, max_batch: int = 1024) -> list[tuple[int, int]]:
+    """Chunks [(begin, end), ...] that a replica set cuts n_src sources into
+    (ent_replicas_plan): contiguous, at most max_batch each."""
+    n = C.c_int32()
+    _check(lib().ent_replicas_plan(n_src, n_replicas, max_batch, None, C.byref(n)))
+    b = np.empty(n.value + 1, dtype=np.int32)
+    _check(lib().ent_replicas_plan(n_src, n_replicas, max_batch, _i32p(b), C.byref(n)))
+    return [(int(b[c]), int(b[c + 1])) for c in range(n.value)]
+
+
+class Replicas:
+    """One graph replicated on several GPUs; many-source requests are spread
+    over them chunk by chunk (ent_replicas_*), results in input order. The
+    Graph handles are borrowed: close the replica set first."""
+
+    def __init__(self, graphs: Sequence[Graph], max_batch: int = 1024):
+        self.graphs = list(graphs)
+        hs = (_P * len(self.graphs))(*[g.handle for g in self.graphs])
+        h = _P()
+        _check(lib().ent_replicas_create(hs, len(self.graphs), C.byref(h)))
+        self._h = h
+        _check(lib().ent_replicas_set_max_batch(self._h, max_batch))
+
+    def bfs_batch(self, sources, depth_out: Optional[np.ndarray] = None, stats: bool = True):
+        """Depth rows (n x V int32) of every source, in input order, and per-source Stats."""
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        n, V = len(src), self.graphs[0].vert_count
+        out = depth_out if depth_out is not None else np.empty((n, V), dtype=np.int32)
+        assert out.dtype == np.int32 and out.shape == (n, V) and out.flags.c_contiguous
+        st = (_Stats * max(n, 1))()
+        _check(lib().ent_replicas_bfs_batch(self._h, _i32p(src), n, out.ctypes.data_as(_P), st if stats else None))
+        return out, ([Stats._from_c(st[i]) for i in range(n)] if stats else None)
+
+    def bfs_batch_u8(self, sources, depth_out: Optional[np.ndarray] = None):
+        """The same rows in the reference's byte depths (255 = unreached)."""
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        n, V = len(src), self.graphs[0].vert_count
+        out = depth_out if depth_out is not None else np.empty((n, V), dtype=np.uint8)
+        assert out.dtype == np.uint8 and out.shape == (n, V) and out.flags.c_contiguous
+        _check(lib().ent_replicas_bfs_batch_u8(self._h, _i32p(src), n, out.ctypes.data_as(_P), None))
+        return out
+
+    def sources_run(self) -> list[int]:
+        """Sources each replica ran in the last call."""
+        a = np.zeros(len(self.graphs), dtype=np.int64)
+        _check(lib().ent_replicas_sources_run(self._h, _i64p(a)))
+        return [int(x) for x in a]
+
+    def close(self):
+        if self._h is not None:
+            lib().ent_replicas_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def __del__(self):
         try:

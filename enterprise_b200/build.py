@@ -38,6 +38,7 @@ SOURCES = [
     "bfs_validate.cu",
     "graph_ingest.cu",
     "serve.cpp",
+    "replicas.cpp",
     "tune.cpp",
 ]
 HEADERS = ["gen_common.h", "ent_internal.h", "dev_graph.h", "dev_common.cuh", "batch_internal.h"]

@@ -40,6 +40,7 @@ struct ent_graph {
   std::mutex mu;
   ent::BfsWorkspace* ws = nullptr;
   ent::BatchWorkspace* bws = nullptr;
+  int32_t probe_levels = -1;  // depth of the graph as probed by its first auto small-frontier batch (-1: not yet)
 };
 
 namespace ent {
@@ -73,5 +74,10 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth_dev, int32_t* paren
                    ent_stats* stats);
 int run_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, cudaStream_t stream,
                   ent_stats* stats, bool bytes = false);
+// Depth (levels) of g seen from the given candidate sources: single-source
+// traversals from up to three of them (the deepest answer wins; a source that
+// reaches a quarter of the graph ends the search). Synchronous, on g->stream;
+// the caller holds g->mu.
+int probe_graph_levels(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* levels);
 
 }  // namespace ent

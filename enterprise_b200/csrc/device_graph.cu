@@ -335,6 +335,8 @@ void ent_bfs_opts_default(ent_bfs_opts* o) {
   o->narrow_max_degree = 256;
   o->narrow_cluster = 0;
   o->fault_inject = 0;
+  o->batch_narrow = 1;
+  o->batch_narrow_levels = 64;
 }
 
 int ent_graph_create(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E, int32_t gpu, ent_graph** out) {
@@ -558,6 +560,8 @@ int ent_graph_set_opts(ent_graph* g, const ent_bfs_opts* o) {
     return fail(ENT_ERR_INVALID_ARG, "need narrow_max_edges >= 0 and 1 <= narrow_max_degree <= 2^20");
   if (o->narrow_cluster < 0 || o->narrow_cluster > 16) return fail(ENT_ERR_INVALID_ARG, "narrow_cluster must be in [0, 16]");
   if (o->fault_inject < 0 || o->fault_inject > 1) return fail(ENT_ERR_INVALID_ARG, "fault_inject must be 0 or 1");
+  if (o->batch_narrow < 0 || o->batch_narrow > 2) return fail(ENT_ERR_INVALID_ARG, "batch_narrow must be 0, 1 or 2");
+  if (o->batch_narrow_levels < 1) return fail(ENT_ERR_INVALID_ARG, "batch_narrow_levels must be >= 1");
   std::lock_guard<std::mutex> lk(g->mu);
   g->opts = *o;
   if (g->ws || g->bws) {  // workspaces were built and captured with the old options

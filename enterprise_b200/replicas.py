@@ -30,6 +30,45 @@ def rank_sources(beg_pos: np.ndarray, scale: int, rank: int, count: int) -> np.n
     return pick_sources(beg_pos, source_seed(scale, rank), count)
 
 
+def rank_chunks(n_src: int, world: int, rank: int, max_batch: int = 1024) -> list[tuple[int, int]]:
+    """The chunks of a shared source list that rank `rank` of `world` runs.
+
+    The list is cut as a replica set on one node cuts it (ent_replicas_plan:
+    contiguous chunks of at most max_batch sources, at least one per rank
+    while sources last); processes share no work counter, so chunk c goes to
+    rank c % world."""
+    from . import replicas_plan
+    return [ch for c, ch in enumerate(replicas_plan(n_src, world, max_batch)) if c % world == rank]
+
+
+def gather_rows(local: list, n_src: int, dist=None):
+    """Assembles per-chunk results in input order on rank 0.
+
+    local: [((begin, end), rows), ...] with rows a (end - begin) x V array for
+    this rank's chunks. Returns the n_src x V array on rank 0 (and without a
+    process group), None on the other ranks. One gather_object on every rank."""
+    parts = local
+    if dist is not None:
+        got = [None] * dist.get_world_size() if dist.get_rank() == 0 else None
+        dist.gather_object(local, got, dst=0)
+        if dist.get_rank() != 0:
+            return None
+        parts = [p for r in got for p in r]
+    if not parts:
+        return None
+    V = parts[0][1].shape[1]
+    out = np.empty((n_src, V), dtype=parts[0][1].dtype)
+    seen = np.zeros(n_src, dtype=bool)
+    for (b, e), rows in parts:
+        if rows.shape != (e - b, V) or seen[b:e].any():
+            raise ValueError(f"chunk ({b}, {e}) does not fit the plan")
+        out[b:e] = rows
+        seen[b:e] = True
+    if not seen.all():
+        raise ValueError("chunks do not cover every source")
+    return out
+
+
 def _reduce(x: float, dist, device, op_name: str) -> float:
     if dist is None:
         return float(x)

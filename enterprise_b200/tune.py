@@ -65,7 +65,7 @@ class TuneCache:
     def put(self, key: str, opts: BfsOpts, ms: float) -> None:
         self.data[key] = {"opts": asdict(opts), "ms": ms, "when": time.strftime("%Y-%m-%dT%H:%M:%S")}
         os.makedirs(os.path.dirname(self.path) or ".", exist_ok=True)
-        tmp = self.path + ".tmp"
+        tmp = f"{self.path}.{os.getpid()}.tmp"  # one per process: ranks of a job may write at once
         with open(tmp, "w") as f:
             json.dump(self.data, f, indent=1, sort_keys=True)
         os.replace(tmp, self.path)

@@ -99,6 +99,15 @@ typedef struct ent_bfs_opts {
                               tiles that wait for it run out their bounded spin
                               (about a second) and the traversal returns
                               ENT_ERR_TIMEOUT with the context still usable */
+  /* small-frontier mode of the batched traversal, for deep graphs (grids,
+     road-like graphs): one thread-block cluster runs every level of a batch of
+     up to 256 sources inside one launch, top-down, writing each (source,
+     vertex) depth as it is found, instead of grid-wide launches per level.
+     0 = off, 1 = auto (on when a probe traversal of the graph, run once per
+     graph by its first such batch, has at least batch_narrow_levels levels),
+     2 = on. */
+  int32_t batch_narrow;
+  int32_t batch_narrow_levels;
 } ent_bfs_opts;
 
 typedef struct ent_stats {
@@ -341,6 +350,38 @@ int ent_multi_create(ent_graph* const* graphs, int32_t n_graphs, const int32_t* 
 int ent_multi_run(ent_multi* plan, double* device_ms);
 int ent_multi_depths(ent_multi* plan, int32_t k, int32_t* depth_out);
 int ent_multi_destroy(ent_multi* plan);
+
+/* ------------------------------------------------- several GPUs --------- */
+/* Many sources over replicas of one graph on several GPUs of a node. No
+ * reference counterpart (the reference drives one GPU, bfs_gpu_opt.cuh:305).
+ * Sources are independent, so nothing is exchanged on the data path: the
+ * source list is cut into contiguous chunks (ent_replicas_plan), one host
+ * thread per replica takes the next unclaimed chunk and runs it as one bitwise
+ * batch on its own GPU, and each chunk's rows land at the chunk's own rows of
+ * the output, so results are in input order whichever replica ran a chunk.
+ * Every kernel reads only its own replica; no peer memory is used. */
+typedef struct ent_replicas ent_replicas;
+/* Chunk boundaries for n_src sources over n_replicas: chunks of
+ * min(max_batch, ceil(n_src / n_replicas)) sources, the last one shorter.
+ * chunk_begin (may be NULL) receives *n_chunks + 1 entries: chunk c covers
+ * sources [chunk_begin[c], chunk_begin[c+1]). Host-only arithmetic. */
+int ent_replicas_plan(int32_t n_src, int32_t n_replicas, int32_t max_batch, int32_t* chunk_begin,
+                      int32_t* n_chunks);
+/* graphs: one handle per replica, the same graph (equal V and E) on the GPUs
+ * of the caller's choice (borrowed: destroy them after the replica set).
+ * Default max_batch 1024 sources per chunk. */
+int ent_replicas_create(ent_graph* const* graphs, int32_t n_replicas, ent_replicas** out);
+int ent_replicas_set_max_batch(ent_replicas* r, int32_t max_batch);
+/* depth_out: HOST n_src x V int32 (row s = src[s]'s depths) or NULL; stats:
+ * n_src entries or NULL. Same depths as ent_bfs_batch / n_src ent_bfs calls. */
+int ent_replicas_bfs_batch(ent_replicas* r, const int32_t* src, int32_t n_src, int32_t* depth_out,
+                           ent_stats* stats);
+/* The same with the reference's byte depths (see ent_bfs_batch_u8). */
+int ent_replicas_bfs_batch_u8(ent_replicas* r, const int32_t* src, int32_t n_src, uint8_t* depth_out,
+                              ent_stats* stats);
+/* Sources each replica ran in the last call (n_replicas entries). */
+int ent_replicas_sources_run(const ent_replicas* r, int64_t* per_replica);
+int ent_replicas_destroy(ent_replicas* r);
 
 /* ------------------------------------------------------ autotuning ------ */
 /* Coordinate-descent search of the traversal thresholds on this graph and

@@ -4,16 +4,32 @@ measured bytes of a batch) parse to the values the summaries state."""
 import os
 import sys
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+import pytest
+
+ROOT =os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 sys.path.insert(0, ROOT)
 
 
 def test_profile_figures_parse():
     import bench
-    assert bench.profiled_traffic("bfs_rmat_s24_traffic.txt") == 0.835e9
+    assert bench.profiled_traffic(bench.TRAFFIC_PROFILE) == 168.5e6
+    assert bench.profiled_traffic(bench.TRAFFIC_PROFILE, "directed_entries") == 128311084
     assert bench.profiled_traffic("bfs_batch_rmat_s21_256_graph.md", "dram_bytes_per_batch") == 4.882e9
     assert bench.profiled_traffic("bfs_batch_rmat_s21_256_graph.md", "directed_entries") == 63536952
     assert bench.profiled_traffic("no_such_summary.md") is None
+
+
+def test_headline_traffic_only_for_the_captured_options():
+    """The roofline's DRAM figure is used only when the run traverses with the
+    options the ncu capture used; otherwise it is withheld with the reason."""
+    import bench
+    want = bench.profiled_options(bench.TRAFFIC_PROFILE)
+    assert want and want["alpha"] == 48.0
+    run = dict(want, policy=0, batch_alpha=4.0)
+    t, basis = bench.headline_traffic(run, 520772318)
+    assert t == pytest.approx(168.5e6 * 520772318 / 128311084) and "same options" in basis
+    t, basis = bench.headline_traffic(dict(run, alpha=24.0), 520772318)
+    assert t is None and "differ" in basis
 
 
 def test_bench_source_seed_matches_replicas():

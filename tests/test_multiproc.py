@@ -63,6 +63,67 @@ def _replica_worker(rank, world, port, out_dir):
         dist.destroy_process_group()
 
 
+def _shard_worker(rank, world, port, out_dir):
+    """One shared source list sharded over the ranks by the product's plan;
+    each rank computes its chunks' rows (the oracle stands in for the GPU
+    batch, which needs a device) and rank 0 assembles them in input order."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    import enterprise_b200 as eb
+    from enterprise_b200 import replicas
+    import oracle
+    dist = _init(rank, world, port)
+    try:
+        csr = eb.Csr.rmat(10, 8, seed=0x5EED000A)
+        srcs = [int(s) for s in eb.pick_sources(csr.beg_pos, 0x5A4D, 37)]
+        mine = replicas.rank_chunks(len(srcs), world, rank, max_batch=8)
+        local = []
+        for b, e in mine:
+            rows = np.stack([oracle.bfs(csr.beg_pos, csr.csr, s)[0] for s in srcs[b:e]])
+            local.append(((b, e), rows))
+        full = replicas.gather_rows(local, len(srcs), dist)
+        res = {"chunks": mine}
+        if rank == 0:
+            exp = np.stack([oracle.bfs(csr.beg_pos, csr.csr, s)[0] for s in srcs])
+            res["in_order"] = bool(np.array_equal(full, exp))
+        else:
+            res["in_order"] = full is None
+        with open(os.path.join(out_dir, f"shard{rank}.json"), "w") as f:
+            json.dump(res, f)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_shard_rows_world2_gloo(tmp_path):
+    codes = _spawn(_shard_worker, 2, tmp_path)
+    assert codes == [0, 0]
+    r0 = json.load(open(tmp_path / "shard0.json"))
+    r1 = json.load(open(tmp_path / "shard1.json"))
+    assert r0["in_order"] and r1["in_order"]
+    got = sorted(tuple(c) for c in r0["chunks"] + r1["chunks"])
+    assert got[0][0] == 0 and got[-1][1] == 37
+    assert all(a[1] == b[0] for a, b in zip(got, got[1:]))  # contiguous, no overlap
+    assert r0["chunks"] and r1["chunks"]  # both ranks got work
+
+
+def test_replicas_plan_rules():
+    sys.path.insert(0, ROOT)
+    import enterprise_b200 as eb
+    for n, reps, mb in [(1000, 2, 256), (5, 8, 1024), (1, 1, 1), (2048, 3, 2048), (4097, 4, 1024), (0, 2, 4)]:
+        chunks = eb.replicas_plan(n, reps, mb)
+        assert sum(e - b for b, e in chunks) == n
+        assert all(0 < e - b <= mb for b, e in chunks)
+        assert all(a[1] == b[0] for a, b in zip(chunks, chunks[1:]))
+        assert (not chunks) or (chunks[0][0] == 0 and chunks[-1][1] == n)
+        if n >= reps:
+            assert len(chunks) >= min(reps, n)  # every replica can get work
+    with pytest.raises(Exception):
+        eb.replicas_plan(10, 0, 4)
+    from enterprise_b200 import replicas
+    allc = [c for r in range(3) for c in replicas.rank_chunks(100, 3, r, 16)]
+    assert sorted(allc) == eb.replicas_plan(100, 3, 16)
+
+
 def _dying_worker(rank, world, port, out_dir):
     dist = _init(rank, world, port, timeout_s=3)
     if rank == 1:
