@@ -383,6 +383,9 @@ def run_ours(args, rank, world, dist):
         line["high_diameter_and_uniform"] = run_deep(args)
         line["ingest"] = run_ingest(args)
         line["serving"] = run_serving(args)
+        if args.burst_seconds > 0:
+            line["serving_rmat_queued"] = run_serving(args, seconds=args.burst_seconds, rate=args.burst_rate,
+                                                      rmat_only=True)
     elif not args.no_extras:
         g.close()
         del depth, flush
@@ -636,6 +639,20 @@ def run_deep(args):
         nl = np.array([x.narrow_levels for x in st])
         # two sources against the CPU oracle, one of them also against the grid-wide path alone
         rows = [g.bfs(int(s))[0] for s in srcs[:2]]
+        batch = None
+        if name.startswith("grid"):
+            # the same sources as one batch call (on a deep graph: concurrent single-source
+            # lanes, one cluster each) against their single-source traversals back to back
+            nb = len(srcs)
+            brows = torch.empty((nb, V), dtype=torch.int32, device="cuda")
+            stb = g.bfs_batch_device([int(s) for s in srcs], brows.data_ptr())  # probe, build, warm
+            tb = [g.bfs_batch_device([int(s) for s in srcs], brows.data_ptr())[0].device_ms for _ in range(2)]
+            brow = [brows[i].cpu().numpy() for i in (0, nb - 1)]
+            del brows
+            batch = {"sources": nb, "ms": round(min(tb), 3), "single_source_total_ms": round(float(ms.sum()), 3),
+                     "speedup_vs_single": round(float(ms.sum()) / min(tb), 2),
+                     "mode": "concurrent single-source lanes" if stb[0].narrow_levels > 0 else "bitwise",
+                     "rows_oracle_checked": 2}
         o = g.opts
         o.narrow_max_frontier = 0
         g.opts = o
@@ -644,6 +661,8 @@ def run_deep(args):
         host = g.download()
         g.close()
         bad = oracle_rows(host, [int(s) for s in srcs[:2]], lambda j: rows[j])
+        if batch is not None:
+            batch["oracle_mismatches"] = oracle_rows(host, [int(srcs[0]), int(srcs[-1])], lambda j: brow[j])
         del host
         out[name] = {"vertices": V, "sources": len(srcs), "ms_per_bfs_mean": round(float(ms.mean()), 3),
                      "gteps_harmonic": round(len(m) / float(np.sum(ms * 1e-3 / m)) / 1e9, 3),
@@ -654,6 +673,8 @@ def run_deep(args):
                      "same_depths_with_small_frontier_mode_off": bool(np.array_equal(on, off)),
                      "oracle_checked": 2, "oracle_mismatches": bad,
                      "autotuned": tuned}
+        if batch is not None:
+            out[name]["batched"] = batch
         del depth
         torch.cuda.empty_cache()
     return out
@@ -720,25 +741,28 @@ def run_ingest(args):
     return out
 
 
-def run_serving(args, rank=0, seconds=None, raw=False):
+def run_serving(args, rank=0, seconds=None, raw=False, rate=None, rmat_only=False):
     """Poisson stream of BFS queries against 16 device-resident graphs (12
     R-MAT s14-22 ef16, 4 grids 1024^2..2048^2 with 10% of edges dropped):
     continuous batching, admission by HBM depth rows, latency percentiles.
-    rank > 0 draws its own query stream (replicas); raw adds the latencies."""
+    rank > 0 draws its own query stream (replicas); raw adds the latencies;
+    rmat_only serves the 12 R-MAT graphs alone (the load point where queries
+    queue and the batched slots take them)."""
     import torch
     import enterprise_b200 as eb
     rmat_scales = [14, 15, 16, 17, 18, 18, 19, 19, 20, 20, 21, 22]
     graphs, begs, hosts = [], [], []
     for k, sc in enumerate(rmat_scales):
         graphs.append(eb.Graph.rmat(sc, 16, seed=0xC5000 + k, **RMAT))
-    for k, w in enumerate([1024, 1448, 1774, 2048]):
+    for k, w in enumerate([] if rmat_only else [1024, 1448, 1774, 2048]):
         graphs.append(eb.Graph.grid(w, w, 0.1, seed=0xC5100 + k))
     for gk in graphs:
         hosts.append(gk.download())  # for the oracle's check of the sampled queries
         begs.append(hosts[-1].beg_pos)
     pools = [eb.pick_sources(b, 0xC5200 + k + 1000 * rank, 512) for k, b in enumerate(begs)]
-    rng = np.random.default_rng(0xC5 + 1000 * rank)
-    duration, rate = (args.serve_seconds if seconds is None else seconds), args.serve_rate
+    rng = np.random.default_rng(0xC5 + 1000 * rank + (7 if rmat_only else 0))
+    duration = args.serve_seconds if seconds is None else seconds
+    rate = args.serve_rate if rate is None else rate
     n_q = int(rng.poisson(rate * duration))
     arrivals = np.sort(rng.uniform(0, duration, n_q))
     which = rng.integers(0, len(graphs), n_q)
@@ -782,7 +806,8 @@ def run_serving(args, rank=0, seconds=None, raw=False):
     checks = len(samples)
     lat = np.array(lat)
     extra = {"latencies_ms": [float(x) for x in lat]} if raw else {}
-    return {**extra, "graphs": "12 R-MAT s14-22 ef16 + 4 grids 1024^2,1448^2,1774^2,2048^2 (10% edges dropped)",
+    return {**extra, "graphs": "12 R-MAT s14-22 ef16" + ("" if rmat_only else
+                                                           " + 4 grids 1024^2,1448^2,1774^2,2048^2 (10% edges dropped)"),
             "arrival": f"Poisson {rate}/s for {duration} s ({n_q} queries, seeded)",
             "completed": int(done), "wall_s": round(wall, 2), "throughput_qps": round(done / wall, 1),
             "gteps": round(edges / wall / 1e9, 2),
@@ -936,6 +961,9 @@ def main():
     ap.add_argument("--batch-loop", choices=["graph", "host"], default="graph",
                     help="host: drive each batch level by level from the host (kernels visible to ncu)")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving run length (the configuration's 60 s)")
+    ap.add_argument("--burst-rate", type=float, default=40000.0,
+                    help="second serving point: R-MAT graphs only, at a rate where queries queue")
+    ap.add_argument("--burst-seconds", type=float, default=10.0, help="its length (0: skip it)")
     ap.add_argument("--serve-seconds-multi", type=float, default=20.0,
                     help="serving run length per rank when --gpus N > 1 (replicas, one stream each)")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
@@ -946,7 +974,7 @@ def main():
     ap.add_argument("--deep-graphs", default="grid,er", help="graphs of the high-diameter/uniform leg")
     ap.add_argument("--deep-sources", type=int, default=32)
     ap.add_argument("--ingest-scale", type=int, default=24)
-    ap.add_argument("--only", choices=["batch", "serve", "deep", "ingest"], default=None,
+    ap.add_argument("--only", choices=["batch", "serve", "deep", "ingest", "burst"], default=None,
                     help="run only one of the extra measurements and print it")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -964,8 +992,9 @@ def main():
         dist = tdist
     try:
         if args.only:
-            line = {"batch": run_batched, "serve": run_serving, "deep": run_deep,
-                    "ingest": run_ingest}[args.only](args)
+            line = {"batch": run_batched, "serve": run_serving, "deep": run_deep, "ingest": run_ingest,
+                    "burst": lambda a: run_serving(a, seconds=a.burst_seconds, rate=a.burst_rate, rmat_only=True)
+                    }[args.only](args)
         elif args.impl == "reference":
             line = run_reference(args, rank, world)
         else:

@@ -60,7 +60,8 @@ class _Opts(C.Structure):
         ("batch_alpha", C.c_double), ("batch_small_max", C.c_int32), ("batch_large_min", C.c_int32),
         ("batch_heavy", C.c_int32), ("narrow_max_frontier", C.c_int32), ("narrow_max_edges", C.c_int32),
         ("narrow_max_degree", C.c_int32), ("narrow_cluster", C.c_int32), ("fault_inject", C.c_int32),
-        ("batch_narrow", C.c_int32), ("batch_narrow_levels", C.c_int32),
+        ("batch_deep", C.c_int32), ("batch_deep_levels", C.c_int32), ("batch_deep_cluster", C.c_int32),
+        ("batch_deep_lanes", C.c_int32),
     ]
 
 
@@ -122,8 +123,10 @@ class BfsOpts:
     narrow_max_degree: int = 256
     narrow_cluster: int = 0
     fault_inject: int = 0  # test hook: 1 makes a bounded device wait run out (ENT_ERR_TIMEOUT)
-    batch_narrow: int = 1  # batched small-frontier mode: 0 off, 1 auto (deep graphs), 2 on
-    batch_narrow_levels: int = 64
+    batch_deep: int = 1  # batches on deep graphs as concurrent single-source lanes: 0 never, 1 auto, 2 always
+    batch_deep_levels: int = 64
+    batch_deep_cluster: int = 0
+    batch_deep_lanes: int = 0
 
     def _c(self) -> _Opts:
         return _Opts(**{f.name: getattr(self, f.name) for f in fields(self)})

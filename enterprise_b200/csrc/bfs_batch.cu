@@ -1073,8 +1073,6 @@ struct BatchWorkspace {
   void* slab = nullptr;
   BatchCtl* ctl = nullptr;
   BatchCtl* ctl_h = nullptr;
-  int32_t* depth = nullptr;  // internal output for host-destination calls
-  size_t depth_cap = 0;
   BatchArgs args;
   int grid = 0, grid_flush = 0, grid_recycle = 0;
   size_t smem = 0, smem_flush = 0;
@@ -1096,7 +1094,6 @@ void destroy_batch_workspace(BatchWorkspace* w) {
   if (w->slab) cudaFree(w->slab);
   if (w->ctl) cudaFree(w->ctl);
   if (w->ctl_h) cudaFreeHost(w->ctl_h);
-  if (w->depth) cudaFree(w->depth);
   if (w->ev0) cudaEventDestroy(w->ev0);
   if (w->ev1) cudaEventDestroy(w->ev1);
   delete w;
@@ -1380,11 +1377,34 @@ int batch_source_stats(BatchWorkspace* w, int32_t n_src, cudaStream_t s, ent_sta
 
 int batch_max_sources(const BatchWorkspace* w) { return w->cap_src; }
 
+// Whether a batch on g runs as concurrent single-source lanes: by option, and
+// in auto mode by the graph's depth, probed once per graph.
+static int choose_deep(ent_graph* g, const int32_t* src, int32_t n_src, bool* deep) {
+  *deep = false;
+  if (g->opts.batch_deep == 0) return ENT_OK;
+  if (g->opts.batch_deep == 2) {
+    *deep = true;
+    return ENT_OK;
+  }
+  if (g->probe_levels < 0) {
+    int32_t lv = 0;
+    const int rc = probe_graph_levels(g, src, n_src, &lv);
+    if (rc != ENT_OK) return rc;
+    g->probe_levels = lv;
+  }
+  *deep = g->probe_levels >= g->opts.batch_deep_levels;
+  return ENT_OK;
+}
+
 int run_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, cudaStream_t stream,
                   ent_stats* stats, bool bytes) {
   for (int i = 0; i < n_src; ++i)
     if (src[i] < 0 || src[i] >= g->V) return fail(ENT_ERR_INVALID_ARG, "source %d out of range", src[i]);
-  int rc = ensure_batch(g, n_src);
+  bool deep = false;
+  int rc = choose_deep(g, src, n_src, &deep);
+  if (rc != ENT_OK) return rc;
+  if (deep) return run_bfs_deep(g, src, n_src, depth_dev, bytes, stream, stats);
+  rc = ensure_batch(g, n_src);
   if (rc != ENT_OK) return rc;
   BatchWorkspace* w = g->bws;
   cudaStream_t s = stream ? stream : g->stream;
@@ -1426,8 +1446,8 @@ int ent_bfs_batch_device_u8(ent_graph* g, const int32_t* src, int32_t n_src, uin
   return run_bfs_batch(g, src, n_src, reinterpret_cast<int32_t*>(depth_dev), (cudaStream_t)stream, stats, true);
 }
 
-// Host rows of either type: the batch writes them into the workspace's
-// device buffer, then one copy brings them back.
+// Host rows of either type: the batch writes them into the graph's staging
+// buffer on the device, then one copy brings them back.
 static int batch_to_host(ent_graph* g, const int32_t* src, int32_t n_src, void* depth_out, bool bytes,
                          ent_stats* stats) {
   clear_error();
@@ -1435,22 +1455,19 @@ static int batch_to_host(ent_graph* g, const int32_t* src, int32_t n_src, void* 
   if (n_src > MAX_BATCH) return fail(ENT_ERR_UNSUPPORTED, "at most %d sources per batch", MAX_BATCH);
   std::lock_guard<std::mutex> lk(g->mu);
   DeviceGuard dg(g->device);
-  int rc = ensure_batch(g, n_src);
-  if (rc != ENT_OK) return rc;
-  BatchWorkspace* w = g->bws;
   const size_t need = (bytes ? 1 : sizeof(int32_t)) * (size_t)n_src * g->V;
-  if (w->depth_cap < need) {
-    if (w->depth) cudaFree(w->depth);
-    w->depth = nullptr;
-    w->depth_cap = 0;
-    ENT_CUDA(cudaMalloc(&w->depth, need));
-    w->depth_cap = need;
+  if (g->stage_cap < need) {
+    if (g->stage) cudaFree(g->stage);
+    g->stage = nullptr;
+    g->stage_cap = 0;
+    ENT_CUDA(cudaMalloc(&g->stage, need));
+    g->stage_cap = need;
   }
   std::vector<ent_stats> local(stats ? 0 : n_src);
-  rc = run_bfs_batch(g, src, n_src, w->depth, g->stream, stats ? stats : local.data(), bytes);
+  int rc = run_bfs_batch(g, src, n_src, static_cast<int32_t*>(g->stage), g->stream, stats ? stats : local.data(), bytes);
   // a byte row past depth 254 still holds the other sources' complete rows
   if (rc != ENT_OK && !(bytes && rc == ENT_ERR_UNSUPPORTED)) return rc;
-  if (depth_out) ENT_CUDA(cudaMemcpyAsync(depth_out, w->depth, need, cudaMemcpyDeviceToHost, g->stream));
+  if (depth_out) ENT_CUDA(cudaMemcpyAsync(depth_out, g->stage, need, cudaMemcpyDeviceToHost, g->stream));
   ENT_CUDA(cudaStreamSynchronize(g->stream));
   return rc;
 }

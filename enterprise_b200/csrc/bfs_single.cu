@@ -1461,6 +1461,179 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, c
   return ENT_OK;
 }
 
+int probe_graph_levels(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* levels) {
+  *levels = 0;
+  if (!g->ws) {
+    int rc = create_workspace(g, &g->ws);
+    if (rc != ENT_OK) return rc;
+  }
+  int tried = 0;
+  for (int32_t i = 0; i < n_src && tried < 3; ++i) {
+    if (i > 0 && src[i] == src[i - 1]) continue;
+    ent_stats st{};
+    int rc = run_bfs_single(g, src[i], g->ws->depth, nullptr, g->stream, &st);
+    if (rc != ENT_OK) return rc;
+    ++tried;
+    *levels = std::max(*levels, st.levels);
+    if (st.reached_vertices * 4 >= g->V) break;  // a source in the bulk of the graph
+  }
+  return ENT_OK;
+}
+
+// ---------------------------------------------------------- deep batches --
+// A batch of sources on a deep graph runs as concurrent single-source
+// traversals, "lanes": each lane is a workspace with its own instantiated
+// CUDA graph and stream, whose small-frontier levels run inside its own
+// cluster of batch_deep_cluster CTAs, and the lanes take the sources round
+// robin. On such graphs a bitwise batch saves nothing (frontiers of different
+// sources are disjoint rings, so per-level work grows with the sources) and
+// pays grid-wide launches per level; lanes instead fill the GPU with as many
+// clusters as it holds, each paying only its own level chain.
+struct DeepLanes {
+  int asked = 0;                     // cluster size the lanes were built for
+  int cluster = 0;                   // CTAs per lane's cluster as built (the GPU may allow fewer)
+  std::vector<BfsWorkspace*> w;
+  std::vector<cudaStream_t> s;
+  std::vector<cudaEvent_t> done;
+  cudaEvent_t start = nullptr, end = nullptr;
+  BfsCtl* ctl_h = nullptr;           // pinned: each source's final control block
+  int32_t ctl_cap = 0;
+};
+
+void destroy_deep_lanes(DeepLanes* l) {
+  if (!l) return;
+  for (cudaStream_t s : l->s)
+    if (s) cudaStreamSynchronize(s);
+  for (BfsWorkspace* w : l->w) destroy_bfs_workspace(w);
+  for (cudaStream_t s : l->s)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : l->done)
+    if (e) cudaEventDestroy(e);
+  if (l->start) cudaEventDestroy(l->start);
+  if (l->end) cudaEventDestroy(l->end);
+  if (l->ctl_h) cudaFreeHost(l->ctl_h);
+  delete l;
+}
+
+// Byte depths of one row at any alignment (the rows of a batch start at
+// multiples of V bytes): depth d (0..254) as d, unreached (-1) as 255.
+__global__ void __launch_bounds__(256) k_depth_u8_row(const int32_t* __restrict__ d, uint8_t* __restrict__ o,
+                                                      int64_t V) {
+  const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < V; j += nth) {
+    const int x = __ldcs(d + j);
+    o[j] = (uint8_t)((x < 0 ? 255 : x) & 0xFF);
+  }
+}
+
+// Lanes the GPU runs at once: as many clusters of the lanes' size as it holds
+// (at most 32, each lane's workspace holding about 11 words per vertex), or
+// the option's cap.
+static int lane_cap(const ent_graph* g, const DeepLanes* l) {
+  const int cap = std::max(1, std::min(32, g->num_sms / std::max(1, l->cluster)));
+  return g->opts.batch_deep_lanes > 0 ? std::min(g->num_sms, g->opts.batch_deep_lanes) : cap;
+}
+
+// Cluster size of the lanes for a batch of n sources: the option, or else the
+// largest power of two in [4, 16] with n lanes of it fitting the GPU's SMs
+// (measured on the 4096^2 grid: 8 sources run fastest with 8-16 CTAs per
+// lane, 32 or more with 4).
+static int lane_cluster(const ent_graph* g, int n) {
+  if (g->opts.batch_deep_cluster > 0) return g->opts.batch_deep_cluster;
+  int c = 16;
+  while (c > 4 && (int64_t)c * n > g->num_sms) c >>= 1;
+  return c;
+}
+
+// Builds lanes up to `want` (at least one, at most lane_cap) for a batch of
+// n_src sources; lanes of another cluster size are rebuilt.
+static int ensure_lanes(ent_graph* g, int n_src) {
+  const int asked = lane_cluster(g, n_src);
+  if (g->lanes && g->lanes->asked != asked) {
+    destroy_deep_lanes(g->lanes);
+    g->lanes = nullptr;
+  }
+  if (!g->lanes) {
+    g->lanes = new DeepLanes();
+    g->lanes->asked = asked;
+    ENT_CUDA(cudaEventCreate(&g->lanes->start));
+    ENT_CUDA(cudaEventCreate(&g->lanes->end));
+  }
+  DeepLanes* l = g->lanes;
+  int want = n_src;
+  if (!l->w.empty()) want = std::min(want, lane_cap(g, l));
+  while ((int)l->w.size() < want) {
+    BfsWorkspace* w = nullptr;
+    int rc = create_workspace(g, &w, true, asked);
+    if (rc != ENT_OK) return rc;
+    l->w.push_back(w);
+    cudaStream_t s = nullptr;
+    cudaEvent_t e = nullptr;
+    ENT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    l->s.push_back(s);
+    ENT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    l->done.push_back(e);
+    if (l->w.size() == 1) {
+      l->cluster = std::max(1, w->narrow_nc);
+      want = std::min(want, lane_cap(g, l));
+    }
+  }
+  return ENT_OK;
+}
+
+int run_bfs_deep(ent_graph* g, const int32_t* src, int32_t n_src, void* depth_dev, bool bytes, cudaStream_t stream,
+                 ent_stats* stats) {
+  int rc = ensure_lanes(g, n_src);
+  if (rc != ENT_OK) return rc;
+  DeepLanes* l = g->lanes;
+  const int n_lanes = std::min<int>((int)l->w.size(), n_src);
+  if (l->ctl_cap < n_src) {
+    if (l->ctl_h) cudaFreeHost(l->ctl_h);
+    l->ctl_h = nullptr;
+    l->ctl_cap = 0;
+    ENT_CUDA(cudaMallocHost(&l->ctl_h, sizeof(BfsCtl) * (size_t)n_src));
+    l->ctl_cap = n_src;
+  }
+  cudaStream_t cs = stream ? stream : g->stream;
+  const int64_t V = g->V;
+  ENT_CUDA(cudaEventRecord(l->start, cs));
+  for (int k = 0; k < n_lanes; ++k) ENT_CUDA(cudaStreamWaitEvent(l->s[k], l->start, 0));
+  const int pack_blocks = (int)std::min<int64_t>((V + 255) / 256, (int64_t)g->num_sms * 8);
+  for (int32_t i = 0; i < n_src; ++i) {
+    const int k = i % n_lanes;
+    BfsWorkspace* w = l->w[k];
+    int32_t* row = bytes ? w->depth : static_cast<int32_t*>(depth_dev) + (size_t)i * V;
+    rc = launch_graph(w, src[i], row, nullptr, l->s[k]);
+    if (rc != ENT_OK) return rc;
+    if (bytes)
+      k_depth_u8_row<<<pack_blocks, 256, 0, l->s[k]>>>(w->depth, static_cast<uint8_t*>(depth_dev) + (size_t)i * V, V);
+    ENT_CUDA(cudaGetLastError());
+    ENT_CUDA(cudaMemcpyAsync(l->ctl_h + i, w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, l->s[k]));
+  }
+  for (int k = 0; k < n_lanes; ++k) {
+    ENT_CUDA(cudaEventRecord(l->done[k], l->s[k]));
+    ENT_CUDA(cudaStreamWaitEvent(cs, l->done[k], 0));
+  }
+  ENT_CUDA(cudaEventRecord(l->end, cs));
+  if (!stats) {
+    g_kernel_launches += (bytes ? 3 : 2) * (int64_t)n_src;  // reset, init (+ pack); level kernels uncounted
+    return ENT_OK;
+  }
+  ENT_CUDA(cudaEventSynchronize(l->end));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, l->start, l->end);
+  int err = 0, deep = 0;
+  for (int32_t i = 0; i < n_src; ++i) {
+    fill_stats(l->ctl_h[i], ms, &stats[i]);
+    g_kernel_launches += stats[i].launches + (bytes ? 1 : 0);
+    err |= l->ctl_h[i].err;
+    deep |= stats[i].levels > 255;
+  }
+  if (err) return fail(ENT_ERR_TIMEOUT, "device traversal reported error flags 0x%x", err);
+  if (bytes && deep) return fail(ENT_ERR_UNSUPPORTED, "a source reaches a depth above 254; byte depths hold 0..254");
+  return ENT_OK;
+}
+
 }  // namespace ent
 
 using namespace ent;

@@ -8,8 +8,10 @@
 namespace ent {
 struct BfsWorkspace;    // single-source direction-optimising traversal
 struct BatchWorkspace;  // bitwise multi-source traversal
+struct DeepLanes;       // concurrent single-source traversals of a batch on a deep graph
 void destroy_bfs_workspace(BfsWorkspace* w);
 void destroy_batch_workspace(BatchWorkspace* w);
+void destroy_deep_lanes(DeepLanes* l);
 }  // namespace ent
 
 // Device memory layout of one graph (all on `device`):
@@ -40,7 +42,10 @@ struct ent_graph {
   std::mutex mu;
   ent::BfsWorkspace* ws = nullptr;
   ent::BatchWorkspace* bws = nullptr;
-  int32_t probe_levels = -1;  // depth of the graph as probed by its first auto small-frontier batch (-1: not yet)
+  ent::DeepLanes* lanes = nullptr;
+  int32_t probe_levels = -1;  // depth of the graph as probed by its first auto-mode batch (-1: not yet)
+  void* stage = nullptr;      // device rows of batches whose results go to host memory
+  size_t stage_cap = 0;
 };
 
 namespace ent {
@@ -79,5 +84,11 @@ int run_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* dept
 // reaches a quarter of the graph ends the search). Synchronous, on g->stream;
 // the caller holds g->mu.
 int probe_graph_levels(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* levels);
+// A batch on a deep graph as concurrent single-source traversals, one per
+// lane; rows as run_bfs_batch writes them (int32, or bytes with 255 for
+// unreached). Ordered after and before `stream` like a launch on it; stats
+// (n_src entries) synchronise. The caller holds g->mu.
+int run_bfs_deep(ent_graph* g, const int32_t* src, int32_t n_src, void* depth_dev, bool bytes, cudaStream_t stream,
+                 ent_stats* stats);
 
 }  // namespace ent

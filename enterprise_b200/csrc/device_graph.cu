@@ -136,6 +136,8 @@ static void graph_free(ent_graph* g) {
   DeviceGuard dg(g->device);
   if (g->ws) destroy_bfs_workspace(g->ws);
   if (g->bws) destroy_batch_workspace(g->bws);
+  if (g->lanes) destroy_deep_lanes(g->lanes);
+  if (g->stage) cudaFree(g->stage);
   if (g->trav && g->trav != g->adj) cudaFree(g->trav);
   if (g->active) cudaFree(g->active);
   if (g->lead) cudaFree(g->lead);
@@ -335,8 +337,10 @@ void ent_bfs_opts_default(ent_bfs_opts* o) {
   o->narrow_max_degree = 256;
   o->narrow_cluster = 0;
   o->fault_inject = 0;
-  o->batch_narrow = 1;
-  o->batch_narrow_levels = 64;
+  o->batch_deep = 1;
+  o->batch_deep_levels = 64;
+  o->batch_deep_cluster = 0;
+  o->batch_deep_lanes = 0;
 }
 
 int ent_graph_create(const int64_t* beg, const int32_t* csr, int64_t V, int64_t E, int32_t gpu, ent_graph** out) {
@@ -560,17 +564,23 @@ int ent_graph_set_opts(ent_graph* g, const ent_bfs_opts* o) {
     return fail(ENT_ERR_INVALID_ARG, "need narrow_max_edges >= 0 and 1 <= narrow_max_degree <= 2^20");
   if (o->narrow_cluster < 0 || o->narrow_cluster > 16) return fail(ENT_ERR_INVALID_ARG, "narrow_cluster must be in [0, 16]");
   if (o->fault_inject < 0 || o->fault_inject > 1) return fail(ENT_ERR_INVALID_ARG, "fault_inject must be 0 or 1");
-  if (o->batch_narrow < 0 || o->batch_narrow > 2) return fail(ENT_ERR_INVALID_ARG, "batch_narrow must be 0, 1 or 2");
-  if (o->batch_narrow_levels < 1) return fail(ENT_ERR_INVALID_ARG, "batch_narrow_levels must be >= 1");
+  if (o->batch_deep < 0 || o->batch_deep > 2) return fail(ENT_ERR_INVALID_ARG, "batch_deep must be 0, 1 or 2");
+  if (o->batch_deep_levels < 1) return fail(ENT_ERR_INVALID_ARG, "batch_deep_levels must be >= 1");
+  if (o->batch_deep_cluster < 0 || o->batch_deep_cluster > 16)
+    return fail(ENT_ERR_INVALID_ARG, "batch_deep_cluster must be in [0, 16]");
+  if (o->batch_deep_lanes < 0 || o->batch_deep_lanes > 256)
+    return fail(ENT_ERR_INVALID_ARG, "batch_deep_lanes must be in [0, 256]");
   std::lock_guard<std::mutex> lk(g->mu);
   g->opts = *o;
-  if (g->ws || g->bws) {  // workspaces were built and captured with the old options
+  if (g->ws || g->bws || g->lanes) {  // workspaces were built and captured with the old options
     DeviceGuard dg(g->device);
     cudaStreamSynchronize(g->stream);
     destroy_bfs_workspace(g->ws);
     g->ws = nullptr;
     destroy_batch_workspace(g->bws);
     g->bws = nullptr;
+    destroy_deep_lanes(g->lanes);  // waits for its lanes' streams
+    g->lanes = nullptr;
   }
   return ENT_OK;
 }

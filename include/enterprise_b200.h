@@ -99,15 +99,21 @@ typedef struct ent_bfs_opts {
                               tiles that wait for it run out their bounded spin
                               (about a second) and the traversal returns
                               ENT_ERR_TIMEOUT with the context still usable */
-  /* small-frontier mode of the batched traversal, for deep graphs (grids,
-     road-like graphs): one thread-block cluster runs every level of a batch of
-     up to 256 sources inside one launch, top-down, writing each (source,
-     vertex) depth as it is found, instead of grid-wide launches per level.
-     0 = off, 1 = auto (on when a probe traversal of the graph, run once per
-     graph by its first such batch, has at least batch_narrow_levels levels),
-     2 = on. */
-  int32_t batch_narrow;
-  int32_t batch_narrow_levels;
+  /* Batches on deep graphs (grids, road-like graphs): their thousands of small
+     levels would cost a grid-wide bitwise batch two launches each, and sources
+     on such graphs share little frontier, so the batch runs instead as
+     concurrent single-source traversals ("lanes"), each running its small
+     frontiers inside its own thread-block cluster of batch_deep_cluster CTAs,
+     as many lanes as the GPU holds clusters (or batch_deep_lanes), each
+     writing its source's row. batch_deep: 0 = never, 1 = auto (when a probe
+     traversal of the graph, run once per graph by its first batch, has at
+     least batch_deep_levels levels), 2 = always. */
+  int32_t batch_deep;
+  int32_t batch_deep_levels;
+  int32_t batch_deep_cluster; /* CTAs per lane's cluster (1..16); 0 = per batch, the
+                                 largest power of two in [4, 16] whose n_src clusters
+                                 fit the SMs                                           */
+  int32_t batch_deep_lanes;   /* concurrent lanes at most, 0 = as many as fit          */
 } ent_bfs_opts;
 
 typedef struct ent_stats {

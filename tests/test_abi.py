@@ -39,7 +39,7 @@ def test_abi_version_and_defaults(eb):
 
 def test_struct_layout_matches_header(eb):
     import ctypes
-    assert ctypes.sizeof(eb._Opts) == 4 + 4 + 8 * 3 + 4 * 5 + 4 + 8 + 4 * 10
+    assert ctypes.sizeof(eb._Opts) == 4 + 4 + 8 * 3 + 4 * 5 + 4 + 8 + 4 * 12
     assert ctypes.sizeof(eb._Stats) == 8 + 8 + 4 * 4 + 8 + 4 * 2
     assert ctypes.sizeof(eb._ServerOpts) == 4 * 4 + 8 + 4 * 6
     assert ctypes.sizeof(eb._ServerCounters) == 8 * 9 + 4 * 2 + 8

@@ -52,23 +52,94 @@ def test_duplicate_and_isolated_sources(eb, orc):
         _check_rows(eb, orc, csr, depth, stats, srcs)
 
 
-def test_tier_graph_deep_levels(eb, orc):
-    """~1000 levels: the level log wraps through many flush windows."""
+def _mode(g, deep):
+    o = g.opts
+    o.batch_deep = deep
+    g.opts = o
+
+
+@pytest.mark.parametrize("deep", [0, 2])
+def test_tier_graph_deep_levels(eb, orc, deep):
+    """~1000 levels: the bitwise batch's level log wraps through many flush
+    windows; as concurrent single-source lanes, each source runs on its own."""
     V, s, d = tier_graph()
     csr = eb.Csr.from_edges(s, d, V)
     srcs = [0, 1, 3000, 3041, 4999, 5999, 5500, 2, 2]
     with eb.Graph.from_csr(csr) as g:
+        _mode(g, deep)
         depth, stats = g.bfs_batch(srcs)
         _check_rows(eb, orc, csr, depth, stats, srcs)
 
 
-def test_grid_batch(eb, orc):
+@pytest.mark.parametrize("deep", [0, 1, 2])
+def test_grid_batch(eb, orc, deep):
     csr = eb.Csr.grid(48, 40, 0.1, seed=4)
     srcs = eb.pick_sources(csr.beg_pos, 3, 100)
     with eb.Graph.from_csr(csr) as g:
+        _mode(g, deep)
         depth, stats = g.bfs_batch(srcs)
         _check_rows(eb, orc, csr, depth, stats, srcs)
 
+
+@pytest.mark.parametrize("n", [1, 7, 64, 65, 300])
+def test_deep_batch_lanes_on_a_grid(eb, orc, n):
+    """A batch on a deep grid runs as concurrent single-source lanes, forced and
+    in auto mode (the probe finds the grid deep), with at most 3 lanes and with
+    as many as fit: every row against the oracle; each source's statistics are
+    its own traversal's (small-frontier levels included)."""
+    csr = eb.Csr.grid(160, 120, 0.1, seed=33 + n)
+    srcs = [int(s) for s in eb.pick_sources(csr.beg_pos, 900 + n, n)]
+    with eb.Graph.from_csr(csr) as g:
+        for deep, lanes in ((2, 3), (1, 0)):
+            o = g.opts
+            o.batch_deep, o.batch_deep_lanes = deep, lanes
+            g.opts = o
+            depth, stats = g.bfs_batch(srcs)
+            _check_rows(eb, orc, csr, depth, stats, srcs)
+            assert all(st.narrow_levels > 0 for st in stats)
+
+
+def test_deep_batch_lanes_device_rows_and_streams(eb, orc):
+    """Device rows through a caller's stream: the call returns before the lanes
+    finish, and work queued on that stream after it sees complete rows."""
+    import torch
+    csr = eb.Csr.grid(200, 90, 0.1, seed=8)
+    srcs = [int(s) for s in eb.pick_sources(csr.beg_pos, 81, 40)]
+    with eb.Graph.from_csr(csr) as g:
+        _mode(g, 2)
+        rows = torch.full((len(srcs), g.vert_count), 7, dtype=torch.int32, device="cuda")
+        strm = torch.cuda.Stream()
+        with torch.cuda.stream(strm):
+            g.bfs_batch_device(srcs, rows.data_ptr(), stream=strm.cuda_stream, stats=False)
+            total = rows.sum(dim=1)  # queued behind the batch on the same stream
+        strm.synchronize()
+        host = rows.cpu().numpy()
+        for i in (0, 13, 39):
+            exp, _ = orc.bfs(csr.beg_pos, csr.csr, srcs[i])
+            np.testing.assert_array_equal(host[i], exp)
+        assert total.cpu().tolist() == host.sum(axis=1).tolist()
+
+
+def test_deep_batch_lanes_on_shallow_and_small_graphs(eb, orc):
+    """Forced onto R-MAT (hubs of thousands of edges, a few levels) and onto a
+    graph with repeated, isolated and small-component sources: the same rows.
+    Auto mode leaves R-MAT to the bitwise batch."""
+    csr = eb.Csr.rmat(13, 16, seed=4242)
+    srcs = [int(s) for s in eb.pick_sources(csr.beg_pos, 4243, 100)]
+    with eb.Graph.from_csr(csr) as g:
+        _mode(g, 2)
+        depth, stats = g.bfs_batch(srcs)
+        _check_rows(eb, orc, csr, depth, stats, srcs)
+        _mode(g, 1)
+        depth, stats = g.bfs_batch(srcs)
+        _check_rows(eb, orc, csr, depth, stats, srcs)
+        assert all(st.narrow_levels == 0 for st in stats)  # the bitwise batch ran
+    csr = eb.Csr.from_edges([0, 1, 2, 3, 9], [1, 2, 3, 4, 10], 12)  # 5..8, 11 isolated
+    with eb.Graph.from_csr(csr) as g:
+        _mode(g, 2)
+        srcs = [2, 2, 0, 7, 4, 2, 6, 9, 11, 10]
+        depth, stats = g.bfs_batch(srcs)
+        _check_rows(eb, orc, csr, depth, stats, srcs)
 
 def test_batch_matches_single_and_repeats(eb, orc):
     csr = eb.Csr.rmat(14, 16, seed=77)
@@ -178,13 +249,15 @@ def test_byte_rows_match_int32_rows(eb, orc, n):
             np.testing.assert_array_equal(d8[i], np.where(exp < 0, 255, exp).astype(np.uint8))
 
 
-def test_byte_rows_refuse_depths_above_254(eb, orc):
+@pytest.mark.parametrize("deep", [0, 2])
+def test_byte_rows_refuse_depths_above_254(eb, orc, deep):
     """A 300-vertex path (depths up to 299, several flush windows): the call
     reports ENT_ERR_UNSUPPORTED; the row of a source whose depths stay below
     255 is still complete."""
     n = 300
     csr = eb.Csr.from_edges(np.arange(n - 1), np.arange(1, n), n)
     with eb.Graph.from_csr(csr) as g:
+        _mode(g, deep)
         out = np.zeros((2, n), dtype=np.uint8)
         with pytest.raises(eb.EntError, match="byte depths") as ei:
             g.bfs_batch_u8([150, 0], depth_out=out)
