@@ -195,8 +195,13 @@ def run_ours(args, rank, world, dist):
         from enterprise_b200 import tune
         t0 = time.time()
         tune_srcs = eb.pick_sources(beg, source_seed(args.scale, rank) + 0x7E57, 16)  # disjoint from the timed set
-        opts, ms, hit = tune.autotune(g, tune_srcs, "single", reps=2, label="rmat", device=local)
+        cache = tune.TuneCache()
+        key = tune.TuneCache.key(tune.gpu_name(local), tune.graph_class(V, E, "rmat"), "single")
+        where = cache.source(key)
+        opts, ms, hit = tune.autotune(g, tune_srcs, "single", reps=2, label="rmat", device=local, cache=cache)
         tuned = {"opts": {k: v for k, v in vars(opts).items() if k != "fault_inject"}, "cached": hit,
+                 "cache": {"user": "this machine's tuning cache", "shipped": "the package's shipped results of an "
+                           "earlier search on this GPU model (enterprise_b200/tuned/b200.json)"}.get(where, "searched now"),
                  "search_s": round(time.time() - t0, 2)}
 
     if args.opts:  # explicit traversal options (on top of the tuner's or the defaults)
@@ -816,7 +821,8 @@ def run_serving(args, rank=0, seconds=None, raw=False, rate=None, rmat_only=Fals
             "p999_ms": round(float(np.percentile(lat, 99.9)), 3) if len(lat) else None,
             "queue_p50_ms": round(float(np.percentile(qwait, 50)), 3) if len(qwait) else None,
             "batches": c["batches"], "mean_batch": round(c["launched"] / max(1, c["batches"]), 2),
-            "max_batch_seen": c["max_batch_seen"], "oracle_checked": checks,
+            "max_batch_seen": c["max_batch_seen"], "joined_running_batches": c["joined"],
+            "fast_slot_queries": c["fast_launches"], "oracle_checked": checks,
             "sampled_exact": not mismatches and bad_status == 0, "bad_status": bad_status,
             "mismatches": mismatches[:5], "max_batch": args.serve_batch, "slots_per_graph": args.serve_slots, "single_cluster": args.serve_cluster,
             "single_source_graphs": c["single_graphs"],

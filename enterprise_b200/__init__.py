@@ -86,7 +86,7 @@ class _ServerOpts(C.Structure):
                 ("max_pending", C.c_int32), ("hbm_budget_bytes", C.c_int64),
                 ("single_source_levels", C.c_int32), ("single_slots", C.c_int32),
                 ("fast_slots", C.c_int32), ("fast_max_waiting", C.c_int32), ("single_cluster", C.c_int32),
-                ("pad", C.c_int32)]
+                ("join", C.c_int32)]
 
 
 class _QueryResult(C.Structure):
@@ -98,7 +98,8 @@ class _QueryResult(C.Structure):
 class _ServerCounters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("submitted", "rejected", "completed", "released", "batches", "launched",
                                          "pending", "rows_total", "rows_free")] + \
-               [("max_batch_seen", C.c_int32), ("single_graphs", C.c_int32), ("fast_launches", C.c_int64)]
+               [("max_batch_seen", C.c_int32), ("single_graphs", C.c_int32), ("fast_launches", C.c_int64),
+                ("joined", C.c_int64)]
 
 
 @dataclass
@@ -728,10 +729,11 @@ class Server:
     def __init__(self, graphs: Sequence[Graph], max_batch: int = 64, slots_per_graph: int = 2,
                  rows_per_graph: int = 0, max_pending: int = 1 << 20, hbm_budget_bytes: int = 0,
                  single_source_levels: int = 64, single_slots: int = 8, fast_slots: int = 2,
-                 fast_max_waiting: int = 2, single_cluster: int = 8):
+                 fast_max_waiting: int = 2, single_cluster: int = 8, join: bool = True):
         self.graphs = list(graphs)
         o = _ServerOpts(max_batch, slots_per_graph, rows_per_graph, max_pending, hbm_budget_bytes,
-                        single_source_levels, single_slots, fast_slots, fast_max_waiting, single_cluster, 0)
+                        single_source_levels, single_slots, fast_slots, fast_max_waiting, single_cluster,
+                        1 if join else 0)
         hs = (_P * len(graphs))(*[g.handle for g in graphs])
         h = _P()
         _check(lib().ent_server_create(hs, len(graphs), C.byref(o), C.byref(h)))

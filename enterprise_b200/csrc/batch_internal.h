@@ -4,6 +4,22 @@
 #include "dev_graph.h"
 
 namespace ent {
+// Sources that join a running bitwise batch at its next level boundary. Lives
+// in mapped, page-locked host memory: the host fills the entries, then bumps
+// seq (release); the batch's level finisher, seeing seq != taken, adds the
+// entries to the next level's frontier and stores taken = seq (release). A
+// post the batch never took (it ended first) stays with taken != seq.
+constexpr int JOIN_MAX = 2048;
+struct JoinBox {
+  int32_t seq;            // written by the host
+  int32_t taken;          // written by the device
+  int32_t n;              // entries of the post
+  int32_t pad;
+  int32_t pos[JOIN_MAX];  // bit position (source slot) in the batch
+  int32_t src[JOIN_MAX];  // source vertex
+  int32_t row[JOIN_MAX];  // depth row (row_map entry) of the source
+};
+
 // Traversal state for one batched run of up to words_for(n_src)*64 sources.
 int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out);
 // Adds one independent branch (memsets, seed, while{expand, commit, flush,
@@ -15,6 +31,12 @@ int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream
 // points at n_src x V bytes.
 int stage_request(ent_graph* g, BatchWorkspace* w, const int32_t* src, int32_t n_src, int32_t* depth_dev,
                   cudaStream_t s, const int32_t* row_map_dev, bool bytes = false);
+// Gives w's branch a join mailbox (device address of a mapped JoinBox); call
+// before append_branch. With one, the batch's n_src may grow while it runs and
+// row_map_dev must hold JOIN_MAX entries.
+void set_join_box(BatchWorkspace* w, JoinBox* box_dev);
+// Sources that joined w's last run (valid after batch_source_stats).
+int batch_joined(const BatchWorkspace* w);
 int batch_source_stats(BatchWorkspace* w, int32_t n_src, cudaStream_t s, ent_stats* stats);
 int batch_max_sources(const BatchWorkspace* w);
 

@@ -30,6 +30,7 @@
 #include <string.h>
 #include <vector>
 
+#include "batch_internal.h"
 #include "dev_common.cuh"
 #include "dev_graph.h"
 
@@ -59,6 +60,9 @@ struct BatchCtl {
   int64_t m_f, m_done;
   uint32_t finished;
   int32_t out_bytes;  // depth rows are uint8 (the reference's depth type, 255 = unreached), not int32
+  int32_t clear_done; // sources joined: the completion bits no longer hold (k_b_recycle clears them)
+  int32_t joined;     // sources that joined this run
+  int32_t if_runs;    // level-loop iterations that ran the flush and recycle nodes
 };
 
 struct BatchArgs {
@@ -90,9 +94,12 @@ struct BatchArgs {
   unsigned long long* st_edges;  // per source: sum of degrees of reached vertices
   unsigned long long* st_verts;  // per source: reached vertices
   int32_t* st_maxd;              // per source: max depth
+  int32_t* join;                 // per source: the level of its depth 0 (0 unless it joined later)
+  JoinBox* box;                  // mapped mailbox of sources joining at a level boundary, or null
   double alpha;      // bottom-up when frontier edges * alpha > unfinished edges
   int32_t heavy_deg; // top-down: from this degree every CTA takes a slice of a vertex
   cudaGraphConditionalHandle cond;
+  cudaGraphConditionalHandle cond_flush;  // the level window is full: run the flush and recycle nodes
   int32_t use_cond;
   int32_t max_levels;
 };
@@ -669,6 +676,61 @@ __device__ __forceinline__ void td_commit_words(const BatchArgs& a, unsigned lon
   }
 }
 
+// The join mailbox is host memory written by the host while the batch runs.
+__device__ __forceinline__ int ld_acquire_sys(const int32_t* p) {
+  int v;
+  asm volatile("ld.acquire.sys.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_sys(int32_t* p, int v) {
+  asm volatile("st.release.sys.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Level finisher (one thread, every CTA of the level done): sources posted to
+// the join mailbox start here, at depth 0 on level L. Each takes its bit
+// position s: the bit goes into its vertex's visited words and into the slot
+// of level L's frontier, the vertex joins that frontier (once), s becomes an
+// active source, and its depths are written relative to L (join[s]). Vertices
+// marked complete lack the new bits, so their marks are dropped (k_b_recycle
+// clears them before the next level).
+__device__ void join_sources(const BatchArgs& a, volatile BatchCtl* vc, int L, int nxt, int64_t& n_next,
+                             int64_t& m_next) {
+  JoinBox* box = a.box;
+  const int seq = ld_acquire_sys(&box->seq);
+  if (seq == *(volatile int32_t*)&box->taken) return;
+  const int nj = *(volatile int32_t*)&box->n;
+  unsigned long long* F = slot_ptr(a, L - vc->base);
+  int32_t* rows = const_cast<int32_t*>(vc->row_map);
+  for (int j = 0; j < nj && j < JOIN_MAX; ++j) {
+    const int s = *(volatile int32_t*)&box->pos[j];
+    const int v = *(volatile int32_t*)&box->src[j];
+    const int r = *(volatile int32_t*)&box->row[j];
+    if (s < 0 || s >= a.W * 64 || v < 0 || v >= a.V) continue;  // the host never posts these
+    const unsigned long long bit = 1ull << (s & 63);
+    const size_t at = (size_t)v * a.W + (s >> 6);
+    a.X[at] |= bit;
+    F[at] |= bit;
+    a.act[nxt][s >> 6] |= bit;
+    a.join[s] = L;
+    if (rows) rows[s] = r;
+    if (s + 1 > vc->n_src) vc->n_src = s + 1;
+    const uint32_t tb = 1u << (v & 31);
+    if (!(a.jfb[nxt][v >> 5] & tb)) {
+      a.jfb[nxt][v >> 5] |= tb;
+      a.jf[nxt][n_next++] = v;
+      const int d = a.deg[v];
+      m_next += d;
+      if (d >= a.heavy_deg) a.heavy[nxt][vc->n_heavy[nxt]++] = v;
+    }
+  }
+  vc->n_jf[nxt] = (int32_t)n_next;
+  vc->joined = vc->joined + nj;
+  vc->clear_done = 1;
+  vc->m_done = 0;
+  __threadfence();
+  st_release_sys(&box->taken, seq);
+}
+
 // Top-down: fold the claimed bits into X and count. Both directions: clear
 // the frontier bitmap of level L (jfb[cur], its words hold only jf[cur]). Then the
 // last CTA advances the level and picks the next direction.
@@ -677,7 +739,10 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
   __shared__ int s_last;
   BatchCtl* c = a.ctl;
   if (c->done) {  // never leave the while node spinning on a finished traversal
-    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
+    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) {
+      cudaGraphSetConditional(a.cond, 0u);
+      cudaGraphSetConditional(a.cond_flush, 0u);
+    }
     return;
   }
   const int cur = c->cur, nxt = cur ^ 1;
@@ -758,12 +823,13 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
   if (!s_last || threadIdx.x != 0) return;
   __threadfence();
   volatile BatchCtl* vc = c;
-  const int64_t n_next = vc->n_jf[nxt];
-  const int64_t m_next = (int64_t)vc->acc_m;
+  int64_t n_next = vc->n_jf[nxt];
+  int64_t m_next = (int64_t)vc->acc_m;
   vc->m_done = vc->m_done + (int64_t)vc->acc_mdone;
   if (dir == 0) vc->td_levels = vc->td_levels + 1; else vc->bu_levels = vc->bu_levels + 1;
   const int L = vc->level + 1;
   vc->level = L;
+  if (a.box) join_sources(a, vc, L, nxt, n_next, m_next);
   // level L's active set is spent: it collects level L+2's from here
   for (int w = 0; w < a.W; ++w) a.act[cur][w] = 0;
   vc->cur = nxt;
@@ -786,7 +852,11 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
   vc->acc_mdone = 0;
   vc->finished = 0;
   __threadfence();
-  if (a.use_cond) cudaGraphSetConditional(a.cond, done ? 0u : 1u);
+  if (a.use_cond) {
+    cudaGraphSetConditional(a.cond, done ? 0u : 1u);
+    // flush and recycle also run when sources joined (k_b_recycle drops the completion bits)
+    cudaGraphSetConditional(a.cond_flush, (vc->flush_now || vc->clear_done) ? 1u : 0u);
+  }
 }
 
 // ----------------------------------------------------------- flush --------
@@ -903,10 +973,12 @@ __device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, in
         if (s0 >= nsrc) break;
         size_t ofs[4];  // element offset of each row's segment (int32 or byte rows)
         bool rv[4];
+        int rbase[4];   // depth of log slot 0 for the row: the window's base level less the source's start
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           rv[j] = s0 + j < nsrc;
           ofs[j] = rv[j] ? (size_t)(row_map ? row_map[s0 + j] : s0 + j) * a.V + v0 + sub : 0;
+          rbase[j] = base - (rv[j] ? a.join[s0 + j] : 0);
         }
         bool deep = false;  // a depth above 254 met in byte rows
         unsigned cnt[4] = {0, 0, 0, 0};
@@ -918,7 +990,7 @@ __device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, in
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             int d = (int)(signed char)(uint8_t)(wv >> (8 * j));
-            if (d >= 0) d += base;
+            if (d >= 0) d += rbase[j];
             if (rv[j]) {
               if (windows == 0 || d >= 0) {
                 if constexpr (BYTES) {
@@ -1008,13 +1080,18 @@ __global__ void __launch_bounds__(BB, 3) k_b_flush(BatchArgs a, int final_flush)
 
 // Recycles the log after a flush with contiguous streams: a window flush
 // copies slot K-1 (the next window's frontier) into slot 0 and zeroes slots
-// 1..K-1, then moves the window; the final flush zeroes slots 0..last.
+// 1..K-1, then moves the window; the final flush zeroes slots 0..last. After
+// sources joined at a level boundary it also clears the completion bits.
 __global__ void __launch_bounds__(BB) k_b_recycle(BatchArgs a, int final_flush) {
   BatchCtl* c = a.ctl;
-  if (!final_flush && !c->flush_now) return;
-  const int last = final_flush ? (c->level - 1 - c->base) : (a.K - 1);
-  const int64_t words = a.V * a.W;  // per slot
+  const bool clear = !final_flush && c->clear_done;  // sources joined at this level boundary
+  const bool flush = final_flush || c->flush_now;
+  if (!flush && !clear) return;
   const int64_t tid = blockIdx.x * (int64_t)BB + threadIdx.x, nth = (int64_t)gridDim.x * BB;
+  if (clear)
+    for (int64_t i = tid; i <= (a.V + 31) >> 5; i += nth) a.donebits[i] = 0u;
+  const int last = !flush ? -1 : (final_flush ? (c->level - 1 - c->base) : (a.K - 1));
+  const int64_t words = a.V * a.W;  // per slot
   // A slot starts at log + k*V*W words: 16-byte aligned for every k only when
   // V*W is even (the log base is 256-byte aligned). Otherwise use 8-byte accesses.
   const bool vec = (words & 1) == 0;
@@ -1043,9 +1120,13 @@ __global__ void __launch_bounds__(BB) k_b_recycle(BatchArgs a, int final_flush) 
   if (!s_last || threadIdx.x != 0) return;
   __threadfence();
   volatile BatchCtl* vc = c;
-  vc->base = vc->base + a.K - 1;
-  vc->windows = vc->windows + 1;
-  vc->flush_now = 0;
+  if (flush) {
+    vc->base = vc->base + a.K - 1;
+    vc->windows = vc->windows + 1;
+    vc->flush_now = 0;
+  }
+  vc->clear_done = 0;
+  vc->if_runs = vc->if_runs + 1;
   vc->finished = 0;
   __threadfence();
 }
@@ -1150,17 +1231,44 @@ int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream
   ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &prev, 1, &cp));
   prev = cond_node;
   cudaGraph_t body = cp.conditional.phGraph_out[0];
+  // Loop body: expand -> commit -> if (window full or sources joined) { flush -> recycle }.
   BatchArgs la = w->args;
   la.cond = handle;
   la.use_cond = 1;
-  ENT_CUDA(cudaStreamBeginCaptureToGraph(cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  k_b_expand<<<w->grid, BB, w->smem, cap_stream>>>(la);
-  k_b_commit<<<w->grid, BB, 0, cap_stream>>>(la);
-  k_b_flush<<<w->grid_flush, BB, w->smem_flush, cap_stream>>>(la, 0);
-  k_b_recycle<<<w->grid_recycle, BB, 0, cap_stream>>>(la, 0);
-  cudaGraph_t captured;
-  cudaError_t e = cudaStreamEndCapture(cap_stream, &captured);
-  if (e != cudaSuccess) return fail(ENT_ERR_CUDA, "batched level-loop capture failed: %s", cudaGetErrorString(e));
+  ENT_CUDA(cudaGraphConditionalHandleCreate(&la.cond_flush, body, 0, cudaGraphCondAssignDefault));
+  {
+    int zero = 0;
+    void* kl[1] = {&la};
+    void* kf[2] = {&la, &zero};
+    cudaKernelNodeParams kp = {};
+    kp.blockDim = dim3(BB);
+    kp.func = (void*)k_b_expand;
+    kp.gridDim = dim3(w->grid);
+    kp.sharedMemBytes = (unsigned)w->smem;
+    kp.kernelParams = kl;
+    cudaGraphNode_t n_expand, n_commit, n_if, n_flush, n_recycle;
+    ENT_CUDA(cudaGraphAddKernelNode(&n_expand, body, nullptr, 0, &kp));
+    kp.func = (void*)k_b_commit;
+    kp.sharedMemBytes = 0;
+    ENT_CUDA(cudaGraphAddKernelNode(&n_commit, body, &n_expand, 1, &kp));
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = la.cond_flush;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    ENT_CUDA(cudaGraphAddNode(&n_if, body, &n_commit, 1, &ip));
+    cudaGraph_t fbody = ip.conditional.phGraph_out[0];
+    kp.func = (void*)k_b_flush;
+    kp.gridDim = dim3(w->grid_flush);
+    kp.sharedMemBytes = (unsigned)w->smem_flush;
+    kp.kernelParams = kf;
+    ENT_CUDA(cudaGraphAddKernelNode(&n_flush, fbody, nullptr, 0, &kp));
+    kp.func = (void*)k_b_recycle;
+    kp.gridDim = dim3(w->grid_recycle);
+    kp.sharedMemBytes = 0;
+    ENT_CUDA(cudaGraphAddKernelNode(&n_recycle, fbody, &n_flush, 1, &kp));
+  }
+  (void)cap_stream;
   {
     int fin = 1;
     void* kargs[2] = {&a0, &fin};
@@ -1197,7 +1305,7 @@ int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
   const size_t sz_q = al(sizeof(int32_t) * (V + 4));
   const size_t sz_mask = al(sizeof(unsigned long long) * W);
   const size_t sz_src = al(sizeof(int32_t) * w->cap_src);
-  const size_t sz_st = al(sizeof(unsigned long long) * w->cap_src) * 2 + al(sizeof(int32_t) * w->cap_src);
+  const size_t sz_st = al(sizeof(unsigned long long) * w->cap_src) * 2 + 2 * al(sizeof(int32_t) * w->cap_src);
   const size_t total = sz_x + sz_log + 4 * sz_bits + 6 * sz_q + 3 * sz_mask + sz_src + sz_st + 256;
   cudaError_t e = cudaMalloc(&w->slab, total);
   if (e != cudaSuccess) { destroy_batch_workspace(w); return fail(ENT_ERR_OOM, "batch workspace (%zu bytes) failed", total); }
@@ -1250,6 +1358,8 @@ int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
   a.st_edges = (unsigned long long*)p; p += al(sizeof(unsigned long long) * w->cap_src);
   a.st_verts = (unsigned long long*)p; p += al(sizeof(unsigned long long) * w->cap_src);
   a.st_maxd = (int32_t*)p; p += al(sizeof(int32_t) * w->cap_src);
+  a.join = (int32_t*)p; p += al(sizeof(int32_t) * w->cap_src);  // zeroed with the statistics
+  a.box = nullptr;
   a.alpha = g->opts.batch_alpha;
   a.heavy_deg = g->opts.batch_heavy;
   a.max_levels = (int32_t)std::min<int64_t>(V + 2, 0x7ffffff0);
@@ -1304,6 +1414,10 @@ static int ensure_batch(ent_graph* g, int n_src) {
   return ENT_OK;
 }
 
+// Kernels one finished graph-driven run launched: seed, final flush and
+// recycle, expand and commit per level, flush and recycle where they ran.
+static int64_t run_launches(const BatchCtl& h) { return 3 + 2 * (int64_t)h.level + 2 * (int64_t)h.if_runs; }
+
 // Uploads sources, mask and the output pointer (the kernels read them from
 // device memory, so one instantiated graph serves every batch).
 int stage_request(ent_graph*, BatchWorkspace* w, const int32_t* src, int32_t n_src, int32_t* depth_dev,
@@ -1346,9 +1460,9 @@ static int read_batch_stats(ent_graph* g, BatchWorkspace* w, int32_t n_src, cuda
     stats[i].status = w->ctl_h->err;
     stats[i].device_ms = ms;
     stats[i].narrow_levels = 0;
-    stats[i].launches = 3 + 4 * w->ctl_h->level;  // shared by the batch
+    stats[i].launches = (int32_t)run_launches(*w->ctl_h);  // shared by the batch
   }
-  g_kernel_launches += 3 + 4 * (int64_t)w->ctl_h->level;
+  g_kernel_launches += run_launches(*w->ctl_h);
   return batch_status(w->ctl_h->err);
 }
 
@@ -1369,13 +1483,17 @@ int batch_source_stats(BatchWorkspace* w, int32_t n_src, cudaStream_t s, ent_sta
     stats[i].status = w->ctl_h->err;
     stats[i].device_ms = 0;
     stats[i].narrow_levels = 0;
-    stats[i].launches = 3 + 4 * w->ctl_h->level;  // shared by the batch
+    stats[i].launches = (int32_t)run_launches(*w->ctl_h);  // shared by the batch
   }
-  g_kernel_launches += 3 + 4 * (int64_t)w->ctl_h->level;
+  g_kernel_launches += run_launches(*w->ctl_h);
   return batch_status(w->ctl_h->err);
 }
 
 int batch_max_sources(const BatchWorkspace* w) { return w->cap_src; }
+
+void set_join_box(BatchWorkspace* w, JoinBox* box_dev) { w->args.box = box_dev; }
+
+int batch_joined(const BatchWorkspace* w) { return w->ctl_h->joined; }
 
 // Whether a batch on g runs as concurrent single-source lanes: by option, and
 // in auto mode by the graph's depth, probed once per graph.
@@ -1668,7 +1786,7 @@ int ent_multi_run(ent_multi* m, double* device_ms) {
   for (size_t k = 0; k < m->graphs.size(); ++k) {
     BatchWorkspace* w = m->ws[k];
     ENT_CUDA(cudaMemcpy(w->ctl_h, w->ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost));
-    g_kernel_launches += 3 + 4 * (int64_t)w->ctl_h->level;
+    g_kernel_launches += run_launches(*w->ctl_h);
     if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "graph %zu: batched traversal error flags 0x%x", k, w->ctl_h->err);
   }
   return ENT_OK;

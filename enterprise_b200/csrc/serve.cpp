@@ -44,6 +44,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstring>
 #include <deque>
 #include <mutex>
 #include <string>
@@ -74,9 +75,14 @@ struct Slot {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;
   int32_t* row_map_dev = nullptr;
-  std::vector<int64_t> qids;
+  std::vector<int64_t> qids;           // the batch's queries, in bit-position order
   bool busy = false;
   bool fast = false;                   // single-source slot of a shallow graph
+  // batched slots: queries join the running batch at a level boundary
+  ent::JoinBox* box = nullptr;         // mapped host mailbox (device sees box_dev)
+  ent::JoinBox* box_dev = nullptr;
+  std::vector<int64_t> posted;         // posted, not yet seen taken
+  int32_t next_pos = 0;                // next free bit position of the running batch
 };
 
 struct GraphState {
@@ -104,6 +110,7 @@ struct ent_server {
   std::deque<int64_t> completed;
   std::atomic<bool> stop{false};
   std::thread worker;
+  cudaStream_t prep = nullptr;      // fills the rows of joining queries with -1
   int64_t next_id = 1;
   int64_t n_pending = 0;
   ent_server_counters ctr{};
@@ -125,12 +132,23 @@ void free_server(ent_server* s) {
       if (sl.ws) destroy_batch_workspace(sl.ws);
       if (sl.sws) destroy_bfs_workspace(sl.sws);
       if (sl.row_map_dev) cudaFree(sl.row_map_dev);
+      if (sl.box) cudaFreeHost(sl.box);
       if (sl.done) cudaEventDestroy(sl.done);
       if (sl.stream) cudaStreamDestroy(sl.stream);
     }
     if (g.pool) cudaFree(g.pool);
   }
+  if (s->prep) cudaStreamDestroy(s->prep);
   delete s;
+}
+
+// Posted joins the batch took move into its query list; host side of the
+// mailbox protocol (the device stores taken = seq once it has seeded them).
+void confirm_joins(Slot& sl) {
+  if (sl.posted.empty()) return;
+  if (__atomic_load_n(&sl.box->taken, __ATOMIC_ACQUIRE) != sl.box->seq) return;
+  sl.qids.insert(sl.qids.end(), sl.posted.begin(), sl.posted.end());
+  sl.posted.clear();
 }
 
 // Retires finished slots; returns true if any finished.
@@ -142,11 +160,24 @@ bool retire(ent_server* s) {
       cudaError_t q = cudaEventQuery(sl.done);
       if (q == cudaErrorNotReady) continue;
       const Clock::time_point now = Clock::now();
+      std::vector<int64_t> untaken;  // posted joins the batch ended without
+      if (sl.box) {
+        confirm_joins(sl);
+        untaken.swap(sl.posted);
+      }
       std::vector<ent_stats> st(sl.qids.size());
       int rc = q != cudaSuccess ? fail(ENT_ERR_CUDA, "batch failed: %s", cudaGetErrorString(q))
                : sl.sws         ? bfs_single_stats(sl.sws, sl.stream, st.data())
                                 : batch_source_stats(sl.ws, (int32_t)sl.qids.size(), sl.stream, st.data());
       std::lock_guard<std::mutex> lk(s->mu);
+      if (!sl.sws && rc == ENT_OK && q == cudaSuccess) s->ctr.joined += batch_joined(sl.ws);
+      for (auto it = untaken.rbegin(); it != untaken.rend(); ++it) {  // back to the queue's front, in order
+        Query& uq = s->queries[*it];
+        g.free_rows.push_back(uq.row);
+        uq.row = -1;
+        g.pending.push_front(*it);
+        ++s->n_pending;
+      }
       for (size_t i = 0; i < sl.qids.size(); ++i) {
         auto it = s->queries.find(sl.qids[i]);
         if (it == s->queries.end()) continue;
@@ -157,6 +188,7 @@ bool retire(ent_server* s) {
         s->completed.push_back(sl.qids[i]);
       }
       s->ctr.completed += (int64_t)sl.qids.size();
+      if ((int64_t)sl.qids.size() > s->ctr.max_batch_seen) s->ctr.max_batch_seen = (int32_t)sl.qids.size();
       if (rc != ENT_OK) {
         s->worker_error = rc;
         s->worker_msg = ent_last_error();
@@ -210,6 +242,11 @@ bool launch(ent_server* s) {
       if (sl.sws) {
         rc = launch_bfs_single(sl.sws, src[0], g.pool + (size_t)rows[0] * g.V, sl.stream);
       } else {
+        sl.box->seq = 0;  // the slot is idle: nothing reads the mailbox
+        sl.box->taken = 0;
+        sl.box->n = 0;
+        sl.posted.clear();
+        sl.next_pos = n;
         e = cudaMemcpyAsync(sl.row_map_dev, rows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, sl.stream);
         rc = e == cudaSuccess ? stage_request(g.g, sl.ws, src.data(), n, g.pool, sl.stream, sl.row_map_dev)
                               : fail(ENT_ERR_CUDA, "row map upload failed");
@@ -241,12 +278,80 @@ bool launch(ent_server* s) {
   return any;
 }
 
+// Queries still waiting join running batches of their graph at the batches'
+// next level boundary: into the free bit positions of a busy batched slot
+// whose previous post was taken. Their rows are filled with -1 first (a
+// window of levels the batch flushed before they joined never writes them).
+bool join(ent_server* s) {
+  bool any = false;
+  for (GraphState& g : s->gs) {
+    for (Slot& sl : g.slots) {
+      if (!sl.busy || !sl.box) continue;
+      confirm_joins(sl);
+      if (!sl.posted.empty()) continue;  // one post in flight per batch
+      const int cap = batch_max_sources(sl.ws);
+      std::vector<int64_t> qs;
+      {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (g.pending.empty() || g.free_rows.empty() || sl.next_pos >= cap) continue;
+        const int take = (int)std::min<size_t>({(size_t)(cap - sl.next_pos), g.pending.size(), g.free_rows.size(),
+                                                (size_t)s->opts.max_batch});
+        const Clock::time_point now = Clock::now();
+        for (int i = 0; i < take; ++i) {
+          const int64_t qid = g.pending.front();
+          g.pending.pop_front();
+          --s->n_pending;
+          Query& q = s->queries[qid];
+          q.row = g.free_rows.back();
+          g.free_rows.pop_back();
+          q.t_launch = now;
+          qs.push_back(qid);
+        }
+        s->ctr.launched += take;
+      }
+      cudaError_t e = cudaSuccess;
+      for (size_t i = 0; i < qs.size() && e == cudaSuccess; ++i) {
+        const int32_t row = s->queries[qs[i]].row;
+        e = cudaMemsetAsync(g.pool + (size_t)row * g.V, 0xFF, sizeof(int32_t) * (size_t)g.V, s->prep);
+      }
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s->prep);
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (e != cudaSuccess) {  // not posted: back to the queue
+        for (auto it = qs.rbegin(); it != qs.rend(); ++it) {
+          Query& q = s->queries[*it];
+          g.free_rows.push_back(q.row);
+          q.row = -1;
+          g.pending.push_front(*it);
+          ++s->n_pending;
+        }
+        s->ctr.launched -= (int64_t)qs.size();
+        s->worker_error = ENT_ERR_CUDA;
+        s->worker_msg = cudaGetErrorString(e);
+        continue;
+      }
+      for (size_t i = 0; i < qs.size(); ++i) {
+        const Query& q = s->queries[qs[i]];
+        sl.box->pos[i] = sl.next_pos + (int32_t)i;
+        sl.box->src[i] = q.src;
+        sl.box->row[i] = q.row;
+      }
+      sl.box->n = (int32_t)qs.size();
+      __atomic_store_n(&sl.box->seq, sl.box->seq + 1, __ATOMIC_RELEASE);
+      sl.next_pos += (int32_t)qs.size();
+      sl.posted = qs;
+      any = true;
+    }
+  }
+  return any;
+}
+
 void scheduler(ent_server* s) {
   cudaSetDevice(s->device);
   while (!s->stop.load()) {
     const bool r = retire(s);
     const bool l = launch(s);
-    if (!r && !l) {
+    const bool j = s->opts.join ? join(s) : false;
+    if (!r && !l && !j) {
       std::unique_lock<std::mutex> lk(s->mu);
       s->cv.wait_for(lk, std::chrono::microseconds(20));
     }
@@ -269,7 +374,7 @@ void ent_server_opts_default(ent_server_opts* o) {
   o->fast_slots = 2;
   o->fast_max_waiting = 2;
   o->single_cluster = 8;
-  o->pad = 0;
+  o->join = 1;
 }
 
 // Depth of one traversal of g from its first non-isolated vertex (0 if the
@@ -306,6 +411,7 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
   if (o.fast_slots < 0 || o.fast_slots > 16) return fail(ENT_ERR_INVALID_ARG, "fast_slots must be 0..16");
   if (o.fast_max_waiting < 1) return fail(ENT_ERR_INVALID_ARG, "fast_max_waiting must be >= 1");
   if (o.single_cluster < 0 || o.single_cluster > 16) return fail(ENT_ERR_INVALID_ARG, "single_cluster must be 0..16");
+  if (o.join < 0 || o.join > 1) return fail(ENT_ERR_INVALID_ARG, "join must be 0 or 1");
   const int dev = graphs[0]->device;
   for (int k = 0; k < n_graphs; ++k)
     if (!graphs[k] || graphs[k]->device != dev) return fail(ENT_ERR_INVALID_ARG, "all graphs must be on one GPU");
@@ -320,6 +426,10 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
   // the lowest: a single-source traversal of a deep graph holds a cluster of
   // SMs for milliseconds, and without priorities the grid-wide kernels of
   // batches queue behind it for SMs.
+  if (cudaStreamCreateWithFlags(&s->prep, cudaStreamNonBlocking) != cudaSuccess) {
+    free_server(s);
+    return fail(ENT_ERR_CUDA, "server stream setup failed");
+  }
   int prio_low = 0, prio_high = 0;
   cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   s->gs.resize(n_graphs);
@@ -390,10 +500,16 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
       if (rc == ENT_OK) {
         cudaError_t e2 = cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, prio_high);
         if (e2 == cudaSuccess) e2 = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
-        if (e2 == cudaSuccess) e2 = cudaMalloc(&sl.row_map_dev, sizeof(int32_t) * 2048);
+        if (e2 == cudaSuccess) e2 = cudaMalloc(&sl.row_map_dev, sizeof(int32_t) * JOIN_MAX);
         if (e2 == cudaSuccess) e2 = cudaGraphCreate(&sl.graph, 0);
+        if (e2 == cudaSuccess) e2 = cudaHostAlloc((void**)&sl.box, sizeof(JoinBox), cudaHostAllocMapped);
+        if (e2 == cudaSuccess) {
+          memset(sl.box, 0, sizeof(JoinBox));
+          e2 = cudaHostGetDevicePointer((void**)&sl.box_dev, sl.box, 0);
+        }
         if (e2 != cudaSuccess) rc = fail(ENT_ERR_CUDA, "slot setup: %s", cudaGetErrorString(e2));
       }
+      if (rc == ENT_OK && o.join) set_join_box(sl.ws, sl.box_dev);
       if (rc == ENT_OK) rc = append_branch(g.g, sl.ws, sl.graph, sl.stream);
       if (rc == ENT_OK && cudaGraphInstantiate(&sl.exec, sl.graph, 0) != cudaSuccess)
         rc = fail(ENT_ERR_CUDA, "slot graph instantiate failed");

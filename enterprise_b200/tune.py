@@ -20,6 +20,9 @@ import numpy as np
 from . import BfsOpts, Graph, _Opts, _check, _i32p, lib
 
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "enterprise_b200", "tune.json")
+# Results of earlier searches that ship with the package (read-only), consulted
+# for keys the user's cache lacks: a fresh machine of a known GPU starts from them.
+SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned", "b200.json")
 MODES = {"single": 0, "batch": 1}
 
 
@@ -41,19 +44,27 @@ def gpu_name(device: int = 0) -> str:
 class TuneCache:
     """JSON file mapping 'gpu|class|mode' -> {'opts': {...}, 'ms': float, 'when': str}."""
 
-    def __init__(self, path: str = DEFAULT_CACHE):
+    def __init__(self, path: str = DEFAULT_CACHE, shipped: Optional[str] = SHIPPED):
         self.path = path
         self.data: dict = {}
+        self.shipped: dict = {}
         if os.path.exists(path):
             with open(path) as f:
                 self.data = json.load(f)
+        if shipped and os.path.exists(shipped):
+            with open(shipped) as f:
+                self.shipped = json.load(f)
 
     @staticmethod
     def key(gpu: str, gclass: str, mode: str) -> str:
         return f"{gpu}|{gclass}|{mode}"
 
+    def source(self, key: str) -> Optional[str]:
+        """Where get() finds `key`: 'user', 'shipped' or None."""
+        return "user" if key in self.data else ("shipped" if key in self.shipped else None)
+
     def get(self, key: str) -> Optional[BfsOpts]:
-        e = self.data.get(key)
+        e = self.data.get(key) or self.shipped.get(key)
         if not e:
             return None
         o = BfsOpts()

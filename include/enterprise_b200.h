@@ -437,7 +437,9 @@ typedef struct ent_server_opts {
   int32_t single_cluster;   /* CTAs per small-frontier cluster of the deep graphs'
                                single-source slots, 0..16 (default 8; 0 = each
                                graph's own narrow_cluster option)                */
-  int32_t pad;              /* reserved, 0                                        */
+  int32_t join;             /* 1 (default): queries waiting while a batch of their
+                               graph runs join it at its next level boundary, in
+                               its free source positions; 0: they wait for a slot */
 } ent_server_opts;
 typedef struct ent_query_result {
   int64_t query_id;
@@ -455,6 +457,7 @@ typedef struct ent_server_counters {
   int32_t max_batch_seen;
   int32_t single_graphs;    /* graphs served one source per launch */
   int64_t fast_launches;    /* queries run on the fast single-source slots of the other graphs */
+  int64_t joined;           /* queries that joined a running batch at a level boundary */
 } ent_server_counters;
 void ent_server_opts_default(ent_server_opts* opts);
 int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_server_opts* opts,

@@ -42,7 +42,7 @@ def test_struct_layout_matches_header(eb):
     assert ctypes.sizeof(eb._Opts) == 4 + 4 + 8 * 3 + 4 * 5 + 4 + 8 + 4 * 12
     assert ctypes.sizeof(eb._Stats) == 8 + 8 + 4 * 4 + 8 + 4 * 2
     assert ctypes.sizeof(eb._ServerOpts) == 4 * 4 + 8 + 4 * 6
-    assert ctypes.sizeof(eb._ServerCounters) == 8 * 9 + 4 * 2 + 8
+    assert ctypes.sizeof(eb._ServerCounters) == 8 * 9 + 4 * 2 + 8 * 2
 
 
 def test_server_option_defaults(eb):

@@ -238,3 +238,67 @@ def test_fast_slots_take_lone_queries(eb, orc):
             else:
                 assert c["fast_launches"] == 0
     g.close()
+
+
+def test_queries_join_a_running_batch(eb, orc):
+    """Continuous batching at level boundaries. On a graph whose batches run
+    about a thousand levels, served by bitwise batches alone (no single-source
+    slots, one batched slot), queries submitted while a batch runs join it in
+    its free source positions at its next level boundary. Every result, joined
+    or not, equals the oracle's depths from its own source."""
+    import time
+    from conftest import tier_graph
+    V, s, d = tier_graph()
+    csr = eb.Csr.from_edges(s, d, V)
+    g = eb.Graph.from_csr(csr)
+    srcs = [int(x) for x in eb.pick_sources(csr.beg_pos, 5, 60)]
+    srcs[:2] = [5999, 5500]  # deep in the tail: the first batch runs ~1000 levels
+    try:
+        with eb.Server([g], max_batch=64, slots_per_graph=1, single_source_levels=0, fast_slots=0) as srv:
+            qs = {srv.submit(0, srcs[0]): srcs[0], srv.submit(0, srcs[1]): srcs[1]}
+            time.sleep(0.003)
+            for x in srcs[2:]:
+                qs[srv.submit(0, x)] = x
+                time.sleep(0.0002)
+            res = _drain(srv, len(qs))
+            c = srv.counters()
+            assert c["joined"] > 0, c
+            for r in res:
+                src = qs[r["query_id"]]
+                assert r["status"] == 0
+                exp, _ = orc.bfs(csr.beg_pos, csr.csr, src)
+                np.testing.assert_array_equal(srv.depth(r["query_id"]), exp, err_msg=f"source {src}")
+                assert (r["traversed_edges"], r["reached_vertices"]) == orc.report(csr.beg_pos, exp)
+                assert r["levels"] == int(exp.max()) + 1
+                srv.release(r["query_id"])
+            c = srv.counters()
+            assert c["completed"] == c["released"] == len(qs) and c["rows_free"] == c["rows_total"]
+            assert c["batches"] < len(qs)
+    finally:
+        g.close()
+
+
+def test_join_off_keeps_waiting_queries_for_the_next_batch(eb, orc):
+    """With joining off, queries that arrive while the batch runs wait for the
+    slot; results are the same."""
+    import time
+    from conftest import tier_graph
+    V, s, d = tier_graph()
+    csr = eb.Csr.from_edges(s, d, V)
+    g = eb.Graph.from_csr(csr)
+    srcs = [5999, 5500] + [int(x) for x in eb.pick_sources(csr.beg_pos, 6, 20)]
+    try:
+        with eb.Server([g], max_batch=64, slots_per_graph=1, single_source_levels=0, fast_slots=0,
+                       join=False) as srv:
+            qs = {srv.submit(0, srcs[0]): srcs[0], srv.submit(0, srcs[1]): srcs[1]}
+            time.sleep(0.003)
+            for x in srcs[2:]:
+                qs[srv.submit(0, x)] = x
+            res = _drain(srv, len(qs))
+            assert srv.counters()["joined"] == 0
+            for r in res:
+                exp, _ = orc.bfs(csr.beg_pos, csr.csr, qs[r["query_id"]])
+                np.testing.assert_array_equal(srv.depth(r["query_id"]), exp)
+                srv.release(r["query_id"])
+    finally:
+        g.close()

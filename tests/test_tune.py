@@ -65,3 +65,20 @@ def test_native_search_keeps_results_exact(eb, orc, mode):
         d, _ = g.bfs_batch(srcs[:5])
         for i in range(5):
             np.testing.assert_array_equal(d[i], orc.bfs(csr.beg_pos, csr.csr, int(srcs[i]))[0])
+
+
+def test_shipped_results_cover_the_headline_class(eb, tmp_path):
+    """The package ships an earlier B200 search for R-MAT scale 24 edge factor
+    16; a fresh cache falls back to it, and the user's own entries win."""
+    from dataclasses import asdict
+    from enterprise_b200 import tune
+    key = tune.TuneCache.key("NVIDIA B200", tune.graph_class(1 << 24, 520772318, "rmat"), "single")
+    cache = tune.TuneCache(str(tmp_path / "none.json"))
+    assert cache.source(key) == "shipped"
+    o = cache.get(key)
+    assert (o.alpha, o.beta, o.small_max, o.large_min, o.chunk_edges) == (48.0, 1024.0, 16, 128, 256)
+    o.alpha = 12.0
+    cache.put(key, o, 1.0)
+    again = tune.TuneCache(str(tmp_path / "none.json"))
+    assert again.source(key) == "user" and again.get(key).alpha == 12.0
+    assert tune.TuneCache(str(tmp_path / "x.json"), shipped=None).source(key) is None
