@@ -389,8 +389,7 @@ def run_ours(args, rank, world, dist):
         line["ingest"] = run_ingest(args)
         line["serving"] = run_serving(args)
         if args.burst_seconds > 0:
-            line["serving_rmat_queued"] = run_serving(args, seconds=args.burst_seconds, rate=args.burst_rate,
-                                                      rmat_only=True)
+            line["serving_rmat_queued"] = run_burst(args)
     elif not args.no_extras:
         g.close()
         del depth, flush
@@ -746,7 +745,7 @@ def run_ingest(args):
     return out
 
 
-def run_serving(args, rank=0, seconds=None, raw=False, rate=None, rmat_only=False):
+def run_serving(args, rank=0, seconds=None, raw=False, rate=None, rmat_only=False, join=1):
     """Poisson stream of BFS queries against 16 device-resident graphs (12
     R-MAT s14-22 ef16, 4 grids 1024^2..2048^2 with 10% of edges dropped):
     continuous batching, admission by HBM depth rows, latency percentiles.
@@ -778,7 +777,7 @@ def run_serving(args, rank=0, seconds=None, raw=False, rate=None, rmat_only=Fals
     checks, bad_status, mismatches, samples = 0, 0, [], []
     graph_of = {}
     with eb.Server(graphs, max_batch=args.serve_batch, slots_per_graph=args.serve_slots,
-                   single_cluster=args.serve_cluster) as srv:
+                   single_cluster=args.serve_cluster, join=join) as srv:
         t0 = time.perf_counter()
         i = 0
         while done < n_q:
@@ -830,6 +829,17 @@ def run_serving(args, rank=0, seconds=None, raw=False, rate=None, rmat_only=Fals
                              "p50_ms": round(float(np.percentile(v, 50)), 3) if v else None,
                              "p99_ms": round(float(np.percentile(v, 99)), 3) if v else None}
                          for k, v in lat_cls.items()}}
+
+
+def run_burst(args):
+    """The second serving point: the 12 R-MAT graphs alone at a rate where
+    queries queue, so that batches form and waiting queries join running
+    batches at level boundaries; then the same stream with joining off."""
+    out = run_serving(args, seconds=args.burst_seconds, rate=args.burst_rate, rmat_only=True)
+    off = run_serving(args, seconds=args.burst_seconds, rate=args.burst_rate, rmat_only=True, join=0)
+    out["join_off"] = {k: off[k] for k in ("completed", "throughput_qps", "gteps", "p50_ms", "p99_ms", "p999_ms",
+                                           "queue_p50_ms", "mean_batch", "batches", "sampled_exact")}
+    return out
 
 
 def oracle_rows(host, srcs, get_row, as_bytes=False):
@@ -999,7 +1009,7 @@ def main():
     try:
         if args.only:
             line = {"batch": run_batched, "serve": run_serving, "deep": run_deep, "ingest": run_ingest,
-                    "burst": lambda a: run_serving(a, seconds=a.burst_seconds, rate=a.burst_rate, rmat_only=True)
+                    "burst": run_burst
                     }[args.only](args)
         elif args.impl == "reference":
             line = run_reference(args, rank, world)

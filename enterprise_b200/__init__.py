@@ -729,11 +729,11 @@ class Server:
     def __init__(self, graphs: Sequence[Graph], max_batch: int = 64, slots_per_graph: int = 2,
                  rows_per_graph: int = 0, max_pending: int = 1 << 20, hbm_budget_bytes: int = 0,
                  single_source_levels: int = 64, single_slots: int = 8, fast_slots: int = 2,
-                 fast_max_waiting: int = 2, single_cluster: int = 8, join: bool = True):
+                 fast_max_waiting: int = 2, single_cluster: int = 8, join: int = 1):
         self.graphs = list(graphs)
         o = _ServerOpts(max_batch, slots_per_graph, rows_per_graph, max_pending, hbm_budget_bytes,
                         single_source_levels, single_slots, fast_slots, fast_max_waiting, single_cluster,
-                        1 if join else 0)
+                        int(join))
         hs = (_P * len(graphs))(*[g.handle for g in graphs])
         h = _P()
         _check(lib().ent_server_create(hs, len(graphs), C.byref(o), C.byref(h)))

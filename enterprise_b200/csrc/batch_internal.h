@@ -6,15 +6,21 @@
 namespace ent {
 // Sources that join a running bitwise batch at its next level boundary. Lives
 // in mapped, page-locked host memory: the host fills the entries, then bumps
-// seq (release); the batch's level finisher, seeing seq != taken, adds the
-// entries to the next level's frontier and stores taken = seq (release). A
-// post the batch never took (it ended first) stays with taken != seq.
+// seq (release); the batch's level finisher, seeing seq != taken at a level no
+// deeper than `limit`, adds the entries to that level's frontier and stores
+// taken = seq (release). A post the batch never took (it ended first, or it
+// was past the limit) stays with taken != seq. The finisher also publishes the
+// level it reached, so the host posts only while a post can still be taken:
+// results come back when the whole batch ends, so a source that joins late
+// would hold back every result of its batch.
 constexpr int JOIN_MAX = 2048;
 struct JoinBox {
   int32_t seq;            // written by the host
   int32_t taken;          // written by the device
   int32_t n;              // entries of the post
-  int32_t pad;
+  int32_t limit;          // deepest level at which the batch takes a post (host)
+  int32_t level;          // level the batch has reached (device)
+  int32_t pad[3];
   int32_t pos[JOIN_MAX];  // bit position (source slot) in the batch
   int32_t src[JOIN_MAX];  // source vertex
   int32_t row[JOIN_MAX];  // depth row (row_map entry) of the source

@@ -686,8 +686,9 @@ __device__ __forceinline__ void st_release_sys(int32_t* p, int v) {
   asm volatile("st.release.sys.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Level finisher (one thread, every CTA of the level done): sources posted to
-// the join mailbox start here, at depth 0 on level L. Each takes its bit
+// Level finisher (one thread, every CTA of the level done): publishes level L
+// to the join mailbox and, while L is no deeper than the mailbox's limit,
+// starts the sources posted there, at depth 0 on level L. Each takes its bit
 // position s: the bit goes into its vertex's visited words and into the slot
 // of level L's frontier, the vertex joins that frontier (once), s becomes an
 // active source, and its depths are written relative to L (join[s]). Vertices
@@ -696,6 +697,8 @@ __device__ __forceinline__ void st_release_sys(int32_t* p, int v) {
 __device__ void join_sources(const BatchArgs& a, volatile BatchCtl* vc, int L, int nxt, int64_t& n_next,
                              int64_t& m_next) {
   JoinBox* box = a.box;
+  *(volatile int32_t*)&box->level = L;
+  if (L > *(volatile int32_t*)&box->limit) return;
   const int seq = ld_acquire_sys(&box->seq);
   if (seq == *(volatile int32_t*)&box->taken) return;
   const int nj = *(volatile int32_t*)&box->n;

@@ -177,6 +177,7 @@ bool retire(ent_server* s) {
         uq.row = -1;
         g.pending.push_front(*it);
         ++s->n_pending;
+        --s->ctr.launched;  // counted again when it launches
       }
       for (size_t i = 0; i < sl.qids.size(); ++i) {
         auto it = s->queries.find(sl.qids[i]);
@@ -245,6 +246,8 @@ bool launch(ent_server* s) {
         sl.box->seq = 0;  // the slot is idle: nothing reads the mailbox
         sl.box->taken = 0;
         sl.box->n = 0;
+        sl.box->limit = s->opts.join;
+        sl.box->level = 0;
         sl.posted.clear();
         sl.next_pos = n;
         e = cudaMemcpyAsync(sl.row_map_dev, rows.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, sl.stream);
@@ -289,8 +292,11 @@ bool join(ent_server* s) {
       if (!sl.busy || !sl.box) continue;
       confirm_joins(sl);
       if (!sl.posted.empty()) continue;  // one post in flight per batch
+      // a post is taken at the next level boundary: only while that is within the limit
+      if (__atomic_load_n(&sl.box->level, __ATOMIC_ACQUIRE) >= s->opts.join) continue;
       const int cap = batch_max_sources(sl.ws);
       std::vector<int64_t> qs;
+      std::vector<int32_t> rows, srcs;  // copied under the lock: submit() may rehash the query map
       {
         std::lock_guard<std::mutex> lk(s->mu);
         if (g.pending.empty() || g.free_rows.empty() || sl.next_pos >= cap) continue;
@@ -306,14 +312,14 @@ bool join(ent_server* s) {
           g.free_rows.pop_back();
           q.t_launch = now;
           qs.push_back(qid);
+          rows.push_back(q.row);
+          srcs.push_back(q.src);
         }
         s->ctr.launched += take;
       }
       cudaError_t e = cudaSuccess;
-      for (size_t i = 0; i < qs.size() && e == cudaSuccess; ++i) {
-        const int32_t row = s->queries[qs[i]].row;
-        e = cudaMemsetAsync(g.pool + (size_t)row * g.V, 0xFF, sizeof(int32_t) * (size_t)g.V, s->prep);
-      }
+      for (size_t i = 0; i < qs.size() && e == cudaSuccess; ++i)
+        e = cudaMemsetAsync(g.pool + (size_t)rows[i] * g.V, 0xFF, sizeof(int32_t) * (size_t)g.V, s->prep);
       if (e == cudaSuccess) e = cudaStreamSynchronize(s->prep);
       std::lock_guard<std::mutex> lk(s->mu);
       if (e != cudaSuccess) {  // not posted: back to the queue
@@ -330,10 +336,9 @@ bool join(ent_server* s) {
         continue;
       }
       for (size_t i = 0; i < qs.size(); ++i) {
-        const Query& q = s->queries[qs[i]];
         sl.box->pos[i] = sl.next_pos + (int32_t)i;
-        sl.box->src[i] = q.src;
-        sl.box->row[i] = q.row;
+        sl.box->src[i] = srcs[i];
+        sl.box->row[i] = rows[i];
       }
       sl.box->n = (int32_t)qs.size();
       __atomic_store_n(&sl.box->seq, sl.box->seq + 1, __ATOMIC_RELEASE);
@@ -411,7 +416,7 @@ int ent_server_create(ent_graph* const* graphs, int32_t n_graphs, const ent_serv
   if (o.fast_slots < 0 || o.fast_slots > 16) return fail(ENT_ERR_INVALID_ARG, "fast_slots must be 0..16");
   if (o.fast_max_waiting < 1) return fail(ENT_ERR_INVALID_ARG, "fast_max_waiting must be >= 1");
   if (o.single_cluster < 0 || o.single_cluster > 16) return fail(ENT_ERR_INVALID_ARG, "single_cluster must be 0..16");
-  if (o.join < 0 || o.join > 1) return fail(ENT_ERR_INVALID_ARG, "join must be 0 or 1");
+  if (o.join < 0) return fail(ENT_ERR_INVALID_ARG, "join must be >= 0");
   const int dev = graphs[0]->device;
   for (int k = 0; k < n_graphs; ++k)
     if (!graphs[k] || graphs[k]->device != dev) return fail(ENT_ERR_INVALID_ARG, "all graphs must be on one GPU");

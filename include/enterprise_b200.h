@@ -437,9 +437,12 @@ typedef struct ent_server_opts {
   int32_t single_cluster;   /* CTAs per small-frontier cluster of the deep graphs'
                                single-source slots, 0..16 (default 8; 0 = each
                                graph's own narrow_cluster option)                */
-  int32_t join;             /* 1 (default): queries waiting while a batch of their
-                               graph runs join it at its next level boundary, in
-                               its free source positions; 0: they wait for a slot */
+  int32_t join;             /* queries waiting while a batch of their graph runs
+                               join it at a level boundary, in its free source
+                               positions, while the batch is at level <= join
+                               (default 1; 0 = never: they wait for a slot). A
+                               batch's results come back when it ends, so joining
+                               late would hold back the results already in it */
 } ent_server_opts;
 typedef struct ent_query_result {
   int64_t query_id;

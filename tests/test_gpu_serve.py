@@ -254,7 +254,9 @@ def test_queries_join_a_running_batch(eb, orc):
     srcs = [int(x) for x in eb.pick_sources(csr.beg_pos, 5, 60)]
     srcs[:2] = [5999, 5500]  # deep in the tail: the first batch runs ~1000 levels
     try:
-        with eb.Server([g], max_batch=64, slots_per_graph=1, single_source_levels=0, fast_slots=0) as srv:
+        # joining allowed at any level here, so that queries submitted milliseconds into the batch join it
+        with eb.Server([g], max_batch=64, slots_per_graph=1, single_source_levels=0, fast_slots=0,
+                       join=1 << 30) as srv:
             qs = {srv.submit(0, srcs[0]): srcs[0], srv.submit(0, srcs[1]): srcs[1]}
             time.sleep(0.003)
             for x in srcs[2:]:
@@ -278,9 +280,11 @@ def test_queries_join_a_running_batch(eb, orc):
         g.close()
 
 
-def test_join_off_keeps_waiting_queries_for_the_next_batch(eb, orc):
+@pytest.mark.parametrize("join", [0, 1])
+def test_join_off_keeps_waiting_queries_for_the_next_batch(eb, orc, join):
     """With joining off, queries that arrive while the batch runs wait for the
-    slot; results are the same."""
+    slot; with the default limit (level 1), they arrive too late to join this
+    batch of a thousand levels and wait as well. Results are the same."""
     import time
     from conftest import tier_graph
     V, s, d = tier_graph()
@@ -289,7 +293,7 @@ def test_join_off_keeps_waiting_queries_for_the_next_batch(eb, orc):
     srcs = [5999, 5500] + [int(x) for x in eb.pick_sources(csr.beg_pos, 6, 20)]
     try:
         with eb.Server([g], max_batch=64, slots_per_graph=1, single_source_levels=0, fast_slots=0,
-                       join=False) as srv:
+                       join=join) as srv:
             qs = {srv.submit(0, srcs[0]): srcs[0], srv.submit(0, srcs[1]): srcs[1]}
             time.sleep(0.003)
             for x in srcs[2:]:
