@@ -28,8 +28,8 @@ struct JoinBox {
 
 // Traversal state for one batched run of up to words_for(n_src)*64 sources.
 int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out);
-// Adds one independent branch (memsets, seed, while{expand, commit, flush,
-// recycle}, final flush) for workspace w to `graph`.
+// Adds one independent branch (memsets, seed, while{expand, commit,
+// if{flush}}, final flush) for workspace w to `graph`.
 int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream_t cap_stream);
 // Uploads sources and output location for the next launch of w's branch.
 // With row_map_dev (device, n_src entries) source s writes depth row row_map[s].

@@ -24,8 +24,8 @@
 // vertex ORs its neighbours' frontier words, stopping once all bits of the
 // active sources it lacks are covered; light, mid and large degree tiers).
 // Depths are never scattered during the traversal: a flush kernel decodes the
-// log into a byte tile per span of vertices and writes the source-major int32
-// depth rows with coalesced 128-byte stores.
+// log into a byte tile per span of vertices, zeroing the slots as it reads
+// them, and writes the source-major depth rows with coalesced vector stores.
 #include <algorithm>
 #include <string.h>
 #include <vector>
@@ -60,9 +60,9 @@ struct BatchCtl {
   int64_t m_f, m_done;
   uint32_t finished;
   int32_t out_bytes;  // depth rows are uint8 (the reference's depth type, 255 = unreached), not int32
-  int32_t clear_done; // sources joined: the completion bits no longer hold (k_b_recycle clears them)
+  int32_t clear_done; // sources joined: the completion bits no longer hold (k_b_flush clears them)
   int32_t joined;     // sources that joined this run
-  int32_t if_runs;    // level-loop iterations that ran the flush and recycle nodes
+  int32_t if_runs;    // level-loop iterations that ran the flush node
 };
 
 struct BatchArgs {
@@ -99,7 +99,7 @@ struct BatchArgs {
   double alpha;      // bottom-up when frontier edges * alpha > unfinished edges
   int32_t heavy_deg; // top-down: from this degree every CTA takes a slice of a vertex
   cudaGraphConditionalHandle cond;
-  cudaGraphConditionalHandle cond_flush;  // the level window is full: run the flush and recycle nodes
+  cudaGraphConditionalHandle cond_flush;  // the level window is full or sources joined: run the flush node
   int32_t use_cond;
   int32_t max_levels;
 };
@@ -692,7 +692,7 @@ __device__ __forceinline__ void st_release_sys(int32_t* p, int v) {
 // position s: the bit goes into its vertex's visited words and into the slot
 // of level L's frontier, the vertex joins that frontier (once), s becomes an
 // active source, and its depths are written relative to L (join[s]). Vertices
-// marked complete lack the new bits, so their marks are dropped (k_b_recycle
+// marked complete lack the new bits, so their marks are dropped (k_b_flush
 // clears them before the next level).
 __device__ void join_sources(const BatchArgs& a, volatile BatchCtl* vc, int L, int nxt, int64_t& n_next,
                              int64_t& m_next) {
@@ -857,30 +857,31 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
   __threadfence();
   if (a.use_cond) {
     cudaGraphSetConditional(a.cond, done ? 0u : 1u);
-    // flush and recycle also run when sources joined (k_b_recycle drops the completion bits)
+    // the flush node also runs when sources joined (it drops the completion bits)
     cudaGraphSetConditional(a.cond_flush, (vc->flush_now || vc->clear_done) ? 1u : 0u);
   }
 }
 
 // ----------------------------------------------------------- flush --------
 // Converts log slots [first, last] (levels base+first .. base+last) into the
-// source-major depth rows. A CTA takes a span of 1024 vertices and walks the W
-// word columns in groups of CG = min(W, 4), VS = 1024 / CG vertices per pass.
+// source-major depth rows and recycles the slots in the same pass. A CTA takes
+// a span of 1024 vertices and walks the W word columns in groups of
+// CG = min(W, 4), VS = 1024 / CG vertices per pass.
 // Decode (thread per vertex): the slots of a vertex are disjoint bit sets, so
 // the vertex's CG words of every slot fold into a found mask and four bit
 // planes of the slot index; each 4-source nibble of those becomes one 32-bit
 // word of four bytes (slot index, 0xFF where not found) by multiply-spreading
-// the nibbles, stored in a vertex-major byte tile [vertex][64*CG sources]
-// whose 32-bit words are XOR-swizzled so that the 32 lanes of a warp hit 32
-// banks in both phases. Write (warp per 4 sources): a lane reads one tile
-// word per vertex, sign-extends its four bytes into the four rows' depths
-// (coalesced 128-byte stores per row) and keeps the rows' statistics. The
-// first window writes every (source, vertex) pair (-1 where not found); later
-// windows only the pairs they found. Recycling the slots (zeroing, carrying
-// the last one into slot 0) is left to k_b_recycle, which streams them
-// contiguously.
+// the nibbles, stored in a vertex-major byte tile [vertex][64*CG sources].
+// Each vertex's slot words are zeroed once decoded (a window flush carries the
+// last slot, the next window's frontier, into slot 0).
+// Write (warp per 4 sources): where every (source, vertex) pair is written
+// (the first window: -1 where not found) and the rows allow it, a lane takes
+// 4 consecutive vertices and stores each row's 4 depths as one vector;
+// otherwise (later windows write only the pairs they found) a lane takes a
+// vertex. Reached vertices, the sum of their degrees and the deepest level
+// are kept per row.
 constexpr int TILE_BYTES = 64 * 1024;  // VS vertices x 64*CG source bytes
-constexpr int FLUSH_TILE_BYTES = TILE_BYTES + 1024 * 4;
+constexpr int FLUSH_TILE_BYTES = TILE_BYTES + 1024 * 4;  // + the span's degrees
 
 template <int CG>
 __device__ __forceinline__ void load_cols(const unsigned long long* p, unsigned long long (&w)[CG]) {
@@ -896,12 +897,26 @@ __device__ __forceinline__ void load_cols(const unsigned long long* p, unsigned 
   }
 }
 
-// Tile word c (4 sources) of vertex vi: rows of 16*CG words, the word index
-// XOR-swizzled by the vertex so that 32 consecutive vertices use 32 banks.
+template <int CG>
+__device__ __forceinline__ void store_cols(unsigned long long* p, unsigned long long x0, unsigned long long x1,
+                                           unsigned long long x2, unsigned long long x3) {
+  if constexpr (CG == 1) {
+    *p = x0;
+  } else {
+    *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(x0, x1);
+    if constexpr (CG == 4) *reinterpret_cast<ulonglong2*>(p + 2) = make_ulonglong2(x2, x3);
+  }
+}
+
+// Tile word c (4 sources) of vertex vi. Rows of 16*CG words, the word index
+// XOR-swizzled by the vertex so that both access patterns spread over the
+// banks: 32 consecutive vertices (decode, and the write of later windows) hit
+// 32 banks, and vertices 4l+t of lanes l = 0..31 (the vector write; the base
+// vertex a multiple of 128) hit 32 banks, or 16 when CG == 1.
 template <int CG>
 __device__ __forceinline__ int tile_word(int vi, int c) {
-  if constexpr (CG == 1) return vi * 16 + (c ^ ((vi >> 1) & 15));
-  else return vi * 16 * CG + (c ^ (vi & 31));
+  if constexpr (CG == 1) return vi * 16 + (c ^ (((vi >> 1) ^ (vi >> 5)) & 15));
+  else return vi * 16 * CG + (c ^ ((vi ^ (vi >> 5)) & 31));
 }
 
 // Bit i (i < 4) of the nibble n moves to bit 8*i + sh: x * 0x00204081 puts
@@ -910,24 +925,55 @@ __device__ __forceinline__ uint32_t spread4(uint32_t n, int sh) {
   return ((n * 0x00204081u) & 0x01010101u) << sh;
 }
 
+// Byte j of w as a signed value (a slot index 0..15, or 0xFF -> -1). In its
+// default mode prmt copies the selected byte's sign bit into every result
+// byte whose selector nibble has its top bit set.
+__device__ __forceinline__ int sext_byte(uint32_t w, uint32_t j) {
+  const uint32_t sel = j | ((8u + j) * 0x1110u);
+  uint32_t r;
+  asm("prmt.b32 %0, %1, 0, %2;" : "=r"(r) : "r"(w), "r"(sel));
+  return (int)r;
+}
+
+// The low bytes of a, b, c, d as one word, a in byte 0.
+__device__ __forceinline__ uint32_t pack_low_bytes(int a, int b, int c, int d) {
+  return __byte_perm(__byte_perm((uint32_t)a, (uint32_t)b, 0x0040u), __byte_perm((uint32_t)c, (uint32_t)d, 0x0040u),
+                     0x5410u);
+}
+
+struct FlushState {
+  int first, last, base, windows, nsrc;
+  bool final_flush;
+  bool vec;                 // whole-window rows take 16-byte (int32) or 4-byte (u8) vector stores
+  int32_t* depth;
+  const int32_t* row_map;
+  uint32_t* tile;
+  const int* s_deg;         // [1024] degrees of the span
+  unsigned* s_cnt;          // [W*64] reached vertices per source
+  unsigned long long* s_edg;  // [W*64] their degrees
+  int* s_maxd;              // [W*64] deepest level
+};
+
 template <int CG, bool BYTES>
-__device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, int last, int base, int windows,
-                           int nsrc, int32_t* depth, const int32_t* row_map, uint32_t* tile,
-                           const int* s_deg, unsigned* s_cnt, int* s_maxd, unsigned long long* s_edg) {
+__device__ void flush_span(const BatchArgs& a, const FlushState& fs, int64_t v0, int nv) {
   constexpr int VS = 1024 / CG;  // vertices per pass
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int first = fs.first, last = fs.last;
   const bool four_planes = last >= 8;
   for (int sub = 0; sub < nv; sub += VS) {
     const int nsub = min(VS, nv - sub);
     for (int cg = 0; cg < a.W; cg += CG) {
-      if (cg * 64 >= nsrc) break;
+      if (cg * 64 >= fs.nsrc) break;  // words of no source: never set, so already zero
       __syncthreads();  // the previous tile has been written out
       for (int vi = threadIdx.x; vi < VS; vi += BB) {
+        const bool in = vi < nsub;
+        const size_t at = (size_t)(v0 + sub + vi) * a.W + cg;
         unsigned long long f[CG], p0[CG], p1[CG], p2[CG], p3[CG];
 #pragma unroll
         for (int cc = 0; cc < CG; ++cc) f[cc] = p0[cc] = p1[cc] = p2[cc] = p3[cc] = 0;
-        if (vi < nsub) {
-          const size_t at = (size_t)(v0 + sub + vi) * a.W + cg;
+        // loads and folds only: no store or warp-collective may sit between
+        // the slot loads, which the compiler then keeps in flight together
+        if (in) {
           for (int k0 = first; k0 <= last; k0 += 2) {
             unsigned long long w[2][CG];
 #pragma unroll
@@ -965,66 +1011,111 @@ __device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, in
               uint32_t o = ~(spread4((fh >> sh) & 15u, 0) * 0xFFu);  // 0xFF where not found
               o |= spread4((h0 >> sh) & 15u, 0) | spread4((h1 >> sh) & 15u, 1) | spread4((h2 >> sh) & 15u, 2);
               if (four_planes) o |= spread4((h3 >> sh) & 15u, 3);
-              tile[tile_word<CG>(vi, cc * 16 + hw * 8 + n)] = o;
+              fs.tile[tile_word<CG>(vi, cc * 16 + hw * 8 + n)] = o;
             }
           }
+        }
+        if (in) {
+          // recycle: a window flush carries slot K-1 (the next window's
+          // frontier) into slot 0 and zeroes slots 1..K-1; the final flush
+          // zeroes slots 0..last (slot 0 too after a window flush)
+          int z0 = 0;
+          if (!fs.final_flush) {
+            unsigned long long x[CG];
+            load_cols<CG>(slot_ptr(a, last) + at, x);
+            store_cols<CG>(slot_ptr(a, 0) + at, x[0], x[CG > 1 ? 1 : 0], x[CG > 2 ? 2 : 0], x[CG > 2 ? 3 : 0]);
+            z0 = 1;
+          }
+          for (int k = z0; k <= last; ++k) store_cols<CG>(slot_ptr(a, k) + at, 0ull, 0ull, 0ull, 0ull);
         }
       }
       __syncthreads();
       for (int r0 = warp * 4; r0 < 64 * CG; r0 += BB / 32 * 4) {
         const int s0 = cg * 64 + r0;
-        if (s0 >= nsrc) break;
+        if (s0 >= fs.nsrc) break;
+        const int c4 = r0 >> 2;
         size_t ofs[4];  // element offset of each row's segment (int32 or byte rows)
         bool rv[4];
-        int rbase[4];   // depth of log slot 0 for the row: the window's base level less the source's start
+        int rb[4];      // depth of log slot 0 for the row: the window's base level less the source's start
+        bool wide = false;  // a byte row whose depths could pass 254 here: checked one by one
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          rv[j] = s0 + j < nsrc;
-          ofs[j] = rv[j] ? (size_t)(row_map ? row_map[s0 + j] : s0 + j) * a.V + v0 + sub : 0;
-          rbase[j] = base - (rv[j] ? a.join[s0 + j] : 0);
+          rv[j] = s0 + j < fs.nsrc;
+          ofs[j] = rv[j] ? (size_t)(fs.row_map ? fs.row_map[s0 + j] : s0 + j) * a.V + v0 + sub : 0;
+          rb[j] = fs.base - (rv[j] ? a.join[s0 + j] : 0);
+          if (BYTES && rv[j] && rb[j] > 239) wide = true;
         }
-        bool deep = false;  // a depth above 254 met in byte rows
         unsigned cnt[4] = {0, 0, 0, 0};
         unsigned long long edg[4] = {0, 0, 0, 0};
         int mx[4] = {-1, -1, -1, -1};
-        for (int vi = lane; vi < nsub; vi += 32) {
-          const uint32_t wv = tile[tile_word<CG>(vi, r0 >> 2)];
-          const int dg = s_deg[sub + vi];
+        if (fs.vec && !wide) {
+          for (int vi = lane * 4; vi < nsub; vi += 128) {
+            uint32_t wv[4];
 #pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            int d = (int)(signed char)(uint8_t)(wv >> (8 * j));
-            if (d >= 0) d += rbase[j];
-            if (rv[j]) {
-              if (windows == 0 || d >= 0) {
-                if constexpr (BYTES) {
-                  reinterpret_cast<uint8_t*>(depth)[ofs[j] + vi] = d < 0 ? (uint8_t)255 : (uint8_t)d;
-                  deep |= d > 254;
-                } else {
-                  depth[ofs[j] + vi] = d;
-                }
+            for (int t = 0; t < 4; ++t) wv[t] = fs.tile[tile_word<CG>(vi + t, c4)];
+            const int4 dg = *reinterpret_cast<const int4*>(fs.s_deg + sub + vi);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              if (!rv[j]) continue;
+              int v[4], m[4];
+#pragma unroll
+              for (int t = 0; t < 4; ++t) {
+                const int d = sext_byte(wv[t], j);
+                m[t] = d >> 31;  // -1 where not found
+                v[t] = d + (rb[j] & ~m[t]);
+                cnt[j] += 1 + m[t];
+                mx[j] = max(mx[j], v[t]);
               }
-              if (d >= 0) {
-                ++cnt[j];
-                edg[j] += (unsigned long long)dg;
-                mx[j] = max(mx[j], d);
-              }
+              // two degrees below 2^31 each cannot overflow 32 bits
+              const uint32_t e01 = (uint32_t)(dg.x & ~m[0]) + (uint32_t)(dg.y & ~m[1]);
+              const uint32_t e23 = (uint32_t)(dg.z & ~m[2]) + (uint32_t)(dg.w & ~m[3]);
+              edg[j] += (unsigned long long)e01 + e23;
+              if constexpr (BYTES)
+                *reinterpret_cast<uint32_t*>(reinterpret_cast<uint8_t*>(fs.depth) + ofs[j] + vi) =
+                    pack_low_bytes(v[0], v[1], v[2], v[3]);
+              else
+                *reinterpret_cast<int4*>(fs.depth + ofs[j] + vi) = make_int4(v[0], v[1], v[2], v[3]);
             }
           }
+        } else {
+          bool deep = false;  // a depth above 254 met in byte rows
+          for (int vi = lane; vi < nsub; vi += 32) {
+            const uint32_t wv = fs.tile[tile_word<CG>(vi, c4)];
+            const int dg = fs.s_deg[sub + vi];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              if (!rv[j]) continue;
+              const int d = sext_byte(wv, j);
+              const int m = d >> 31;
+              const int v = d + (rb[j] & ~m);
+              if (fs.windows == 0 || d >= 0) {
+                if constexpr (BYTES) {
+                  reinterpret_cast<uint8_t*>(fs.depth)[ofs[j] + vi] = (uint8_t)v;  // -1 -> 255
+                  deep |= v > 254;
+                } else {
+                  fs.depth[ofs[j] + vi] = v;
+                }
+              }
+              cnt[j] += 1 + m;
+              edg[j] += (uint32_t)(dg & ~m);
+              mx[j] = max(mx[j], v);
+            }
+          }
+          if constexpr (BYTES)
+            if (__any_sync(FULL, deep) && lane == 0) atomicOr(&a.ctl->err, 16);
         }
-        if constexpr (BYTES)
-          if (__any_sync(FULL, deep) && lane == 0) atomicOr(&a.ctl->err, 16);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            cnt[j] += __shfl_xor_sync(FULL, cnt[j], o);
-            edg[j] += __shfl_xor_sync(FULL, edg[j], o);
-            mx[j] = max(mx[j], __shfl_xor_sync(FULL, mx[j], o));
-          }
-          if (lane == 0 && rv[j] && cnt[j]) {
-            s_cnt[s0 + j] += cnt[j];
-            s_edg[s0 + j] += edg[j];
-            s_maxd[s0 + j] = max(s_maxd[s0 + j], mx[j]);
+          // a lane's degree sum is below 2^36 (at most 32 vertices), so both
+          // 16-bit-split halves sum over 32 lanes without overflow
+          const unsigned c = __reduce_add_sync(FULL, cnt[j]);
+          const unsigned elo = __reduce_add_sync(FULL, (unsigned)(edg[j] & 0xFFFFu));
+          const unsigned ehi = __reduce_add_sync(FULL, (unsigned)(edg[j] >> 16));
+          const int dmax = __reduce_max_sync(FULL, mx[j]);
+          if (lane == 0 && rv[j] && c) {  // a source's rows are always this warp's
+            fs.s_cnt[s0 + j] += c;
+            fs.s_edg[s0 + j] += ((unsigned long long)ehi << 16) + elo;
+            fs.s_maxd[s0 + j] = max(fs.s_maxd[s0 + j], dmax);
           }
         }
       }
@@ -1033,82 +1124,68 @@ __device__ void flush_span(const BatchArgs& a, int64_t v0, int nv, int first, in
   __syncthreads();
 }
 
+// Runs after a level when the log window is full (flush_now) or sources
+// joined (clear_done), and once at the end (final_flush). Joined sources void
+// the completion bits, which are cleared. A flush writes the window's depth
+// rows and per-source statistics and recycles the slots (flush_span); a window
+// flush then moves the window by K-1 levels.
 __global__ void __launch_bounds__(BB, 3) k_b_flush(BatchArgs a, int final_flush) {
   extern __shared__ __align__(16) unsigned char s_flush[];
-  BatchCtl* c = a.ctl;
-  if (!final_flush && !c->flush_now) return;
-  const int base = c->base, windows = c->windows;
-  // final: levels base .. level-1 are in slots 0 .. level-1-base
-  const int last = final_flush ? (c->level - 1 - base) : (a.K - 1);
-  const int first = windows == 0 ? 0 : 1;
-  const int nsrc = c->n_src;
-  const int NSRC = a.W * 64;
-  uint32_t* tile = reinterpret_cast<uint32_t*>(s_flush);
-  int* s_deg = reinterpret_cast<int*>(s_flush + TILE_BYTES);  // [1024]
-  unsigned* s_cnt = reinterpret_cast<unsigned*>(s_flush + FLUSH_TILE_BYTES);
-  int* s_maxd = reinterpret_cast<int*>(s_cnt + NSRC);
-  unsigned long long* s_edg = reinterpret_cast<unsigned long long*>(s_maxd + NSRC);
-  for (int i = threadIdx.x; i < NSRC; i += BB) { s_cnt[i] = 0; s_maxd[i] = -1; s_edg[i] = 0; }
-  int32_t* depth = c->depth;
-  const bool bytes = c->out_bytes != 0;
-  const int64_t units = (a.V + 1023) / 1024;
-  for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
-    const int64_t v0 = u * 1024;
-    const int nv = (int)min((int64_t)1024, a.V - v0);
-    __syncthreads();
-    for (int i = threadIdx.x; i < 1024; i += BB) s_deg[i] = i < nv ? a.deg[v0 + i] : 0;
-    __syncthreads();
-    const int32_t* row_map = c->row_map;
-#define ENT_FLUSH(CG, B) flush_span<CG, B>(a, v0, nv, first, last, base, windows, nsrc, depth, row_map, tile, s_deg, s_cnt, s_maxd, s_edg)
-    if (bytes) {
-      if (a.W == 1) ENT_FLUSH(1, true);
-      else if (a.W == 2) ENT_FLUSH(2, true);
-      else ENT_FLUSH(4, true);
-    } else {
-      if (a.W == 1) ENT_FLUSH(1, false);
-      else if (a.W == 2) ENT_FLUSH(2, false);
-      else ENT_FLUSH(4, false);
-    }
-#undef ENT_FLUSH
-  }
-  __syncthreads();
-  for (int s = threadIdx.x; s < nsrc; s += BB) {
-    if (s_cnt[s]) {
-      atomicAdd(&a.st_verts[s], (unsigned long long)s_cnt[s]);
-      atomicAdd(&a.st_edges[s], s_edg[s]);
-      atomicMax(&a.st_maxd[s], s_maxd[s]);
-    }
-  }
-}
-
-// Recycles the log after a flush with contiguous streams: a window flush
-// copies slot K-1 (the next window's frontier) into slot 0 and zeroes slots
-// 1..K-1, then moves the window; the final flush zeroes slots 0..last. After
-// sources joined at a level boundary it also clears the completion bits.
-__global__ void __launch_bounds__(BB) k_b_recycle(BatchArgs a, int final_flush) {
   BatchCtl* c = a.ctl;
   const bool clear = !final_flush && c->clear_done;  // sources joined at this level boundary
   const bool flush = final_flush || c->flush_now;
   if (!flush && !clear) return;
-  const int64_t tid = blockIdx.x * (int64_t)BB + threadIdx.x, nth = (int64_t)gridDim.x * BB;
-  if (clear)
+  if (clear) {
+    const int64_t tid = blockIdx.x * (int64_t)BB + threadIdx.x, nth = (int64_t)gridDim.x * BB;
     for (int64_t i = tid; i <= (a.V + 31) >> 5; i += nth) a.donebits[i] = 0u;
-  const int last = !flush ? -1 : (final_flush ? (c->level - 1 - c->base) : (a.K - 1));
-  const int64_t words = a.V * a.W;  // per slot
-  // A slot starts at log + k*V*W words: 16-byte aligned for every k only when
-  // V*W is even (the log base is 256-byte aligned). Otherwise use 8-byte accesses.
-  const bool vec = (words & 1) == 0;
-  const ulonglong2 z = make_ulonglong2(0ull, 0ull);
-  for (int k = 0; k <= last; ++k) {
-    const bool copy = !final_flush && k == 0;
-    if (vec) {
-      ulonglong2* d = reinterpret_cast<ulonglong2*>(slot_ptr(a, k));
-      const ulonglong2* sp = reinterpret_cast<const ulonglong2*>(slot_ptr(a, last));
-      for (int64_t i = tid; i < words / 2; i += nth) d[i] = copy ? sp[i] : z;
-    } else {
-      unsigned long long* d = slot_ptr(a, k);
-      const unsigned long long* sp = slot_ptr(a, last);
-      for (int64_t i = tid; i < words; i += nth) d[i] = copy ? sp[i] : 0ull;
+  }
+  if (flush) {
+    FlushState fs;
+    fs.base = c->base;
+    fs.windows = c->windows;
+    // final: levels base .. level-1 are in slots 0 .. level-1-base
+    fs.last = final_flush ? (c->level - 1 - fs.base) : (a.K - 1);
+    fs.first = fs.windows == 0 ? 0 : 1;
+    fs.nsrc = c->n_src;
+    fs.final_flush = final_flush != 0;
+    fs.depth = c->depth;
+    fs.row_map = c->row_map;
+    const bool bytes = c->out_bytes != 0;
+    // vector stores: every pair is written and each row segment (row * V + a
+    // multiple of 4) starts 16-byte (int32) or 4-byte (u8) aligned
+    fs.vec = fs.windows == 0 && (a.V & 3) == 0 && ((uintptr_t)fs.depth & (bytes ? 3 : 15)) == 0;
+    const int NSRC = a.W * 64;
+    fs.tile = reinterpret_cast<uint32_t*>(s_flush);
+    fs.s_deg = reinterpret_cast<const int*>(s_flush + TILE_BYTES);
+    fs.s_cnt = reinterpret_cast<unsigned*>(s_flush + FLUSH_TILE_BYTES);
+    fs.s_edg = reinterpret_cast<unsigned long long*>(fs.s_cnt + NSRC);  // NSRC is a multiple of 64: 8-byte aligned
+    fs.s_maxd = reinterpret_cast<int*>(fs.s_edg + NSRC);
+    int* s_deg = reinterpret_cast<int*>(s_flush + TILE_BYTES);
+    for (int i = threadIdx.x; i < NSRC; i += BB) { fs.s_cnt[i] = 0; fs.s_edg[i] = 0; fs.s_maxd[i] = -1; }
+    const int64_t units = (a.V + 1023) / 1024;
+    for (int64_t u = blockIdx.x; u < units; u += gridDim.x) {
+      const int64_t v0 = u * 1024;
+      const int nv = (int)min((int64_t)1024, a.V - v0);
+      __syncthreads();
+      for (int i = threadIdx.x; i < 1024; i += BB) s_deg[i] = i < nv ? a.deg[v0 + i] : 0;
+      __syncthreads();
+      if (bytes) {
+        if (a.W == 1) flush_span<1, true>(a, fs, v0, nv);
+        else if (a.W == 2) flush_span<2, true>(a, fs, v0, nv);
+        else flush_span<4, true>(a, fs, v0, nv);
+      } else {
+        if (a.W == 1) flush_span<1, false>(a, fs, v0, nv);
+        else if (a.W == 2) flush_span<2, false>(a, fs, v0, nv);
+        else flush_span<4, false>(a, fs, v0, nv);
+      }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < fs.nsrc; s += BB) {
+      if (fs.s_cnt[s]) {
+        atomicAdd(&a.st_verts[s], (unsigned long long)fs.s_cnt[s]);
+        atomicAdd(&a.st_edges[s], fs.s_edg[s]);
+        atomicMax(&a.st_maxd[s], fs.s_maxd[s]);
+      }
     }
   }
   if (final_flush) return;
@@ -1158,7 +1235,7 @@ struct BatchWorkspace {
   BatchCtl* ctl = nullptr;
   BatchCtl* ctl_h = nullptr;
   BatchArgs args;
-  int grid = 0, grid_flush = 0, grid_recycle = 0;
+  int grid = 0, grid_flush = 0;
   size_t smem = 0, smem_flush = 0;
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
@@ -1234,7 +1311,7 @@ int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream
   ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &prev, 1, &cp));
   prev = cond_node;
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  // Loop body: expand -> commit -> if (window full or sources joined) { flush -> recycle }.
+  // Loop body: expand -> commit -> if (window full or sources joined) { flush }.
   BatchArgs la = w->args;
   la.cond = handle;
   la.use_cond = 1;
@@ -1249,7 +1326,7 @@ int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream
     kp.gridDim = dim3(w->grid);
     kp.sharedMemBytes = (unsigned)w->smem;
     kp.kernelParams = kl;
-    cudaGraphNode_t n_expand, n_commit, n_if, n_flush, n_recycle;
+    cudaGraphNode_t n_expand, n_commit, n_if, n_flush;
     ENT_CUDA(cudaGraphAddKernelNode(&n_expand, body, nullptr, 0, &kp));
     kp.func = (void*)k_b_commit;
     kp.sharedMemBytes = 0;
@@ -1266,10 +1343,6 @@ int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream
     kp.sharedMemBytes = (unsigned)w->smem_flush;
     kp.kernelParams = kf;
     ENT_CUDA(cudaGraphAddKernelNode(&n_flush, fbody, nullptr, 0, &kp));
-    kp.func = (void*)k_b_recycle;
-    kp.gridDim = dim3(w->grid_recycle);
-    kp.sharedMemBytes = 0;
-    ENT_CUDA(cudaGraphAddKernelNode(&n_recycle, fbody, &n_flush, 1, &kp));
   }
   (void)cap_stream;
   {
@@ -1284,10 +1357,6 @@ int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream
     cudaGraphNode_t n;
     ENT_CUDA(cudaGraphAddKernelNode(&n, graph, &prev, 1, &kp));
     prev = n;
-    kp.func = (void*)k_b_recycle;
-    kp.gridDim = dim3(w->grid_recycle);
-    kp.sharedMemBytes = 0;
-    ENT_CUDA(cudaGraphAddKernelNode(&n, graph, &prev, 1, &kp));
   }
   return ENT_OK;
 }
@@ -1387,8 +1456,8 @@ int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
   const int64_t want = std::max<int64_t>(1, (V + BB * 8 - 1) / (BB * 8));
   w->grid = (int)std::min<int64_t>((int64_t)g->num_sms * occ, want);
   w->grid_flush = (int)std::min<int64_t>((int64_t)g->num_sms * 3, std::max<int64_t>(1, (V + 1023) / 1024));
-  w->grid_recycle = (int)std::min<int64_t>((int64_t)g->num_sms * 4, std::max<int64_t>(1, (V * W / 2 + BB - 1) / BB));
-  w->smem_flush = FLUSH_TILE_BYTES + (size_t)W * 64 * (4 + 4 + 8) + 16;
+  // tile and degrees; per source: reached vertices, their degree sum, deepest level
+  w->smem_flush = FLUSH_TILE_BYTES + (size_t)W * 64 * (4 + 8 + 4) + 16;
   {
     e = cudaFuncSetAttribute(k_b_flush, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->smem_flush);
     if (e != cudaSuccess) { destroy_batch_workspace(w); return fail(ENT_ERR_CUDA, "flush smem attribute failed"); }
@@ -1417,9 +1486,9 @@ static int ensure_batch(ent_graph* g, int n_src) {
   return ENT_OK;
 }
 
-// Kernels one finished graph-driven run launched: seed, final flush and
-// recycle, expand and commit per level, flush and recycle where they ran.
-static int64_t run_launches(const BatchCtl& h) { return 3 + 2 * (int64_t)h.level + 2 * (int64_t)h.if_runs; }
+// Kernels one finished graph-driven run launched: seed, final flush, expand
+// and commit per level, and the flush where it ran.
+static int64_t run_launches(const BatchCtl& h) { return 2 + 2 * (int64_t)h.level + (int64_t)h.if_runs; }
 
 // Uploads sources, mask and the output pointer (the kernels read them from
 // device memory, so one instantiated graph serves every batch).
@@ -1630,11 +1699,13 @@ int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t
   cudaEvent_t e[4];
   for (int i = 0; i < 4; ++i) ENT_CUDA(cudaEventCreate(&e[i]));
   int n = 0;
+  int64_t iters = 0;  // level-loop iterations: expand, commit and flush launches each
   for (;;) {
     ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
     ENT_CUDA(cudaStreamSynchronize(s));
     const BatchCtl h = *w->ctl_h;
     if (h.done || n >= max_levels) break;
+    ++iters;
     ent_level_trace& t = out[n];
     t.level = h.level;
     t.direction = h.dir;
@@ -1648,7 +1719,6 @@ int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t
     ENT_CUDA(cudaEventRecord(e[1], s));
     k_b_commit<<<w->grid, BB, 0, s>>>(a);
     k_b_flush<<<w->grid_flush, BB, w->smem_flush, s>>>(a, 0);
-    k_b_recycle<<<w->grid_recycle, BB, 0, s>>>(a, 0);
     ENT_CUDA(cudaEventRecord(e[2], s));
     ENT_CUDA(cudaGetLastError());
     ENT_CUDA(cudaEventSynchronize(e[2]));
@@ -1661,7 +1731,6 @@ int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t
   }
   ENT_CUDA(cudaEventRecord(e[0], s));
   k_b_flush<<<w->grid_flush, BB, w->smem_flush, s>>>(a, 1);
-  k_b_recycle<<<w->grid_recycle, BB, 0, s>>>(a, 1);
   ENT_CUDA(cudaEventRecord(e[1], s));
   ENT_CUDA(cudaStreamSynchronize(s));
   float tf = 0;
@@ -1674,7 +1743,7 @@ int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t
     ++n;
   }
   for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]);
-  g_kernel_launches += 3 + 4 * (int64_t)n;
+  g_kernel_launches += 2 + 3 * (int64_t)iters;
   *n_levels = n;
   if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "batched traversal error flags 0x%x", w->ctl_h->err);
   return ENT_OK;
