@@ -869,9 +869,9 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
 // CG = min(W, 4), VS = 1024 / CG vertices per pass.
 // Decode (thread per vertex): the slots of a vertex are disjoint bit sets, so
 // the vertex's CG words of every slot fold into a found mask and four bit
-// planes of the slot index; each 4-source nibble of those becomes one 32-bit
-// word of four bytes (slot index, 0xFF where not found) by multiply-spreading
-// the nibbles, stored in a vertex-major byte tile [vertex][64*CG sources].
+// planes of the slot index; a bit-block transpose turns those into one byte
+// per source (slot index, 0xFF where not found), stored in a vertex-major
+// byte tile [vertex][64*CG sources].
 // Each vertex's slot words are zeroed once decoded (a window flush carries the
 // last slot, the next window's frontier, into slot 0).
 // Write (warp per 4 sources): where every (source, vertex) pair is written
@@ -919,10 +919,51 @@ __device__ __forceinline__ int tile_word(int vi, int c) {
   else return vi * 16 * CG + (c ^ ((vi ^ (vi >> 5)) & 31));
 }
 
-// Bit i (i < 4) of the nibble n moves to bit 8*i + sh: x * 0x00204081 puts
-// copies of n at bits 0, 7, 14, 21, which do not overlap, so no carries.
-__device__ __forceinline__ uint32_t spread4(uint32_t n, int sh) {
-  return ((n * 0x00204081u) & 0x01010101u) << sh;
+// One step of an 8x8 bit-block transpose (per byte column of the rows):
+// swaps the s-bit blocks that mask selects in b with the blocks s bits above
+// them in a.
+__device__ __forceinline__ void swap_blocks(uint32_t& a, uint32_t& b, int s, uint32_t mask) {
+  const uint32_t t = ((a >> s) ^ b) & mask;
+  b ^= t;
+  a ^= t << s;
+}
+
+// 4x4 byte transpose: t[g] = byte g of a, b, c, d (a in byte 0).
+__device__ __forceinline__ void byte_transpose4(uint32_t a, uint32_t b, uint32_t c, uint32_t d, uint32_t& t0,
+                                                uint32_t& t1, uint32_t& t2, uint32_t& t3) {
+  const uint32_t ab_lo = __byte_perm(a, b, 0x5140u), ab_hi = __byte_perm(a, b, 0x7362u);
+  const uint32_t cd_lo = __byte_perm(c, d, 0x5140u), cd_hi = __byte_perm(c, d, 0x7362u);
+  t0 = __byte_perm(ab_lo, cd_lo, 0x5410u);
+  t1 = __byte_perm(ab_lo, cd_lo, 0x7632u);
+  t2 = __byte_perm(ab_hi, cd_hi, 0x5410u);
+  t3 = __byte_perm(ab_hi, cd_hi, 0x7632u);
+}
+
+// 32 sources' tile words from their found mask f and slot-index bit planes
+// h0..h3: byte r of out[n] is the slot index of source 4n+r, 0xFF where not
+// found. The rows (h0..h3 each ORed with not-found, then not-found four times)
+// are transposed as 8x8 bit blocks per byte column, which turns byte g of row
+// c into the 8 bits of source 8g+c; two 4x4 byte transposes then gather each
+// word's four consecutive sources.
+__device__ __forceinline__ void planes_to_tile_words(uint32_t f, uint32_t h0, uint32_t h1, uint32_t h2, uint32_t h3,
+                                                     uint32_t (&out)[8]) {
+  const uint32_t nf = ~f;
+  uint32_t r0 = h0 | nf, r1 = h1 | nf, r2 = h2 | nf, r3 = h3 | nf, r4 = nf, r5 = nf, r6 = nf, r7 = nf;
+  swap_blocks(r0, r1, 1, 0x55555555u);
+  swap_blocks(r2, r3, 1, 0x55555555u);
+  swap_blocks(r4, r5, 1, 0x55555555u);
+  swap_blocks(r6, r7, 1, 0x55555555u);
+  swap_blocks(r0, r2, 2, 0x33333333u);
+  swap_blocks(r1, r3, 2, 0x33333333u);
+  swap_blocks(r4, r6, 2, 0x33333333u);
+  swap_blocks(r5, r7, 2, 0x33333333u);
+  swap_blocks(r0, r4, 4, 0x0F0F0F0Fu);
+  swap_blocks(r1, r5, 4, 0x0F0F0F0Fu);
+  swap_blocks(r2, r6, 4, 0x0F0F0F0Fu);
+  swap_blocks(r3, r7, 4, 0x0F0F0F0Fu);
+  // sources 4n..4n+3 sit in rows 4(n&1)..4(n&1)+3, byte n>>1
+  byte_transpose4(r0, r1, r2, r3, out[0], out[2], out[4], out[6]);
+  byte_transpose4(r4, r5, r6, r7, out[1], out[3], out[5], out[7]);
 }
 
 // Byte j of w as a signed value (a slot index 0..15, or 0xFF -> -1). In its
@@ -959,7 +1000,6 @@ __device__ void flush_span(const BatchArgs& a, const FlushState& fs, int64_t v0,
   constexpr int VS = 1024 / CG;  // vertices per pass
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int first = fs.first, last = fs.last;
-  const bool four_planes = last >= 8;
   for (int sub = 0; sub < nv; sub += VS) {
     const int nsub = min(VS, nv - sub);
     for (int cg = 0; cg < a.W; cg += CG) {
@@ -974,26 +1014,30 @@ __device__ void flush_span(const BatchArgs& a, const FlushState& fs, int64_t v0,
         // loads and folds only: no store or warp-collective may sit between
         // the slot loads, which the compiler then keeps in flight together
         if (in) {
-          for (int k0 = first; k0 <= last; k0 += 2) {
-            unsigned long long w[2][CG];
+          // slots in groups of four from a multiple of 4: bits 0 and 1 of a
+          // slot's index follow from its place in the group, bits 2 and 3 are
+          // the group's
+          for (int k0 = 0; k0 <= last; k0 += 4) {
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-              if (k0 + q <= last) load_cols<CG>(slot_ptr(a, k0 + q) + at, w[q]);
+            for (int h = 0; h < 2; ++h) {
+              const int ka = k0 + 2 * h, kb = ka + 1;
+              unsigned long long wa[CG], wb[CG];
+              if (ka >= first && ka <= last) load_cols<CG>(slot_ptr(a, ka) + at, wa);
               else
 #pragma unroll
-                for (int cc = 0; cc < CG; ++cc) w[q][cc] = 0;
-            }
+                for (int cc = 0; cc < CG; ++cc) wa[cc] = 0;
+              if (kb >= first && kb <= last) load_cols<CG>(slot_ptr(a, kb) + at, wb);
+              else
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
-              const int k = k0 + q;
+                for (int cc = 0; cc < CG; ++cc) wb[cc] = 0;
 #pragma unroll
               for (int cc = 0; cc < CG; ++cc) {
-                const unsigned long long x = w[q][cc];
-                f[cc] |= x;
-                if (k & 1) p0[cc] |= x;
-                if (k & 2) p1[cc] |= x;
-                if (k & 4) p2[cc] |= x;
-                if (k & 8) p3[cc] |= x;
+                const unsigned long long u = wa[cc] | wb[cc];
+                f[cc] |= u;
+                p0[cc] |= wb[cc];
+                if (h) p1[cc] |= u;
+                if (k0 & 4) p2[cc] |= u;
+                if (k0 & 8) p3[cc] |= u;
               }
             }
           }
@@ -1002,17 +1046,12 @@ __device__ void flush_span(const BatchArgs& a, const FlushState& fs, int64_t v0,
         for (int cc = 0; cc < CG; ++cc) {
 #pragma unroll
           for (int hw = 0; hw < 2; ++hw) {
-            const uint32_t fh = (uint32_t)(f[cc] >> (32 * hw)), h0 = (uint32_t)(p0[cc] >> (32 * hw)),
-                           h1 = (uint32_t)(p1[cc] >> (32 * hw)), h2 = (uint32_t)(p2[cc] >> (32 * hw)),
-                           h3 = (uint32_t)(p3[cc] >> (32 * hw));
+            uint32_t o[8];
+            planes_to_tile_words((uint32_t)(f[cc] >> (32 * hw)), (uint32_t)(p0[cc] >> (32 * hw)),
+                                 (uint32_t)(p1[cc] >> (32 * hw)), (uint32_t)(p2[cc] >> (32 * hw)),
+                                 (uint32_t)(p3[cc] >> (32 * hw)), o);
 #pragma unroll
-            for (int n = 0; n < 8; ++n) {
-              const int sh = 4 * n;
-              uint32_t o = ~(spread4((fh >> sh) & 15u, 0) * 0xFFu);  // 0xFF where not found
-              o |= spread4((h0 >> sh) & 15u, 0) | spread4((h1 >> sh) & 15u, 1) | spread4((h2 >> sh) & 15u, 2);
-              if (four_planes) o |= spread4((h3 >> sh) & 15u, 3);
-              fs.tile[tile_word<CG>(vi, cc * 16 + hw * 8 + n)] = o;
-            }
+            for (int n = 0; n < 8; ++n) fs.tile[tile_word<CG>(vi, cc * 16 + hw * 8 + n)] = o[n];
           }
         }
         if (in) {
