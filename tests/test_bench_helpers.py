@@ -14,7 +14,7 @@ def test_profile_figures_parse():
     import bench
     assert bench.profiled_traffic(bench.TRAFFIC_PROFILE) == 168.5e6
     assert bench.profiled_traffic(bench.TRAFFIC_PROFILE, "directed_entries") == 128311084
-    assert bench.profiled_traffic("bfs_batch_rmat_s21_256_graph.md", "dram_bytes_per_batch") == 4.882e9
+    assert bench.profiled_traffic("bfs_batch_rmat_s21_256_graph.md", "dram_bytes_per_batch") == 4.890e9
     assert bench.profiled_traffic("bfs_batch_rmat_s21_256_graph.md", "directed_entries") == 63536952
     assert bench.profiled_traffic("no_such_summary.md") is None
 
