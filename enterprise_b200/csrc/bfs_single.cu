@@ -69,6 +69,7 @@ constexpr int NROUND = 4;        // rounds of 32 edges a warp keeps in flight to
 constexpr int NC_MAX = 16;       // CTAs per cluster, at most
 constexpr int NQCAP = 4096;      // small-frontier entries per CTA and buffer
 constexpr uint32_t NF_HEAVY = 1, NF_SPILL = 2;
+constexpr int LCAP = 128;        // vertices a CTA of a listing bottom-up level keeps (then the bitmap is used)
 constexpr int BU_ILP = 2;        // bottom-up light path: neighbours checked per step (2 beat 4 and 8)
 
 // Device-resident loop state. Written only by the reset kernel's and the
@@ -103,7 +104,8 @@ struct BfsCtl {
   uint32_t tile_ticket;
   uint32_t finished;
   uint32_t epoch;
-  uint32_t pad2;
+  int32_t bu_list;    // the bottom-up level being expanded also lists what it finds in raw
+  int32_t list_over;  // ... and a CTA found more than it could list: use the frontier bitmap
 };
 
 struct LevelArgs {
@@ -237,6 +239,8 @@ __global__ void k_init(LevelArgs a, int32_t src, int32_t* depth, int32_t* parent
     c->n_chunks = 0;
   }
   c->n_raw = 0;
+  c->bu_list = 0;
+  c->list_over = 0;
   c->done = 0;
   c->narrow = 0;
   c->err = 0;
@@ -395,6 +399,13 @@ __device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, 
       s_hub[i] = key ? (int)(uint32_t)key : -1;
     }
   }
+  // listing levels: this CTA's finds, appended to raw once at the end
+  __shared__ uint32_t s_lcnt, s_lbase, s_listing;
+  __shared__ int32_t s_list[LCAP];
+  if (threadIdx.x == 0) {
+    s_lcnt = 0;
+    s_listing = c->bu_list;  // read from shared memory where needed: no register held in the loop
+  }
   __syncthreads();
   const Front is_front{fbc, s_hub, a.hub_slots, a.hub_shift};
   const int lane = threadIdx.x & 31;
@@ -475,6 +486,37 @@ __device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, 
       a.vis[wi] = a.vis[wi] | fm;
       fbn[wi] = fm;
     }
+  }
+  if (s_listing) {
+    // List this CTA's finds: re-read the next-frontier words its warps wrote
+    // (kept out of the loop above, which runs at its register limit). Lane 0
+    // wrote them: the warp barrier orders those stores before these loads.
+    __syncwarp();
+    for (int64_t w0 = gw; w0 < W; w0 += nw * 32) {
+      const int64_t wl = w0 + (int64_t)lane * nw;
+      const uint32_t fw = wl < W ? __ldcg(fbn + wl) : 0u;
+      unsigned any_w = __ballot_sync(FULL, fw != 0);
+      while (any_w) {
+        const int j = __ffs(any_w) - 1;
+        any_w &= any_w - 1;
+        const uint32_t fm = __shfl_sync(FULL, fw, j);
+        const int64_t wj = w0 + (int64_t)j * nw;
+        uint32_t p = 0;
+        if (lane == 0) p = atomicAdd(&s_lcnt, (uint32_t)__popc(fm));
+        p = __shfl_sync(FULL, p, 0) + __popc(fm & lanemask_lt());
+        if (((fm >> lane) & 1u) && p < (uint32_t)LCAP) s_list[p] = (int32_t)(wj * 32 + lane);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t n = s_lcnt;
+      s_lbase = 0;
+      if (n > (uint32_t)LCAP) c->list_over = 1;
+      else if (n) s_lbase = (uint32_t)atomicAdd(&c->n_raw, (int)n);
+    }
+    __syncthreads();
+    if (s_lcnt <= (uint32_t)LCAP)
+      for (uint32_t i = threadIdx.x; i < s_lcnt; i += BT) a.raw[s_lbase + i] = s_list[i];
   }
   const int any = __syncthreads_or(my_n != 0);
   if (any) {
@@ -615,7 +657,43 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
             n_next < c->n_f;
     const int64_t W = (a.V + 31) >> 5;
     for (int64_t i = gtid; i < W; i += nth) fbo[i] = 0;
-    if (to_td) {
+    if (to_td && c->bu_list && !c->list_over) {
+      // Hand over to TD from the list the expander made: classify raw (its
+      // vertices in the order the CTAs listed them) into q[qcur^1].
+      const int64_t n = c->n_raw;
+      const uint32_t ntiles = (uint32_t)((n + TILE - 1) / TILE);
+      while (true) {
+        const uint32_t tile = acquire_tile(c, &s_tile);
+        if (tile >= ntiles) break;
+        int32_t v[IPT];
+        load_tile(a.raw, (int64_t)tile * TILE, n, v);
+        int dg[IPT], cl[IPT];
+        uint32_t cnt[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < IPT; ++j) {
+          dg[j] = v[j] >= 0 ? a.deg[v[j]] : 0;
+          cl[j] = v[j] >= 0 ? cls_of(dg[j], a) : -1;
+          if (cl[j] >= 0) {
+            cnt[cl[j]]++;
+            my_maxd = max(my_maxd, (uint32_t)dg[j]);
+            if (cl[j] == 2) cnt[3] += n_chunks_of(dg[j], a);
+          }
+        }
+        uint32_t pre[4] = {cnt[0], cnt[1], cnt[2], cnt[3]}, agg[4], excl[4];
+        block_excl_scan<4>(pre, agg, s_scan);
+        lookback<4, KS>(a.tiles, tile, epoch, agg, excl, s_excl, err, a.fault_inject != 0);
+        uint32_t pos[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) pos[k] = excl[k] + pre[k];
+#pragma unroll
+        for (int j = 0; j < IPT; ++j)
+          if (cl[j] >= 0) qo.put(a, v[j], cl[j], dg[j], pos);
+        if (tile == ntiles - 1 && threadIdx.x == 0) {
+          for (int k = 0; k < 4; ++k) c->tot[k] = excl[k] + agg[k];
+          __threadfence();
+        }
+      }
+    } else if (to_td) {
       // Hand over to TD: classify the frontier bitmap (ascending ids) into
       // q[qcur^1]. A tile is BT*WPT words, WPT consecutive words per thread
       // (the frontier is sparse here: few look-back tiles, not few words).
@@ -693,7 +771,7 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   const int32_t n_raw = __ldcg(&c->n_raw), err0 = __ldcg(&c->err), it0 = __ldcg(&c->iters);
   const int32_t tdl = __ldcg(&c->td_levels), bul = __ldcg(&c->bu_levels);
   const int64_t acc_n = ld64(&c->acc_n), acc_m = ld64(&c->acc_m);
-  const int64_t n_vis0 = ld64(&c->n_vis), m_vis0 = ld64(&c->m_vis);
+  const int64_t n_vis0 = ld64(&c->n_vis), m_vis0 = ld64(&c->m_vis), n_f0 = ld64(&c->n_f);
   const uint32_t maxd = __ldcg(&c->acc_maxd);
   uint32_t tot[KS];
 #pragma unroll
@@ -746,6 +824,11 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   c->err = err1;
   c->done = done;
   c->narrow = narrow;
+  // A bottom-up level on a shrinking frontier usually finds few vertices and
+  // then hands over to top-down: it also lists them, so the inspector need not
+  // scan the frontier bitmap to classify them.
+  c->bu_list = !done && next_dir == BU && a.policy == ENT_POLICY_BEAMER && n_next < n_f0;
+  c->list_over = 0;
   c->skip = 0;
   c->acc_maxd = 0;
   c->iters = it0 + 1;

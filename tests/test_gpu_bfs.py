@@ -76,6 +76,22 @@ def test_option_variants(eb, orc, opts):
             _check(eb, orc, csr, g, src)
 
 
+@pytest.mark.parametrize("loop", ["graph", "host"])
+@pytest.mark.parametrize("alpha,beta", [(2.0, 4.0), (8.0, 16.0), (48.0, 1024.0), (4.0, 1e6)])
+def test_bottom_up_to_top_down_from_the_list(eb, orc, alpha, beta, loop):
+    """A bottom-up level on a shrinking frontier also lists what it finds, and
+    a switch to top-down after it classifies that list instead of scanning the
+    frontier bitmap; a CTA that finds more than it can list sends the switch
+    back to the bitmap. Small graphs give each CTA few status words, so both
+    happen across these direction thresholds (beta 1e6 switches back only for
+    tiny frontiers)."""
+    for csr in (eb.Csr.rmat(14, 16, seed=0x7157), eb.Csr.er(30000, 8.0, seed=0x7158)):
+        with _graph(eb, csr, loop=loop, alpha=alpha, beta=beta, narrow_max_frontier=0) as g:
+            for src in eb.pick_sources(csr.beg_pos, 19, 6):
+                st = _check(eb, orc, csr, g, src)
+                assert st.td_levels + st.bu_levels == st.levels
+
+
 def test_rmat_s16_64_sources_bit_exact(eb, orc):
     """R-MAT scale 16, edge factor 16, 64 seeded non-isolated sources."""
     host = eb.Csr.rmat(16, 16, seed=0x5EED0016)
