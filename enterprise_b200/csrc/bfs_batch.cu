@@ -632,7 +632,12 @@ __device__ void b_bu_expand(const BatchArgs& a, BatchCtl* c, unsigned long long*
   }
 }
 
-__global__ void __launch_bounds__(BB, 4) k_b_expand(BatchArgs a) {
+// One instantiation per width class: batches of up to 2 words per vertex fit
+// 6 resident CTAs per SM without spills, while 4 words per lane need the
+// registers of 4 (capped at 6 they spill, and the bottom-up levels slow down
+// more than the occupancy gains: s22/256 5.71 -> 6.37 ms, s22/64 2.66 -> 2.45).
+template <bool WIDE>
+__global__ void __launch_bounds__(BB, WIDE ? 4 : 6) k_b_expand(BatchArgs a) {
   extern __shared__ unsigned long long s_f[];
   __shared__ unsigned long long s_red[BB / 32], s_act[WMAX];
   BatchCtl* c = a.ctl;
@@ -644,9 +649,11 @@ __global__ void __launch_bounds__(BB, 4) k_b_expand(BatchArgs a) {
     __syncthreads();
     if (a.W == 1) b_bu_expand<1>(a, c, s_red, s_act);
     else if (a.W == 2) b_bu_expand<2>(a, c, s_red, s_act);
-    else b_bu_expand<4>(a, c, s_red, s_act);
+    else if constexpr (WIDE) b_bu_expand<4>(a, c, s_red, s_act);
   }
 }
+
+static void* expand_kernel(int W) { return W > 2 ? (void*)k_b_expand<true> : (void*)k_b_expand<false>; }
 
 // ----------------------------------------------------------- commit -------
 // Folds v's claimed words NB[v] into X[v] (warp-uniform call; `valid` lanes
@@ -1361,7 +1368,7 @@ int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream
     void* kf[2] = {&la, &zero};
     cudaKernelNodeParams kp = {};
     kp.blockDim = dim3(BB);
-    kp.func = (void*)k_b_expand;
+    kp.func = expand_kernel(w->W);
     kp.gridDim = dim3(w->grid);
     kp.sharedMemBytes = (unsigned)w->smem;
     kp.kernelParams = kl;
@@ -1488,7 +1495,7 @@ int create_batch_workspace(ent_graph* g, int n_src, BatchWorkspace** out) {
     a.n_large = hc[1];
   }
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_b_expand, BB, w->smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, expand_kernel(W), BB, w->smem);
   if (occ < 1) occ = 1;
   // small graphs get small grids so that the branches of a multi-graph
   // launch can run side by side
@@ -1754,7 +1761,8 @@ int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t
     t.frontier_edges = h.m_f;
     t.unvisited_queued = (int64_t)g->E - h.m_done;
     ENT_CUDA(cudaEventRecord(e[0], s));
-    k_b_expand<<<w->grid, BB, w->smem, s>>>(a);
+    if (w->W > 2) k_b_expand<true><<<w->grid, BB, w->smem, s>>>(a);
+    else k_b_expand<false><<<w->grid, BB, w->smem, s>>>(a);
     ENT_CUDA(cudaEventRecord(e[1], s));
     k_b_commit<<<w->grid, BB, 0, s>>>(a);
     k_b_flush<<<w->grid_flush, BB, w->smem_flush, s>>>(a, 0);
