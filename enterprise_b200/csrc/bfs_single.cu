@@ -47,6 +47,7 @@
 //    a classification whose wait ran out ends the traversal with an error
 //    bit instead of handing on inconsistent queues.
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 #include <string.h>
 
@@ -195,9 +196,31 @@ __device__ void fill_neg1(int32_t* p, int64_t n, int64_t tid, int64_t nth) {
   for (int64_t i = head + nvec * 4 + tid; i < n; i += nth) p[i] = -1;
 }
 
-__global__ void __launch_bounds__(BT) k_reset(LevelArgs a, int32_t src, int32_t* depth, int32_t* parent) {
+// Byte depths, the reference's depth_t (unsigned char, comm.h:69): depth d
+// (0..254) as d, unreached as 255 (INFTY, comm.h:131).
+__device__ void fill_ff(uint8_t* p, int64_t n, int64_t tid, int64_t nth) {
+  const uintptr_t addr = (uintptr_t)p;
+  int64_t head = (int64_t)((16 - (addr & 15)) & 15);
+  if (head > n) head = n;
+  for (int64_t i = tid; i < head; i += nth) p[i] = 0xFF;
+  const int64_t nvec = (n - head) >> 4;
+  uint4* pv = reinterpret_cast<uint4*>(p + head);
+  for (int64_t i = tid; i < nvec; i += nth) pv[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
+  for (int64_t i = head + nvec * 16 + tid; i < n; i += nth) p[i] = 0xFF;
+}
+__device__ __forceinline__ void fill_unreached(int32_t* p, int64_t n, int64_t tid, int64_t nth) {
+  fill_neg1(p, n, tid, nth);
+}
+__device__ __forceinline__ void fill_unreached(uint8_t* p, int64_t n, int64_t tid, int64_t nth) {
+  fill_ff(p, n, tid, nth);
+}
+
+// The level kernels are instantiated for int32 depths and for the reference's
+// byte depths (DT = uint8_t: written directly, no conversion pass).
+template <class DT>
+__global__ void __launch_bounds__(BT) k_reset(LevelArgs a, int32_t src, DT* depth, int32_t* parent) {
   const int64_t tid = blockIdx.x * (int64_t)BT + threadIdx.x, nth = (int64_t)gridDim.x * BT;
-  fill_neg1(depth, a.V, tid, nth);
+  fill_unreached(depth, a.V, tid, nth);
   if (parent) fill_neg1(parent, a.V, tid, nth);
   const int64_t W = (a.V + 31) >> 5;
   for (int64_t i = tid; i < W; i += nth) {
@@ -214,7 +237,8 @@ __global__ void __launch_bounds__(BT) k_reset(LevelArgs a, int32_t src, int32_t*
 // Initialises the loop state for one traversal (one thread; runs after
 // k_reset, so it needs no completion counter and also resets the counters
 // the level kernels use).
-__global__ void k_init(LevelArgs a, int32_t src, int32_t* depth, int32_t* parent) {
+template <class DT>
+__global__ void k_init(LevelArgs a, int32_t src, DT* depth, int32_t* parent) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   BfsCtl* c = a.ctl;
   const int d = a.deg[src];
@@ -225,7 +249,7 @@ __global__ void k_init(LevelArgs a, int32_t src, int32_t* depth, int32_t* parent
   a.fb[0][src >> 5] = 1u << (src & 31);
   a.q[0][cl][0] = src;
   c->src = src;
-  c->depth = depth;
+  c->depth = reinterpret_cast<int32_t*>(depth);  // the level kernels of this DT cast it back
   c->parent = parent;
   c->level = 0;
   c->dir = a.policy == ENT_POLICY_BU_ONLY ? BU : TD;
@@ -264,8 +288,9 @@ __global__ void k_init(LevelArgs a, int32_t src, int32_t* depth, int32_t* parent
 }
 
 // ------------------------------------------------------------ top-down ----
+template <class DT>
 __device__ __forceinline__ void td_visit(const LevelArgs& a, BfsCtl* c, int v, int u, bool valid, int ln,
-                                         int32_t* depth, int32_t* parent, uint32_t* fbn) {
+                                         DT* depth, int32_t* parent, uint32_t* fbn) {
   bool mine = false;
   if (valid) {
     const uint32_t w = (uint32_t)v >> 5, b = 1u << (v & 31);
@@ -273,7 +298,7 @@ __device__ __forceinline__ void td_visit(const LevelArgs& a, BfsCtl* c, int v, i
       const uint32_t old = atomicOr(a.vis + w, b);
       if (!(old & b)) {
         mine = true;
-        depth[v] = ln;
+        depth[v] = (DT)ln;
         if (parent) parent[v] = u;
         red_or(fbn + w, b);
       }
@@ -290,7 +315,8 @@ __device__ __forceinline__ void td_visit(const LevelArgs& a, BfsCtl* c, int v, i
   }
 }
 
-__device__ void td_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, int32_t* parent) {
+template <class DT>
+__device__ void td_expand(const LevelArgs& a, BfsCtl* c, int L, DT* depth, int32_t* parent) {
   const int qc = c->qcur;
   const int ns = c->n_q[0], nm = c->n_q[1], nl = c->n_q[2], nch = c->n_chunks;
   const int32_t* __restrict__ qs = a.q[qc][0];
@@ -387,7 +413,8 @@ struct Front {
   }
 };
 
-__device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, int32_t* parent, int32_t* s_hub,
+template <class DT>
+__device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, DT* depth, int32_t* parent, int32_t* s_hub,
                           unsigned long long* s_red) {
   const uint32_t* fbc = a.fb[L & 1];
   uint32_t* fbn = a.fb[(L + 1) & 1];
@@ -474,7 +501,7 @@ __device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, 
       if (lane == j && hit >= 0) { found = true; pu = hit; }
     }
     if (found) {
-      depth[v] = ln;
+      depth[v] = (DT)ln;
       if (parent) parent[v] = pu;
       my_n++;
       my_m += (unsigned long long)d;
@@ -527,14 +554,16 @@ __device__ void bu_expand(const LevelArgs& a, BfsCtl* c, int L, int32_t* depth, 
   }
 }
 
+template <class DT>
 __global__ void __launch_bounds__(BT, 8) k_expand(LevelArgs a) {
   extern __shared__ int32_t s_hub[];
   __shared__ unsigned long long s_red[BT / 32];
   BfsCtl* c = a.ctl;
   if (c->done || c->skip) return;
   const int L = c->level;
-  if (c->dir == TD) td_expand(a, c, L, c->depth, c->parent);
-  else bu_expand(a, c, L, c->depth, c->parent, s_hub, s_red);
+  DT* depth = reinterpret_cast<DT*>(c->depth);
+  if (c->dir == TD) td_expand(a, c, L, depth, c->parent);
+  else bu_expand(a, c, L, depth, c->parent, s_hub, s_red);
 }
 
 // ----------------------------------------------------------- inspector ----
@@ -927,6 +956,7 @@ __device__ __forceinline__ void narrow_append(const LevelArgs& a, BfsCtl* c, boo
 //    shared-memory entries) and arrives.
 // Every CTA takes the same decisions from the same counts, so all reach the
 // same barriers; there are no spin waits.
+template <class DT>
 __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
   extern __shared__ int4 s_q[];  // [2][NQCAP]
   __shared__ uint32_t s_cnt[2], s_flag[2];
@@ -940,7 +970,7 @@ __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const bool coord = warp == NWE;
   const int gw = rank * NWE + warp, nwt = nc * NWE;
-  int32_t* depth = c->depth;
+  DT* depth = reinterpret_cast<DT*>(c->depth);
   int32_t* parent = c->parent;
   const int L0 = c->level;
   const int qcur = c->qcur;
@@ -1078,7 +1108,7 @@ __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
                 vd[q] = (int)(o1 - o0);
                 // the next level walks this row: start its first sector towards L2 now
                 asm volatile("prefetch.global.L2 [%0];" ::"l"(a.adj + o0));
-                depth[x] = ln;
+                depth[x] = (DT)ln;
                 if (parent) parent[x] = uj[q];
               }
             }
@@ -1163,24 +1193,15 @@ __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
   __threadfence();
 }
 
-// Packs int32 depths into the reference's byte format (depth_t = unsigned
-// char, comm.h:69): depth d (0..254) as d, unreached (-1) as 255 (INFTY,
-// comm.h:131). A thread packs 16 depths: four 16-byte loads, one 16-byte store.
-__global__ void __launch_bounds__(256) k_depth_u8(const int32_t* __restrict__ d, uint8_t* __restrict__ o, int64_t V) {
-  const auto pk = [](int x) { return (uint32_t)(x < 0 ? 255 : x) & 0xFFu; };
-  const int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 16;
-  if (i + 16 <= V) {  // both buffers are allocation bases and i % 16 == 0: 16-byte aligned
-    const int4* p = reinterpret_cast<const int4*>(d + i);
-    uint32_t w[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int4 x = __ldcs(p + q);
-      w[q] = pk(x.x) | pk(x.y) << 8 | pk(x.z) << 16 | pk(x.w) << 24;
-    }
-    *reinterpret_cast<uint4*>(o + i) = make_uint4(w[0], w[1], w[2], w[3]);
-  } else {
-    for (int64_t j = i; j < V; ++j) o[j] = (uint8_t)pk(d[j]);
-  }
+// Pulls a finished byte-depth row into L2 (kept there preferentially) before
+// its copy to the host: the traversal wrote it as bytes scattered over all its
+// levels, mostly evicted since, and the copy engine would otherwise read it
+// from DRAM that the next traversal keeps busy (s24, 64 sources: 36.2 against
+// 44.9 ms with every row copied; one prefetch per 128-byte line).
+__global__ void __launch_bounds__(256) k_row_to_l2(const uint8_t* __restrict__ p, int64_t n) {
+  const int64_t step = (int64_t)gridDim.x * blockDim.x * 128;
+  for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) * 128; i < n; i += step)
+    asm volatile("prefetch.global.L2::evict_last [%0];" ::"l"(p + i));
 }
 
 // ------------------------------------------------------------- host -------
@@ -1197,10 +1218,11 @@ struct BfsWorkspace {
   size_t smem_expand = 0;
   int narrow_nc = 0;        // CTAs of the small-frontier cluster (0: mode off)
   size_t smem_narrow = 0;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  cudaGraphNode_t reset_node = nullptr;
-  cudaGraphNode_t init_node = nullptr;
+  // the traversal graph, [0] for int32 depths, [1] for byte depths (built on first use)
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  cudaGraphNode_t reset_node[2] = {nullptr, nullptr};
+  cudaGraphNode_t init_node[2] = {nullptr, nullptr};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // ent_bfs_many: a second depth buffer, a copy stream and pinned per-source
   // copies of the control block (created on first use)
@@ -1210,13 +1232,18 @@ struct BfsWorkspace {
   BfsCtl* many_ctl_h = nullptr;
   int32_t many_cap = 0;
   std::vector<cudaEvent_t> many_ev;          // [2i], [2i+1] bracket traversal i
-  cudaEvent_t many_sync[3] = {nullptr, nullptr, nullptr};  // buffer 0 / 1 copied, row packed
+  cudaEvent_t many_sync[3] = {nullptr, nullptr, nullptr};  // buffer 0 / 1 copied, byte row in L2
 };
+
+template <class DT>
+constexpr int depth_kind() { return std::is_same<DT, uint8_t>::value ? 1 : 0; }
 
 void destroy_bfs_workspace(BfsWorkspace* w) {
   if (!w) return;
-  if (w->exec) cudaGraphExecDestroy(w->exec);
-  if (w->graph) cudaGraphDestroy(w->graph);
+  for (int k = 0; k < 2; ++k) {
+    if (w->exec[k]) cudaGraphExecDestroy(w->exec[k]);
+    if (w->graph[k]) cudaGraphDestroy(w->graph[k]);
+  }
   if (w->slab) cudaFree(w->slab);
   if (w->ctl) cudaFree(w->ctl);
   if (w->ctl_h) cudaFreeHost(w->ctl_h);
@@ -1235,27 +1262,29 @@ void destroy_bfs_workspace(BfsWorkspace* w) {
   delete w;
 }
 
+template <class DT>
 static int build_graph(ent_graph* g, BfsWorkspace* w) {
+  const int k = depth_kind<DT>();
   cudaGraph_t graph;
   ENT_CUDA(cudaGraphCreate(&graph, 0));
-  w->graph = graph;
+  w->graph[k] = graph;
   LevelArgs ra = w->args;
   ra.use_cond = 0;
   int32_t src0 = 0;
-  int32_t* d0 = w->depth;
+  DT* d0 = reinterpret_cast<DT*>(w->depth);  // placeholders: launch_graph sets each launch's
   int32_t* p0 = nullptr;
   void* rargs[4] = {&ra, &src0, &d0, &p0};
   cudaKernelNodeParams kp = {};
-  kp.func = (void*)k_reset;
+  kp.func = (void*)k_reset<DT>;
   kp.gridDim = dim3(w->grid_reset);
   kp.blockDim = dim3(BT);
   kp.sharedMemBytes = 0;
   kp.kernelParams = rargs;
-  ENT_CUDA(cudaGraphAddKernelNode(&w->reset_node, graph, nullptr, 0, &kp));
-  kp.func = (void*)k_init;
+  ENT_CUDA(cudaGraphAddKernelNode(&w->reset_node[k], graph, nullptr, 0, &kp));
+  kp.func = (void*)k_init<DT>;
   kp.gridDim = dim3(1);
   kp.blockDim = dim3(32);
-  ENT_CUDA(cudaGraphAddKernelNode(&w->init_node, graph, &w->reset_node, 1, &kp));
+  ENT_CUDA(cudaGraphAddKernelNode(&w->init_node[k], graph, &w->reset_node[k], 1, &kp));
   cudaGraphConditionalHandle handle;
   ENT_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
   cudaGraphNodeParams cp = {};
@@ -1264,7 +1293,7 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
   cp.conditional.type = cudaGraphCondTypeWhile;
   cp.conditional.size = 1;
   cudaGraphNode_t cond_node;
-  ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &w->init_node, 1, &cp));
+  ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &w->init_node[k], 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   // Loop body: expand -> inspect -> if (narrow) { small-frontier cluster }.
   LevelArgs la = w->args;
@@ -1274,7 +1303,7 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
     ENT_CUDA(cudaGraphConditionalHandleCreate(&la.cond_narrow, body, 0, cudaGraphCondAssignDefault));
   void* largs[1] = {&la};
   cudaKernelNodeParams bp = {};
-  bp.func = (void*)k_expand;
+  bp.func = (void*)k_expand<DT>;
   bp.gridDim = dim3(w->grid_expand);
   bp.blockDim = dim3(BT);
   bp.sharedMemBytes = (unsigned)w->smem_expand;
@@ -1293,7 +1322,7 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
     ip.conditional.size = 1;
     cudaGraphNode_t n_if, n_narrow;
     ENT_CUDA(cudaGraphAddNode(&n_if, body, &n_inspect, 1, &ip));
-    bp.func = (void*)k_narrow;
+    bp.func = (void*)k_narrow<DT>;
     bp.gridDim = dim3(w->narrow_nc);
     bp.blockDim = dim3(NT);
     bp.sharedMemBytes = (unsigned)w->smem_narrow;
@@ -1304,10 +1333,11 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
     cv.clusterDim.z = 1;
     ENT_CUDA(cudaGraphKernelNodeSetAttribute(n_narrow, cudaLaunchAttributeClusterDimension, &cv));
   }
-  ENT_CUDA(cudaGraphInstantiate(&w->exec, graph, 0));
+  ENT_CUDA(cudaGraphInstantiate(&w->exec[k], graph, 0));
   return ENT_OK;
 }
 
+template <class DT>
 static cudaError_t launch_narrow(const BfsWorkspace* w, const LevelArgs& la, cudaStream_t s) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(w->narrow_nc);
@@ -1321,14 +1351,16 @@ static cudaError_t launch_narrow(const BfsWorkspace* w, const LevelArgs& la, cud
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_narrow, la);
+  return cudaLaunchKernelEx(&cfg, k_narrow<DT>, la);
 }
 
 // Largest cluster (<= limit CTAs, 0 = no limit) of the small-frontier kernel
 // that can be resident on this GPU; 0 if none.
 static int pick_narrow_cluster(int limit, size_t smem) {
-  if (cudaFuncSetAttribute(k_narrow, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-      cudaFuncSetAttribute(k_narrow, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+  if (cudaFuncSetAttribute(k_narrow<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_narrow<int32_t>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess ||
+      cudaFuncSetAttribute(k_narrow<uint8_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(k_narrow<uint8_t>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -1346,7 +1378,7 @@ static int pick_narrow_cluster(int limit, size_t smem) {
     cfg.attrs = at;
     cfg.numAttrs = 1;
     int n = 0;
-    if (cudaOccupancyMaxActiveClusters(&n, k_narrow, &cfg) == cudaSuccess && n >= 1) return nc;
+    if (cudaOccupancyMaxActiveClusters(&n, k_narrow<int32_t>, &cfg) == cudaSuccess && n >= 1) return nc;
     cudaGetLastError();
   }
   return 0;
@@ -1421,7 +1453,7 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out, bool force_graph =
   a.max_levels = (int32_t)std::min<int64_t>(V + 2, 0x7ffffff0);
   w->smem_expand = sizeof(int32_t) * (hub > 0 ? hub : 1);
   int occ_e = 0, occ_i = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e, k_expand, BT, w->smem_expand);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_e, k_expand<int32_t>, BT, w->smem_expand);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_i, k_inspect, BT, 0);
   if (occ_e < 1) occ_e = 1;
   if (occ_i < 1) occ_i = 1;
@@ -1440,7 +1472,7 @@ static int create_workspace(ent_graph* g, BfsWorkspace** out, bool force_graph =
     a.narrow_deg = o.narrow_max_degree;
   }
   if (o.loop == ENT_LOOP_GRAPH || force_graph) {
-    int rc = build_graph(g, w);
+    int rc = build_graph<int32_t>(g, w);
     if (rc != ENT_OK) { destroy_bfs_workspace(w); return rc; }
   }
   *out = w;
@@ -1464,28 +1496,34 @@ static void fill_stats(const BfsCtl& h, float ms, ent_stats* stats) {
 }
 
 // One launch of the workspace's instantiated traversal graph on stream s.
-static int launch_graph(BfsWorkspace* w, int32_t src, int32_t* depth, int32_t* parent, cudaStream_t s) {
+template <class DT>
+static int launch_graph(ent_graph* g, BfsWorkspace* w, int32_t src, DT* depth, int32_t* parent, cudaStream_t s) {
+  const int k = depth_kind<DT>();
+  if (!w->exec[k]) {  // the byte-depth graph is built on first use
+    int rc = build_graph<DT>(g, w);
+    if (rc != ENT_OK) return rc;
+  }
   LevelArgs ra = w->args;
   ra.use_cond = 0;
   void* rargs[4] = {&ra, &src, &depth, &parent};
   cudaKernelNodeParams kp = {};
-  kp.func = (void*)k_reset;
+  kp.func = (void*)k_reset<DT>;
   kp.gridDim = dim3(w->grid_reset);
   kp.blockDim = dim3(BT);
   kp.sharedMemBytes = 0;
   kp.kernelParams = rargs;
-  ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec, w->reset_node, &kp));
-  kp.func = (void*)k_init;
+  ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec[k], w->reset_node[k], &kp));
+  kp.func = (void*)k_init<DT>;
   kp.gridDim = dim3(1);
   kp.blockDim = dim3(32);
-  ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec, w->init_node, &kp));
-  ENT_CUDA(cudaGraphLaunch(w->exec, s));
+  ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec[k], w->init_node[k], &kp));
+  ENT_CUDA(cudaGraphLaunch(w->exec[k], s));
   return ENT_OK;
 }
 
 int launch_bfs_single(BfsWorkspace* w, int32_t src, int32_t* depth_dev, cudaStream_t s) {
   g_kernel_launches += 2;  // reset + init; the level kernels are counted by bfs_single_stats
-  return launch_graph(w, src, depth_dev, nullptr, s);
+  return launch_graph(nullptr, w, src, depth_dev, nullptr, s);  // int32 graph: built with the workspace
 }
 
 int bfs_single_stats(BfsWorkspace* w, cudaStream_t s, ent_stats* stats) {
@@ -1497,7 +1535,8 @@ int bfs_single_stats(BfsWorkspace* w, cudaStream_t s, ent_stats* stats) {
   return ENT_OK;
 }
 
-int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, cudaStream_t stream, ent_stats* stats) {
+template <class DT>
+static int run_bfs_typed(ent_graph* g, int32_t src, DT* depth, int32_t* parent, cudaStream_t stream, ent_stats* stats) {
   if (!g->ws) {
     int rc = create_workspace(g, &g->ws);
     if (rc != ENT_OK) return rc;
@@ -1506,18 +1545,18 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, c
   cudaStream_t s = stream ? stream : g->stream;
   if (stats) ENT_CUDA(cudaEventRecord(w->ev0, s));
   if (g->opts.loop == ENT_LOOP_GRAPH) {
-    int rc = launch_graph(w, src, depth, parent, s);
+    int rc = launch_graph(g, w, src, depth, parent, s);
     if (rc != ENT_OK) return rc;
   } else {
     LevelArgs la = w->args;
     la.use_cond = 0;
-    k_reset<<<w->grid_reset, BT, 0, s>>>(la, src, depth, parent);
-    k_init<<<1, 32, 0, s>>>(la, src, depth, parent);
+    k_reset<DT><<<w->grid_reset, BT, 0, s>>>(la, src, depth, parent);
+    k_init<DT><<<1, 32, 0, s>>>(la, src, depth, parent);
     g_kernel_launches += 2;
     ENT_CUDA(cudaGetLastError());
     int32_t* flags_h = &w->ctl_h->done;  // done, narrow
     for (int64_t it = 0;; ++it) {
-      k_expand<<<w->grid_expand, BT, w->smem_expand, s>>>(la);
+      k_expand<DT><<<w->grid_expand, BT, w->smem_expand, s>>>(la);
       k_inspect<<<w->grid_inspect, BT, 0, s>>>(la);
       g_kernel_launches += 2;
       ENT_CUDA(cudaGetLastError());
@@ -1525,7 +1564,7 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, c
       ENT_CUDA(cudaStreamSynchronize(s));
       if (flags_h[0]) break;
       if (flags_h[1]) {
-        ENT_CUDA(launch_narrow(w, la, s));
+        ENT_CUDA(launch_narrow<DT>(w, la, s));
         g_kernel_launches += 1;
       }
       if (it > w->V + 2) return fail(ENT_ERR_INTERNAL, "level loop did not terminate");
@@ -1544,6 +1583,10 @@ int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, c
     g_kernel_launches += 2;  // reset + init; level kernels are counted when stats are read
   }
   return ENT_OK;
+}
+
+int run_bfs_single(ent_graph* g, int32_t src, int32_t* depth, int32_t* parent, cudaStream_t stream, ent_stats* stats) {
+  return run_bfs_typed<int32_t>(g, src, depth, parent, stream, stats);
 }
 
 int probe_graph_levels(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* levels) {
@@ -1688,7 +1731,7 @@ int run_bfs_deep(ent_graph* g, const int32_t* src, int32_t n_src, void* depth_de
     const int k = i % n_lanes;
     BfsWorkspace* w = l->w[k];
     int32_t* row = bytes ? w->depth : static_cast<int32_t*>(depth_dev) + (size_t)i * V;
-    rc = launch_graph(w, src[i], row, nullptr, l->s[k]);
+    rc = launch_graph(g, w, src[i], row, nullptr, l->s[k]);
     if (rc != ENT_OK) return rc;
     if (bytes)
       k_depth_u8_row<<<pack_blocks, 256, 0, l->s[k]>>>(w->depth, static_cast<uint8_t*>(depth_dev) + (size_t)i * V, V);
@@ -1754,8 +1797,8 @@ int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_l
   LevelArgs la = w->args;
   la.use_cond = 0;
   ENT_CUDA(cudaEventRecord(w->ev0, s));
-  k_reset<<<w->grid_reset, BT, 0, s>>>(la, src, w->depth, nullptr);
-  k_init<<<1, 32, 0, s>>>(la, src, w->depth, nullptr);
+  k_reset<int32_t><<<w->grid_reset, BT, 0, s>>>(la, src, w->depth, nullptr);
+  k_init<int32_t><<<1, 32, 0, s>>>(la, src, w->depth, nullptr);
   g_kernel_launches += 2;
   int n = 0;
   for (;;) {
@@ -1773,7 +1816,7 @@ int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_l
       t.frontier_edges = h.m_f;
       t.unvisited_queued = 0;
       ENT_CUDA(cudaEventRecord(e[0], s));
-      ENT_CUDA(launch_narrow(w, la, s));
+      ENT_CUDA(launch_narrow<int32_t>(w, la, s));
       ENT_CUDA(cudaEventRecord(e[1], s));
       g_kernel_launches += 1;
       ENT_CUDA(cudaEventSynchronize(e[1]));
@@ -1792,7 +1835,7 @@ int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_l
     t.frontier_edges = h.m_f;
     t.unvisited_queued = 0;
     ENT_CUDA(cudaEventRecord(e[0], s));
-    k_expand<<<w->grid_expand, BT, w->smem_expand, s>>>(la);
+    k_expand<int32_t><<<w->grid_expand, BT, w->smem_expand, s>>>(la);
     ENT_CUDA(cudaEventRecord(e[1], s));
     k_inspect<<<w->grid_inspect, BT, 0, s>>>(la);
     ENT_CUDA(cudaEventRecord(e[2], s));
@@ -1866,7 +1909,7 @@ static int bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, void* const
   }
   if (n_src == 0) return ENT_OK;
   BfsWorkspace* w = g->ws;
-  if (!w->depth_b && cudaMalloc(&w->depth_b, sizeof(int32_t) * g->V) != cudaSuccess) {
+  if (!bytes && !w->depth_b && cudaMalloc(&w->depth_b, sizeof(int32_t) * g->V) != cudaSuccess) {
     w->depth_b = nullptr;
     return fail(ENT_ERR_OOM, "second depth buffer (%lld bytes) failed", (long long)(sizeof(int32_t) * g->V));
   }
@@ -1888,7 +1931,7 @@ static int bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, void* const
   }
   const cudaStream_t s = g->stream, cs = w->copy_stream;
   // events (kept in the workspace): two per traversal for its time, and three
-  // to order the streams: each depth buffer's latest copy done, a row packed
+  // to order the streams: each depth buffer's latest copy done, a byte row in L2
   while (w->many_ev.size() < 2 * (size_t)n_src) {
     cudaEvent_t e = nullptr;
     if (cudaEventCreate(&e) != cudaSuccess) return fail(ENT_ERR_CUDA, "event creation failed");
@@ -1900,12 +1943,11 @@ static int bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, void* const
       return fail(ENT_ERR_CUDA, "event creation failed");
     }
   const std::vector<cudaEvent_t>& ev = w->many_ev;
-  int32_t* buf[2] = {w->depth, w->depth_b};
+  // byte depths are written by the traversal itself (the reference's depth_t)
+  void* buf[2] = {bytes ? (void*)w->depth8[0] : (void*)w->depth, bytes ? (void*)w->depth8[1] : (void*)w->depth_b};
   cudaEvent_t freed[2] = {w->many_sync[0], w->many_sync[1]};
-  const cudaEvent_t packed = w->many_sync[2];
   bool copied[2] = {false, false};
   const size_t row_bytes = (bytes ? 1 : sizeof(int32_t)) * g->V;
-  const unsigned pack_grid = (unsigned)((g->V + 16 * 256 - 1) / (16 * 256));
   int rc = ENT_OK;
   cudaError_t ce = cudaSuccess;
   int32_t done = 0;
@@ -1914,24 +1956,23 @@ static int bfs_many(ent_graph* g, const int32_t* src, int32_t n_src, void* const
     if (copied[b]) ce = cudaStreamWaitEvent(s, freed[b], 0);  // source i-2's copy has read buf[b]
     if (ce == cudaSuccess) ce = cudaEventRecord(ev[2 * (size_t)i], s);
     if (ce != cudaSuccess) break;
-    rc = run_bfs_single(g, src[i], buf[b], nullptr, s, nullptr);
+    rc = bytes ? run_bfs_typed<uint8_t>(g, src[i], (uint8_t*)buf[b], nullptr, s, nullptr)
+               : run_bfs_typed<int32_t>(g, src[i], (int32_t*)buf[b], nullptr, s, nullptr);
     if (rc != ENT_OK) break;
     ce = cudaEventRecord(ev[2 * (size_t)i + 1], s);
     if (ce == cudaSuccess)
       ce = cudaMemcpyAsync(&w->many_ctl_h[i], w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s);
     if (ce == cudaSuccess && depth_out && depth_out[i]) {
-      const void* from = buf[b];
       cudaEvent_t ready = ev[2 * (size_t)i + 1];
-      if (bytes) {  // pack on the traversal stream; buf[b] is reused only after this
-        k_depth_u8<<<pack_grid, 256, 0, s>>>(buf[b], w->depth8[b], g->V);
+      if (bytes) {
+        k_row_to_l2<<<(unsigned)((g->V + 128 * 256 - 1) / (128 * 256)), 256, 0, s>>>((const uint8_t*)buf[b], g->V);
         g_kernel_launches += 1;
         ce = cudaGetLastError();
-        if (ce == cudaSuccess) ce = cudaEventRecord(packed, s);
-        from = w->depth8[b];
-        ready = packed;
+        if (ce == cudaSuccess) ce = cudaEventRecord(w->many_sync[2], s);
+        ready = w->many_sync[2];
       }
       if (ce == cudaSuccess) ce = cudaStreamWaitEvent(cs, ready, 0);
-      if (ce == cudaSuccess) ce = cudaMemcpyAsync(depth_out[i], from, row_bytes, cudaMemcpyDeviceToHost, cs);
+      if (ce == cudaSuccess) ce = cudaMemcpyAsync(depth_out[i], buf[b], row_bytes, cudaMemcpyDeviceToHost, cs);
       if (ce == cudaSuccess) ce = cudaEventRecord(freed[b], cs);
       copied[b] = true;
     }

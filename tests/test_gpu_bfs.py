@@ -178,20 +178,33 @@ def test_many_sources_pipelined_to_host(eb, orc, loop):
             g.bfs_many([srcs[0], V], [None, None])
 
 
-def test_many_sources_byte_depths(eb, orc):
-    """ent_bfs_many_u8: the reference's byte depths (255 = unreached) equal
-    the oracle's depths; a traversal deeper than 254 levels is refused while
-    the other sources' rows are still written."""
-    csr = eb.Csr.rmat(13, 8, seed=23)  # isolated vertices give 255 entries
-    srcs = [int(s) for s in eb.pick_sources(csr.beg_pos, 24, 5)]
-    V = csr.vert_count
-    with eb.Graph.from_csr(csr) as g:
-        outs = [np.zeros(V, dtype=np.uint8) for _ in srcs]
-        stats = g.bfs_many(srcs, outs)
-        for s, d, st in zip(srcs, outs, stats):
-            exp, _ = orc.bfs(csr.beg_pos, csr.csr, s)
-            np.testing.assert_array_equal(d, np.where(exp < 0, 255, exp).astype(np.uint8))
-            assert st.reached_vertices == (exp >= 0).sum()
+@pytest.mark.parametrize("loop", ["graph", "host"])
+def test_many_sources_byte_depths(eb, orc, loop):
+    """ent_bfs_many_u8: the traversal writes the reference's byte depths (255 =
+    unreached) itself, equal to the oracle's depths, on an R-MAT graph and on a
+    grid that runs in the small-frontier kernel (under 255 levels); a
+    traversal deeper than 254 levels is refused while the other sources' rows
+    are still written."""
+    rm = eb.Csr.rmat(13, 8, seed=23)  # isolated vertices give 255 entries
+    grid = eb.Csr.grid(90, 70, 0.1, seed=25)
+    for csr, n_src in ((rm, 5), (grid, 3)):
+        srcs = [int(s) for s in eb.pick_sources(csr.beg_pos, 24, n_src)]
+        V = csr.vert_count
+        with _graph(eb, csr, loop=loop) as g:
+            outs = [np.zeros(V, dtype=np.uint8) for _ in srcs]
+            stats = g.bfs_many(srcs, outs)
+            for s, d, st in zip(srcs, outs, stats):
+                exp, _ = orc.bfs(csr.beg_pos, csr.csr, s)
+                assert exp.max() < 255
+                np.testing.assert_array_equal(d, np.where(exp < 0, 255, exp).astype(np.uint8))
+                assert st.reached_vertices == (exp >= 0).sum()
+                if csr is grid:
+                    assert st.narrow_levels > 0
+            # int32 rows from the same graph afterwards (the other instantiation)
+            d32 = [np.zeros(V, dtype=np.int32) for _ in srcs]
+            g.bfs_many(srcs, d32)
+            for s, d in zip(srcs, d32):
+                np.testing.assert_array_equal(d, orc.bfs(csr.beg_pos, csr.csr, s)[0])
     n = 300  # a path: depths up to 299
     path = eb.Csr.from_edges(np.arange(n - 1), np.arange(1, n), n)
     with eb.Graph.from_csr(path) as g:
