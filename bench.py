@@ -307,17 +307,20 @@ def run_ours(args, rank, world, dist):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
-            g.bfs_many(src_list, outs)
+            st_many = g.bfs_many(src_list, outs)
         el = time.perf_counter() - t0
         _, _, rate = replicas.job_rate(edges_per_step * e2e_steps, el, dist, dev)
+        # the same call's traversals alone (CUDA events around each, last step)
+        trav_ms = sum(x.device_ms for x in st_many)
+        trav_rate = sum(x.traversed_edges for x in st_many) / (trav_ms * 1e-3) if trav_ms > 0 else 0.0
         want = depth_ref_last if dtype == np.int32 else np.where(depth_ref_last < 0, 255, depth_ref_last).astype(np.uint8)
         ok = bool(np.array_equal(outs[-1], want))
         if pinned:
             eb.host_unregister(host)
-        return rate / 1e9, rows, pinned, ok
+        return rate / 1e9, rows, pinned, ok, trav_rate / 1e9
 
-    e2e_value, e2e_rows, pinned, e2e_ok = e2e_run(np.uint8)
-    e2e_i32, _, _, e2e_ok32 = e2e_run(np.int32)
+    e2e_value, e2e_rows, pinned, e2e_ok, trav_u8 = e2e_run(np.uint8)
+    e2e_i32, _, _, e2e_ok32, _ = e2e_run(np.int32)
 
     # ------------------------------------------- CPU baseline (rank 0, N=1)
     cpu = None
@@ -371,6 +374,9 @@ def run_ours(args, rank, world, dist):
                 "api": "ent_bfs_many_u8 (C ABI): every source's depths, in the reference's byte depth "
                        "type, copied to a host row, the copy overlapping the next traversal",
                 "host_rows": e2e_rows, "host_buffer_pinned": pinned, "last_row_matches_device_run": e2e_ok,
+                "traversal_device_gteps": round(trav_u8, 3),
+                "traversal_device_rule": "the call's traversals alone, CUDA events around each (last step): "
+                                         "the byte-depth traversal writes the reference's depth type itself",
                 "int32_depths": {"value": round(e2e_i32, 3), "api": "ent_bfs_many",
                                  "d2h_bytes_per_step": 4 * V * len(srcs), "last_row_matches_device_run": e2e_ok32}},
         "gpu_launches": launches,
