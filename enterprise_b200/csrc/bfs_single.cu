@@ -1107,7 +1107,8 @@ __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
                 vst[q] = o0;
                 vd[q] = (int)(o1 - o0);
                 // the next level walks this row: start its first sector towards L2 now
-                asm volatile("prefetch.global.L2 [%0];" ::"l"(a.adj + o0));
+                // (an empty row may start one past the array: nothing to fetch)
+                if (o1 > o0) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.adj + o0));
                 depth[x] = (DT)ln;
                 if (parent) parent[x] = uj[q];
               }
