@@ -120,6 +120,22 @@ def test_heavy_vertex_leaves_the_mode(eb, orc):
         assert 0 < st.narrow_levels < st.levels
 
 
+@pytest.mark.parametrize("loop", ["graph", "host"])
+def test_directed_path_ending_in_an_empty_row(eb, orc, loop):
+    """A directed CSR (top-down policy: it follows out-edges only) whose last
+    vertex, reached at the last level, has an empty row starting at E, one past
+    the adjacency array: the cluster claims it without touching that address."""
+    n = 400
+    beg = np.concatenate([np.arange(n, dtype=np.int64), [n - 1]])
+    adj = np.arange(1, n, dtype=np.int32)
+    csr = eb.Csr(beg, adj)
+    with _graph(eb, csr, loop=loop, policy="td") as g:
+        d, _, st = g.bfs(0)
+        exp, _ = orc.bfs(csr.beg_pos, csr.csr, 0)
+        np.testing.assert_array_equal(d, exp)
+        assert d[n - 1] == n - 1 and st.narrow_levels > 0
+
+
 def test_trace_shows_cluster_runs(eb, orc, grid):
     src = int(eb.pick_sources(grid.beg_pos, 15, 1)[0])
     with _graph(eb, grid) as g:
