@@ -595,7 +595,8 @@ def run_batched(args, rank=0, no_multi=False):
                 oracle_rows(hosts[k], [int(sources[k][0]), int(sources[k][63])], lambda j: dk[0 if j == 0 else 63])]
     out["multi_graph_48"] = {"ms": round(ms, 3), "graphs": 48, "sources_per_graph": 64, "vertices_total": total_v,
                              "gteps": round(edges / ms / 1e6, 2), "oracle_checked": 96, "oracle_mismatches": bad,
-                             "launches": "one CUDA graph launch, one branch per graph"}
+                             "launches": "one CUDA graph launch: one batched traversal over the disjoint union of "
+                                         "the graphs (one width class, shared source slots)"}
     plan.close()
     for gk in graphs:
         gk.close()

@@ -232,6 +232,7 @@ def lib() -> C.CDLL:
         "ent_multi_run": (C.c_int, [_P, C.POINTER(C.c_double)]),
         "ent_multi_depths": (C.c_int, [_P, C.c_int32, _I32P]),
         "ent_multi_destroy": (C.c_int, [_P]),
+        "ent_multi_trace": (C.c_int, [_P, C.c_int32, C.POINTER(_Trace), C.c_int32, _I32P]),
         "ent_replicas_plan": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, _I32P, _I32P]),
         "ent_replicas_create": (C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_P)]),
         "ent_replicas_set_max_batch": (C.c_int, [_P, C.c_int32]),
@@ -609,7 +610,9 @@ class Graph:
 
 
 class MultiPlan:
-    """Many graphs (one GPU) with their own sources, traversed by one launch."""
+    """Many graphs (one GPU) with their own sources, traversed by one launch
+    (mirror of ``ent_multi_*``): one batched traversal per width class over
+    the disjoint union of its graphs, copied at creation."""
 
     def __init__(self, graphs: Sequence[Graph], sources: Sequence[Sequence[int]]):
         self.graphs = list(graphs)
@@ -631,10 +634,24 @@ class MultiPlan:
         _check(lib().ent_multi_depths(self._h, k, _i32p(out)))
         return out
 
+    def trace(self, k: int = 0, max_levels: int = 100000) -> list[dict]:
+        """Per-level trace of the union that holds graph k (host-driven run of
+        the plan's kernels; its rows are then readable with depths())."""
+        buf = (_Trace * max_levels)()
+        n = C.c_int32()
+        _check(lib().ent_multi_trace(self._h, k, buf, max_levels, C.byref(n)))
+        return [{f[0]: getattr(buf[i], f[0]) for f in _Trace._fields_ if f[0] != "pad"} for i in range(n.value)]
+
     def close(self):
         if self._h is not None:
             lib().ent_multi_destroy(self._h)
             self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def __del__(self):
         try:

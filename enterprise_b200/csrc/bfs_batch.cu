@@ -63,6 +63,7 @@ struct BatchCtl {
   int32_t clear_done; // sources joined: the completion bits no longer hold (k_b_flush clears them)
   int32_t joined;     // sources that joined this run
   int32_t if_runs;    // level-loop iterations that ran the flush node
+  int32_t n_seed;     // entries of the seed list (0: one seed per source, src[s] for source s)
 };
 
 struct BatchArgs {
@@ -90,7 +91,8 @@ struct BatchArgs {
   int32_t n_mid, n_large;
   int32_t* jf[2];
   int32_t* heavy[2];
-  const int32_t* src;   // [n_src]
+  const int32_t* src;   // [n_src], or the seed vertices of a seed list
+  const int32_t* seed_slot;  // source of each seed-list entry (null: entry i seeds source i)
   unsigned long long* st_edges;  // per source: sum of degrees of reached vertices
   unsigned long long* st_verts;  // per source: reached vertices
   int32_t* st_maxd;              // per source: max depth
@@ -160,8 +162,12 @@ __global__ void k_b_seed(BatchArgs a) {
   __shared__ unsigned long long s_m;
   if (threadIdx.x == 0) { s_n = 0; s_h = 0; s_m = 0; }
   __syncthreads();
-  for (int s = threadIdx.x; s < c->n_src; s += blockDim.x) {
-    const int v = a.src[s];
+  // A seed list gives a source several start vertices: a traversal over the
+  // disjoint union of many graphs seeds source s in every graph at once.
+  const int n_seed = c->n_seed > 0 ? c->n_seed : c->n_src;
+  for (int i = threadIdx.x; i < n_seed; i += blockDim.x) {
+    const int v = a.src[i];
+    const int s = a.seed_slot ? a.seed_slot[i] : i;
     const unsigned long long bit = 1ull << (s & 63);
     atomicOr(&a.X[(size_t)v * a.W + (s >> 6)], bit);
     atomicOr(&s0[(size_t)v * a.W + (s >> 6)], bit);
@@ -1632,6 +1638,80 @@ static int choose_deep(ent_graph* g, const int32_t* src, int32_t n_src, bool* de
   return ENT_OK;
 }
 
+// One staged run of workspace w driven level by level from the host (the
+// kernels of the CUDA-graph loop, launched directly): memsets, seed, then
+// expand, commit and flush per level while the run is not done, and the final
+// flush. With `out`, one trace row per level (at most max_levels, the final
+// flush as level -1 if room is left) and *n_levels rows; with total_ms, the
+// device time of the whole run. Synchronises s.
+static int host_batch_loop(BatchWorkspace* w, int64_t E, BatchArgs a, cudaStream_t s, ent_level_trace* out,
+                           int32_t max_levels, int32_t* n_levels, float* total_ms) {
+  ENT_CUDA(cudaMemsetAsync(w->x_ptr, 0, w->x_bytes, s));
+  ENT_CUDA(cudaMemsetAsync(w->small_ptr, 0, w->small_bytes, s));
+  ENT_CUDA(cudaMemsetAsync(w->stats_ptr, 0, w->stats_bytes, s));
+  a.use_cond = 0;
+  cudaEvent_t e[4];
+  for (int i = 0; i < 4; ++i) ENT_CUDA(cudaEventCreate(&e[i]));
+  ENT_CUDA(cudaEventRecord(e[3], s));
+  k_b_seed<<<1, BB, 0, s>>>(a);
+  int n = 0;
+  int64_t iters = 0;  // level-loop iterations: expand, commit and flush launches each
+  for (;;) {
+    ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
+    ENT_CUDA(cudaStreamSynchronize(s));
+    const BatchCtl h = *w->ctl_h;
+    if (h.done || iters >= max_levels) break;
+    ++iters;
+    if (out) {
+      ent_level_trace& t = out[n];
+      t.level = h.level;
+      t.direction = h.dir;
+      t.bu_sweep = h.dir;
+      t.pad = 0;
+      t.frontier_vertices = h.n_jf[h.cur];
+      t.frontier_edges = h.m_f;
+      t.unvisited_queued = E - h.m_done;
+    }
+    ENT_CUDA(cudaEventRecord(e[0], s));
+    if (w->W > 2) k_b_expand<true><<<w->grid, BB, w->smem, s>>>(a);
+    else k_b_expand<false><<<w->grid, BB, w->smem, s>>>(a);
+    ENT_CUDA(cudaEventRecord(e[1], s));
+    k_b_commit<<<w->grid, BB, 0, s>>>(a);
+    k_b_flush<<<w->grid_flush, BB, w->smem_flush, s>>>(a, 0);
+    ENT_CUDA(cudaEventRecord(e[2], s));
+    ENT_CUDA(cudaGetLastError());
+    if (out) {
+      ENT_CUDA(cudaEventSynchronize(e[2]));
+      float ta = 0, tb = 0;
+      cudaEventElapsedTime(&ta, e[0], e[1]);
+      cudaEventElapsedTime(&tb, e[1], e[2]);
+      out[n].expand_ms = ta;
+      out[n].inspect_ms = tb;
+      ++n;
+    }
+  }
+  ENT_CUDA(cudaEventRecord(e[0], s));
+  k_b_flush<<<w->grid_flush, BB, w->smem_flush, s>>>(a, 1);
+  ENT_CUDA(cudaEventRecord(e[1], s));
+  ENT_CUDA(cudaStreamSynchronize(s));
+  float tf = 0, tt = 0;
+  cudaEventElapsedTime(&tf, e[0], e[1]);
+  cudaEventElapsedTime(&tt, e[3], e[1]);
+  if (total_ms) *total_ms = tt;
+  if (out && n < max_levels) {
+    ent_level_trace& t = out[n];
+    memset(&t, 0, sizeof(t));
+    t.level = -1;  // the final flush (depth rows + per-source stats)
+    t.inspect_ms = tf;
+    ++n;
+  }
+  for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]);
+  g_kernel_launches += 2 + 3 * iters;
+  if (n_levels) *n_levels = out ? n : (int32_t)iters;
+  if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "batched traversal error flags 0x%x", w->ctl_h->err);
+  return ENT_OK;
+}
+
 int run_bfs_batch(ent_graph* g, const int32_t* src, int32_t n_src, int32_t* depth_dev, cudaStream_t stream,
                   ent_stats* stats, bool bytes) {
   for (int i = 0; i < n_src; ++i)
@@ -1733,79 +1813,102 @@ int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t
   int rc = ensure_batch(g, n_src);
   if (rc != ENT_OK) return rc;
   BatchWorkspace* w = g->bws;
-  cudaStream_t s = g->stream;
-  rc = stage_request(g, w, src, n_src, depth_dev, s, nullptr, false);
+  rc = stage_request(g, w, src, n_src, depth_dev, g->stream, nullptr, false);
   if (rc != ENT_OK) return rc;
-  ENT_CUDA(cudaMemsetAsync(w->x_ptr, 0, w->x_bytes, s));
-  ENT_CUDA(cudaMemsetAsync(w->small_ptr, 0, w->small_bytes, s));
-  ENT_CUDA(cudaMemsetAsync(w->stats_ptr, 0, w->stats_bytes, s));
-  BatchArgs a = w->args;
-  a.use_cond = 0;
-  k_b_seed<<<1, BB, 0, s>>>(a);
-  cudaEvent_t e[4];
-  for (int i = 0; i < 4; ++i) ENT_CUDA(cudaEventCreate(&e[i]));
-  int n = 0;
-  int64_t iters = 0;  // level-loop iterations: expand, commit and flush launches each
-  for (;;) {
-    ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, s));
-    ENT_CUDA(cudaStreamSynchronize(s));
-    const BatchCtl h = *w->ctl_h;
-    if (h.done || n >= max_levels) break;
-    ++iters;
-    ent_level_trace& t = out[n];
-    t.level = h.level;
-    t.direction = h.dir;
-    t.bu_sweep = h.dir;
-    t.pad = 0;
-    t.frontier_vertices = h.n_jf[h.cur];
-    t.frontier_edges = h.m_f;
-    t.unvisited_queued = (int64_t)g->E - h.m_done;
-    ENT_CUDA(cudaEventRecord(e[0], s));
-    if (w->W > 2) k_b_expand<true><<<w->grid, BB, w->smem, s>>>(a);
-    else k_b_expand<false><<<w->grid, BB, w->smem, s>>>(a);
-    ENT_CUDA(cudaEventRecord(e[1], s));
-    k_b_commit<<<w->grid, BB, 0, s>>>(a);
-    k_b_flush<<<w->grid_flush, BB, w->smem_flush, s>>>(a, 0);
-    ENT_CUDA(cudaEventRecord(e[2], s));
-    ENT_CUDA(cudaGetLastError());
-    ENT_CUDA(cudaEventSynchronize(e[2]));
-    float ta = 0, tb = 0;
-    cudaEventElapsedTime(&ta, e[0], e[1]);
-    cudaEventElapsedTime(&tb, e[1], e[2]);
-    t.expand_ms = ta;
-    t.inspect_ms = tb;
-    ++n;
-  }
-  ENT_CUDA(cudaEventRecord(e[0], s));
-  k_b_flush<<<w->grid_flush, BB, w->smem_flush, s>>>(a, 1);
-  ENT_CUDA(cudaEventRecord(e[1], s));
-  ENT_CUDA(cudaStreamSynchronize(s));
-  float tf = 0;
-  cudaEventElapsedTime(&tf, e[0], e[1]);
-  if (n < max_levels) {
-    ent_level_trace& t = out[n];
-    memset(&t, 0, sizeof(t));
-    t.level = -1;  // the final flush (depth rows + per-source stats)
-    t.inspect_ms = tf;
-    ++n;
-  }
-  for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]);
-  g_kernel_launches += 2 + 3 * (int64_t)iters;
-  *n_levels = n;
-  if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "batched traversal error flags 0x%x", w->ctl_h->err);
-  return ENT_OK;
+  return host_batch_loop(w, g->E, w->args, g->stream, out, max_levels, n_levels, nullptr);
 }
 
 }  // extern "C"
 
-// Many graphs, one launch: each graph's batched traversal is an independent
-// branch (its own while node) of one CUDA graph.
+// Many graphs, one launch. The graphs share no vertex, so one batched
+// traversal over their disjoint union computes every graph's rows at once:
+// source slot s starts at the s-th source of every graph (a seed list), and a
+// slot's bits never leave the graph they started in. Each level then runs one
+// expand and one commit for all graphs together, over the whole GPU, instead
+// of one small launch chain per graph. The descriptor table (MultiPart) says
+// where each graph sits in its union (first vertex, first edge); graph k's
+// sources are slots 0 .. n_src[k]-1. Graphs are grouped by the width class of
+// their request (64-bit words per vertex), one union per class, so a narrow
+// request never carries a wide one's words; each class is one branch of the
+// plan's CUDA graph. A graph's slots past its own sources repeat them
+// (slot s starts at source s % n_src[k]): every slot then reaches every
+// graph's components as in an ordinary batch, and vertices stop needing bits
+// exactly as they would there. Those rows are computed and never returned.
+struct MultiPart {
+  int32_t graph;   // index in the plan's graph list
+  int64_t v0, e0;  // first vertex and first edge of the graph in its union
+};
+
+struct MultiUnion {
+  ent_graph* u = nullptr;    // the union's CSR and traversal arrays
+  BatchWorkspace* w = nullptr;
+  int32_t* depth = nullptr;  // [slots][u->V]
+  int32_t* seeds = nullptr;  // seed vertices [n_seed], then their slots [n_seed]
+  int32_t slots = 0, n_seed = 0;
+  std::vector<MultiPart> parts;
+};
+
+// Uploads a union's run state (its sources are the plan's seed list, already
+// on the device) and source mask on stream s.
+static int stage_union(const MultiUnion& mu, cudaStream_t s) {
+  BatchWorkspace* w = mu.w;
+  std::vector<unsigned long long> mask(w->W, 0);
+  for (int i = 0; i < mu.slots; ++i) mask[i >> 6] |= 1ull << (i & 63);
+  ENT_CUDA(cudaMemcpyAsync((void*)w->args.mask, mask.data(), sizeof(unsigned long long) * w->W, cudaMemcpyHostToDevice, s));
+  BatchCtl init = {};
+  init.n_src = mu.slots;
+  init.n_seed = mu.n_seed;
+  init.depth = mu.depth;
+  ENT_CUDA(cudaMemcpyAsync(w->ctl, &init, sizeof(BatchCtl), cudaMemcpyHostToDevice, s));
+  return ENT_OK;
+}
+
+// The union's direction threshold (batch alpha), measured once at creation.
+// A union's frontier at level L sums its graphs' level-L frontiers, so the
+// threshold that suits one graph alone need not suit the sum: on 48 R-MAT
+// graphs of scales 12-20, alpha 4 runs level 1 top-down over 72M frontier
+// edges in 6.7 ms where bottom-up takes 2.5 ms. Candidates are the value of
+// the member with the most edges and 2..32, each run twice host-driven; the
+// lowest time wins. Depths never depend on it. A union deeper than 64 levels
+// keeps the member's value: its frontiers are small, and each candidate would
+// cost a long host-driven run.
+static int tune_union_alpha(MultiUnion& mu, cudaStream_t s) {
+  BatchWorkspace* w = mu.w;
+  const double own = w->args.alpha;
+  std::vector<double> cand = {own};
+  for (double c : {2.0, 4.0, 8.0, 16.0, 32.0})
+    if (c != own) cand.push_back(c);
+  double best = own;
+  float best_ms = 0.f;
+  for (size_t i = 0; i < cand.size(); ++i) {
+    BatchArgs a = w->args;
+    a.alpha = cand[i];
+    float t = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      int rc = stage_union(mu, s);
+      if (rc != ENT_OK) return rc;
+      float ms = 0.f;
+      int32_t levels = 0;
+      rc = host_batch_loop(w, mu.u->E, a, s, nullptr, INT32_MAX, &levels, &ms);
+      if (rc != ENT_OK) return rc;
+      if (i == 0 && levels > 64) return ENT_OK;
+      t = rep == 0 ? ms : std::min(t, ms);
+    }
+    if (i == 0 || t < best_ms) {
+      best_ms = t;
+      best = cand[i];
+    }
+  }
+  w->args.alpha = best;
+  return ENT_OK;
+}
+
 struct ent_multi {
   std::vector<ent_graph*> graphs;
   std::vector<int32_t> n_src;
-  std::vector<std::vector<int32_t>> src;
-  std::vector<int32_t*> depth;  // device outputs, one per graph
-  std::vector<BatchWorkspace*> ws;  // the plan's own traversal state per graph
+  std::vector<int64_t> vcount;  // V of each graph: after creation the plan reads no member graph
+  std::vector<MultiUnion> unions;
+  std::vector<std::pair<int32_t, int32_t>> where;  // graph k: (union, part)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t stream = nullptr;
@@ -1816,15 +1919,74 @@ struct ent_multi {
 static void multi_free(ent_multi* m) {
   if (!m) return;
   DeviceGuard dg(m->device);
+  if (m->stream) cudaStreamSynchronize(m->stream);
   if (m->exec) cudaGraphExecDestroy(m->exec);
   if (m->graph) cudaGraphDestroy(m->graph);
-  for (int32_t* p : m->depth)
-    if (p) cudaFree(p);
-  for (BatchWorkspace* w : m->ws) destroy_batch_workspace(w);
+  for (MultiUnion& mu : m->unions) {
+    destroy_batch_workspace(mu.w);
+    if (mu.depth) cudaFree(mu.depth);
+    if (mu.seeds) cudaFree(mu.seeds);
+    if (mu.u) ent_graph_destroy(mu.u);
+  }
   if (m->ev0) cudaEventDestroy(m->ev0);
   if (m->ev1) cudaEventDestroy(m->ev1);
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
+}
+
+// Graph k's offsets into the union's, shifted by the edges before it (n = V_k + 1
+// entries; the last equals the next graph's first, so the overlap is harmless).
+__global__ void k_union_off(const int64_t* __restrict__ off, int64_t n, int64_t e0, int64_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = off[i] + e0;
+}
+
+// Graph k's neighbour ids into the union's, shifted by the vertices before it.
+__global__ void k_union_adj(const int32_t* __restrict__ adj, int64_t n, int32_t v0, int32_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = adj[i] + v0;
+}
+
+// Builds union mu (its parts listed) on the device: CSR by shifted copies of
+// the member graphs', then degrees, traversal order and lead entries as for
+// any graph. Batch options are those of the member with the most edges.
+static int build_union(ent_multi* m, MultiUnion& mu) {
+  int64_t V = 0, E = 0;
+  int32_t big = mu.parts[0].graph;
+  for (MultiPart& p : mu.parts) {
+    const ent_graph* g = m->graphs[p.graph];
+    p.v0 = V;
+    p.e0 = E;
+    V += g->V;
+    E += g->E;
+    if (g->E > m->graphs[big]->E) big = p.graph;
+  }
+  if (V > (int64_t)INT32_MAX - 64)
+    return fail(ENT_ERR_UNSUPPORTED, "graphs of one width class hold %lld vertices together; ids are int32",
+                (long long)V);
+  ent_graph* u = new ent_graph();
+  u->device = m->device;
+  mu.u = u;  // freed with the plan on any error below
+  int rc = graph_alloc(u, V, E);
+  if (rc != ENT_OK) return rc;
+  ENT_CUDA(cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking));
+  int sms = 0;
+  ENT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device));
+  auto blocks = [&](int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 16)); };
+  for (const MultiPart& p : mu.parts) {
+    const ent_graph* g = m->graphs[p.graph];
+    k_union_off<<<blocks(g->V + 1), 256, 0, u->stream>>>(g->off, g->V + 1, p.e0, u->off + p.v0);
+    g_kernel_launches++;
+    if (g->E > 0) {
+      k_union_adj<<<blocks(g->E), 256, 0, u->stream>>>(g->adj, g->E, (int32_t)p.v0, u->adj + p.e0);
+      g_kernel_launches++;
+    }
+    ENT_CUDA(cudaGetLastError());
+  }
+  rc = graph_finish(u);
+  if (rc != ENT_OK) return rc;
+  u->opts = m->graphs[big]->opts;
+  return ENT_OK;
 }
 
 extern "C" {
@@ -1834,45 +1996,71 @@ int ent_multi_create(ent_graph* const* graphs, int32_t n_graphs, const int32_t* 
   clear_error();
   if (!graphs || !src || !n_src || !out || n_graphs < 1) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
   *out = nullptr;
+  for (int k = 0; k < n_graphs; ++k)
+    if (!graphs[k]) return fail(ENT_ERR_INVALID_ARG, "graph %d is null", k);
+  // a graph may be listed more than once (several source sets): every entry
+  // is its own part of a union
   const int dev = graphs[0]->device;
   for (int k = 0; k < n_graphs; ++k) {
-    if (!graphs[k]) return fail(ENT_ERR_INVALID_ARG, "graph %d is null", k);
     if (graphs[k]->device != dev) return fail(ENT_ERR_INVALID_ARG, "all graphs must be on one GPU");
     if (n_src[k] < 1 || n_src[k] > MAX_BATCH) return fail(ENT_ERR_INVALID_ARG, "graph %d: bad source count", k);
-    for (int j = k + 1; j < n_graphs; ++j)
-      if (graphs[j] == graphs[k]) return fail(ENT_ERR_INVALID_ARG, "graph %d listed twice", k);
+  }
+  int64_t at = 0;
+  for (int k = 0; k < n_graphs; ++k) {
+    for (int i = 0; i < n_src[k]; ++i)
+      if (src[at + i] < 0 || src[at + i] >= graphs[k]->V)
+        return fail(ENT_ERR_INVALID_ARG, "graph %d: source %d out of range", k, src[at + i]);
+    at += n_src[k];
   }
   DeviceGuard dg(dev);
   ent_multi* m = new ent_multi();
   m->device = dev;
-  int64_t at = 0;
-  for (int k = 0; k < n_graphs; ++k) {
-    m->graphs.push_back(graphs[k]);
-    m->n_src.push_back(n_src[k]);
-    m->src.emplace_back(src + at, src + at + n_src[k]);
-    for (int32_t s : m->src.back())
-      if (s < 0 || s >= graphs[k]->V) {
-        multi_free(m);
-        return fail(ENT_ERR_INVALID_ARG, "graph %d: source %d out of range", k, s);
+  m->graphs.assign(graphs, graphs + n_graphs);
+  m->n_src.assign(n_src, n_src + n_graphs);
+  for (int k = 0; k < n_graphs; ++k) m->vcount.push_back(graphs[k]->V);
+  m->where.resize(n_graphs);
+  // one union per width class, graphs in request order within it
+  for (int cls = 1; cls <= WMAX; cls <<= 1) {
+    MultiUnion mu;
+    for (int k = 0; k < n_graphs; ++k)
+      if (words_for(n_src[k]) == cls) {
+        m->where[k] = {(int32_t)m->unions.size(), (int32_t)mu.parts.size()};
+        mu.parts.push_back({k, 0, 0});
+        mu.slots = std::max(mu.slots, n_src[k]);
       }
-    at += n_src[k];
+    if (mu.parts.empty()) continue;
+    mu.n_seed = mu.slots * (int32_t)mu.parts.size();
+    m->unions.push_back(std::move(mu));
   }
   cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&m->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&m->ev1);
   if (e == cudaSuccess) e = cudaGraphCreate(&m->graph, 0);
   if (e != cudaSuccess) { multi_free(m); return fail(ENT_ERR_CUDA, "multi setup: %s", cudaGetErrorString(e)); }
-  for (int k = 0; k < n_graphs; ++k) {
-    ent_graph* g = graphs[k];
-    BatchWorkspace* w = nullptr;
-    int rc = create_batch_workspace(g, n_src[k], &w);
+  std::vector<int64_t> first(n_graphs + 1, 0);
+  for (int k = 0; k < n_graphs; ++k) first[k + 1] = first[k] + n_src[k];
+  for (MultiUnion& mu : m->unions) {
+    int rc = build_union(m, mu);
+    if (rc == ENT_OK) rc = create_batch_workspace(mu.u, mu.slots, &mu.w);
     if (rc != ENT_OK) { multi_free(m); return rc; }
-    m->ws.push_back(w);
-    int32_t* d = nullptr;
-    e = cudaMalloc(&d, sizeof(int32_t) * (size_t)n_src[k] * g->V);
-    if (e != cudaSuccess) { multi_free(m); return fail(ENT_ERR_OOM, "multi output allocation failed"); }
-    m->depth.push_back(d);
-    rc = append_branch(g, w, m->graph, m->stream);
+    // seed list: slot i of graph k starts at its source i % n_src[k]
+    std::vector<int32_t> h(2 * (size_t)mu.n_seed);
+    size_t j = 0;
+    for (const MultiPart& p : mu.parts) {
+      const int32_t n = n_src[p.graph];
+      for (int32_t i = 0; i < mu.slots; ++i, ++j) {
+        h[j] = (int32_t)p.v0 + src[first[p.graph] + i % n];
+        h[mu.n_seed + j] = i;
+      }
+    }
+    e = cudaMalloc(&mu.seeds, sizeof(int32_t) * h.size());
+    if (e == cudaSuccess) e = cudaMemcpy(mu.seeds, h.data(), sizeof(int32_t) * h.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&mu.depth, sizeof(int32_t) * (size_t)mu.slots * mu.u->V);
+    if (e != cudaSuccess) { multi_free(m); return fail(ENT_ERR_OOM, "multi seed list or output allocation failed"); }
+    mu.w->args.src = mu.seeds;
+    mu.w->args.seed_slot = mu.seeds + mu.n_seed;
+    rc = tune_union_alpha(mu, m->stream);
+    if (rc == ENT_OK) rc = append_branch(mu.u, mu.w, m->graph, m->stream);
     if (rc != ENT_OK) { multi_free(m); return rc; }
   }
   e = cudaGraphInstantiate(&m->exec, m->graph, 0);
@@ -1886,13 +2074,8 @@ int ent_multi_run(ent_multi* m, double* device_ms) {
   clear_error();
   if (!m) return fail(ENT_ERR_INVALID_ARG, "null plan");
   DeviceGuard dg(m->device);
-  // hold every graph for the whole launch (pointer order avoids lock cycles)
-  std::vector<ent_graph*> order(m->graphs);
-  std::sort(order.begin(), order.end());
-  std::vector<std::unique_lock<std::mutex>> locks;
-  for (ent_graph* g : order) locks.emplace_back(g->mu);
-  for (size_t k = 0; k < m->graphs.size(); ++k) {
-    int rc = stage_request(m->graphs[k], m->ws[k], m->src[k].data(), m->n_src[k], m->depth[k], m->stream, nullptr, false);
+  for (MultiUnion& mu : m->unions) {
+    const int rc = stage_union(mu, m->stream);
     if (rc != ENT_OK) return rc;
   }
   ENT_CUDA(cudaEventRecord(m->ev0, m->stream));
@@ -1902,11 +2085,11 @@ int ent_multi_run(ent_multi* m, double* device_ms) {
   float ms = 0.f;
   cudaEventElapsedTime(&ms, m->ev0, m->ev1);
   if (device_ms) *device_ms = ms;
-  for (size_t k = 0; k < m->graphs.size(); ++k) {
-    BatchWorkspace* w = m->ws[k];
+  for (size_t i = 0; i < m->unions.size(); ++i) {
+    BatchWorkspace* w = m->unions[i].w;
     ENT_CUDA(cudaMemcpy(w->ctl_h, w->ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost));
     g_kernel_launches += run_launches(*w->ctl_h);
-    if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "graph %zu: batched traversal error flags 0x%x", k, w->ctl_h->err);
+    if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "width class %zu: batched traversal error flags 0x%x", i, w->ctl_h->err);
   }
   return ENT_OK;
 }
@@ -1915,9 +2098,30 @@ int ent_multi_depths(ent_multi* m, int32_t k, int32_t* depth_out) {
   clear_error();
   if (!m || !depth_out || k < 0 || k >= (int32_t)m->graphs.size()) return fail(ENT_ERR_INVALID_ARG, "bad arguments");
   DeviceGuard dg(m->device);
-  ENT_CUDA(cudaMemcpy(depth_out, m->depth[k], sizeof(int32_t) * (size_t)m->n_src[k] * m->graphs[k]->V,
-                      cudaMemcpyDeviceToHost));
+  const MultiUnion& mu = m->unions[m->where[k].first];
+  const MultiPart& p = mu.parts[m->where[k].second];
+  const size_t width = sizeof(int32_t) * (size_t)m->vcount[k], pitch = sizeof(int32_t) * (size_t)mu.u->V;
+  int max_pitch = 0;
+  ENT_CUDA(cudaDeviceGetAttribute(&max_pitch, cudaDevAttrMaxPitch, m->device));
+  if (pitch <= (size_t)max_pitch) {
+    ENT_CUDA(cudaMemcpy2D(depth_out, width, mu.depth + p.v0, pitch, width, m->n_src[k], cudaMemcpyDeviceToHost));
+  } else {
+    for (int32_t i = 0; i < m->n_src[k]; ++i)
+      ENT_CUDA(cudaMemcpy(depth_out + (size_t)i * m->vcount[k], mu.depth + (size_t)i * mu.u->V + p.v0, width,
+                          cudaMemcpyDeviceToHost));
+  }
   return ENT_OK;
+}
+
+int ent_multi_trace(ent_multi* m, int32_t k, ent_level_trace* out, int32_t max_levels, int32_t* n_levels) {
+  clear_error();
+  if (!m || !out || !n_levels || max_levels < 1 || k < 0 || k >= (int32_t)m->graphs.size())
+    return fail(ENT_ERR_INVALID_ARG, "bad arguments");
+  DeviceGuard dg(m->device);
+  MultiUnion& mu = m->unions[m->where[k].first];
+  const int rc = stage_union(mu, m->stream);
+  if (rc != ENT_OK) return rc;
+  return host_batch_loop(mu.w, mu.u->E, mu.w->args, m->stream, out, max_levels, n_levels, nullptr);
 }
 
 int ent_multi_destroy(ent_multi* m) {

@@ -342,20 +342,41 @@ int ent_bfs_batch_trace(ent_graph* g, const int32_t* src, int32_t n_src, int32_t
 
 /* Many graphs of uneven sizes in one launch: graphs[k] gets n_src[k] sources
  * from src (concatenated). depth_out[k] is a HOST array n_src[k] x V_k or
- * NULL. All graphs must live on the same GPU. */
+ * NULL. All graphs must live on the same GPU; a graph may be listed more than
+ * once (several source sets). */
 int ent_bfs_multi(ent_graph* const* graphs, int32_t n_graphs, const int32_t* src,
                   const int32_t* n_src, int32_t* const* depth_out);
 
-/* The same as a reusable plan: create once (allocates the plan's own
- * traversal state and device outputs, builds one CUDA graph with one branch
- * per graph), run many times (one graph launch; device_ms may be NULL),
- * read each graph's n_src[k] x V_k depths, destroy. */
+/* The same as a reusable plan: create once, run many times (one graph
+ * launch; device_ms may be NULL), read each graph's n_src[k] x V_k depths,
+ * destroy. The graphs are grouped by the width class of their request (64-bit
+ * words per vertex: ceil(n_src / 64) rounded up to a power of two), and each
+ * class runs as ONE batched traversal over the disjoint union of its graphs:
+ * create copies the graphs' CSR into one union per class (vertex and edge
+ * offsets per graph, the plan's descriptor table) and seeds source slot s at
+ * the s-th source of every graph of the class; a graph with fewer sources
+ * than the class's widest request repeats its own (slot s at source
+ * s % n_src[k]). Every level then runs one expand and one commit for all
+ * graphs of a class over the whole GPU. Create also measures each union's
+ * direction threshold (batch alpha: the member with the most edges' own value
+ * and 2, 4, 8, 16, 32, two host-driven runs each, the fastest kept; unions
+ * deeper than 64 levels keep the member's value). The plan holds its own copies (CSR,
+ * traversal state, outputs of the widest request x the union's vertices), so
+ * the graphs may be closed after create; one run at a time per plan. Apart
+ * from alpha, a union runs with the batch options of its member with the most
+ * edges. */
 typedef struct ent_multi ent_multi;
 int ent_multi_create(ent_graph* const* graphs, int32_t n_graphs, const int32_t* src,
                      const int32_t* n_src, ent_multi** out);
 int ent_multi_run(ent_multi* plan, double* device_ms);
 int ent_multi_depths(ent_multi* plan, int32_t k, int32_t* depth_out);
 int ent_multi_destroy(ent_multi* plan);
+/* Per-level trace of the union that holds graph k: one host-driven run of the
+ * plan's kernels for that width class (its rows are then readable with
+ * ent_multi_depths), one row per level and the final flush as level -1, as
+ * ent_bfs_batch_trace writes them; *n_levels rows. */
+int ent_multi_trace(ent_multi* plan, int32_t k, ent_level_trace* out, int32_t max_levels,
+                    int32_t* n_levels);
 
 /* ------------------------------------------------- several GPUs --------- */
 /* Many sources over replicas of one graph on several GPUs of a node. No

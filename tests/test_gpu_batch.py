@@ -189,6 +189,77 @@ def test_multi_graph_one_launch(eb, orc):
         g.close()
 
 
+def test_multi_graph_union_every_row(eb, orc):
+    """The plan runs each width class as one traversal over the disjoint union
+    of its graphs. One class mixes a deep grid (many flush windows), R-MAT
+    graphs with 1 and 64 sources (padded slots), a source on an isolated
+    vertex and one graph listed twice with other sources; a second class holds
+    a 100-source request. Every row of every graph against the oracle, twice,
+    and the plan still answers after its graphs are closed."""
+    grid = eb.Csr.grid(60, 50, 0.1, seed=0x6E1D77)
+    r1 = eb.Csr.rmat(11, 8, seed=0x5EED0101)
+    r2 = eb.Csr.rmat(12, 16, seed=0x5EED0102)
+    iso_s = np.array([0, 1, 2], dtype=np.int64)
+    iso = eb.Csr.from_edges(iso_s, iso_s + 1, 6)  # path 0-1-2-3, vertices 4 and 5 isolated
+    csrs = [grid, r1, r2, iso, r2, r1]
+    graphs = [eb.Graph.from_csr(c) for c in csrs[:4]]
+    handles = graphs + [graphs[2], graphs[1]]
+    srcs = [eb.pick_sources(grid.beg_pos, 700, 5),
+            eb.pick_sources(r1.beg_pos, 701, 1),
+            eb.pick_sources(r2.beg_pos, 702, 64),
+            np.array([5, 0, 3], dtype=np.int32),
+            eb.pick_sources(r2.beg_pos, 703, 7),
+            eb.pick_sources(r1.beg_pos, 704, 100)]
+    plan = eb.MultiPlan(handles, srcs)
+    try:
+        for _ in range(2):
+            plan.run()
+            for k, (c, s) in enumerate(zip(csrs, srcs)):
+                d = plan.depths(k)
+                assert d.shape == (len(s), c.vert_count)
+                for i, v in enumerate(s):
+                    exp, _ = orc.bfs(c.beg_pos, c.csr, int(v))
+                    np.testing.assert_array_equal(d[i], exp, err_msg=f"graph {k} row {i}")
+        for g in graphs:
+            g.close()
+        plan.run()
+        exp, _ = orc.bfs(grid.beg_pos, grid.csr, int(srcs[0][4]))
+        np.testing.assert_array_equal(plan.depths(0)[4], exp)
+    finally:
+        plan.close()
+        for g in graphs:
+            g.close()
+
+
+def test_multi_graph_trace(eb, orc):
+    """A plan's per-level trace of one width class: a row per level up to the
+    deepest graph of the union, the final flush last, and the rows of the
+    traced run readable afterwards; the other class keeps its own rows."""
+    r1 = eb.Csr.rmat(12, 16, seed=0x5EED0201)
+    grid = eb.Csr.grid(40, 30, 0.0, seed=1)
+    csrs = [r1, grid, r1]
+    graphs = [eb.Graph.from_csr(r1), eb.Graph.from_csr(grid)]
+    srcs = [eb.pick_sources(r1.beg_pos, 801, 20), np.array([0, 1199], dtype=np.int32),
+            eb.pick_sources(r1.beg_pos, 802, 200)]
+    with eb.MultiPlan([graphs[0], graphs[1], graphs[0]], srcs) as plan:
+        plan.run()
+        rows = plan.trace(1)
+        assert rows[-1]["level"] == -1
+        assert [r["level"] for r in rows[:-1]] == list(range(len(rows) - 1))
+        deepest = max(int(orc.bfs(c.beg_pos, c.csr, int(v))[0].max()) for c, s in zip(csrs[:2], srcs[:2]) for v in s)
+        assert len(rows) - 1 == deepest + 1  # the level that finds nothing ends the run
+        assert all(r["direction"] in (0, 1) for r in rows[:-1])
+        for k, (c, s) in enumerate(zip(csrs, srcs)):
+            d = plan.depths(k)
+            for i in (0, len(s) - 1):
+                exp, _ = orc.bfs(c.beg_pos, c.csr, int(s[i]))
+                np.testing.assert_array_equal(d[i], exp, err_msg=f"graph {k} row {i}")
+        with pytest.raises(eb.EntError):
+            plan.trace(3)
+    for g in graphs:
+        g.close()
+
+
 @pytest.mark.parametrize("n", [40, 130, 600])
 def test_sources_in_small_components(eb, orc, n):
     """Sources of small components mixed with giant-component sources. Once a
