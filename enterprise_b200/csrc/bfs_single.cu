@@ -96,6 +96,7 @@ struct BfsCtl {
   int32_t narrow_levels;
   int32_t iters;      // inspector launches (level-loop iterations)
   int32_t narrow_runs;
+  int32_t narrow_calls;  // launches of the small-frontier kernel, those that left at once included
   uint32_t n_spill;   // small-frontier entries that did not fit in shared memory
   uint32_t acc_maxd;  // maximum degree in the next frontier being classified
   int64_t n_f, m_f;   // frontier size and degree sum
@@ -128,7 +129,6 @@ struct LevelArgs {
   int32_t policy;
   double alpha, beta, ref_ratio;
   cudaGraphConditionalHandle cond;
-  cudaGraphConditionalHandle cond_narrow;
   int32_t use_cond;
   int32_t max_levels;
   // small-frontier mode: enter at <= narrow_f vertices, <= narrow_m edges and
@@ -274,6 +274,7 @@ __global__ void k_init(LevelArgs a, int32_t src, DT* depth, int32_t* parent) {
   c->narrow_levels = 0;
   c->iters = 0;
   c->narrow_runs = 0;
+  c->narrow_calls = 0;
   c->n_spill = 0;
   c->acc_maxd = 0;
   c->n_f = 1;
@@ -614,7 +615,6 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
       c->iters = c->iters + 1;
       if (a.use_cond) {
         cudaGraphSetConditional(a.cond, 0u);
-        if (a.narrow_f > 0) cudaGraphSetConditional(a.cond_narrow, 0u);
       }
     }
     return;
@@ -871,7 +871,6 @@ __global__ void __launch_bounds__(BT) k_inspect(LevelArgs a) {
   __threadfence();
   if (a.use_cond) {
     cudaGraphSetConditional(a.cond, done ? 0u : 1u);
-    if (a.narrow_f > 0) cudaGraphSetConditional(a.cond_narrow, narrow ? 1u : 0u);
   }
 }
 
@@ -965,6 +964,7 @@ __global__ void __launch_bounds__(NT, 1) k_narrow(LevelArgs a) {
   __shared__ unsigned long long r_m[2][NC_MAX];
   cg::cluster_group cl = cg::this_cluster();
   BfsCtl* c = a.ctl;
+  if (blockIdx.x == 0 && threadIdx.x == 0) c->narrow_calls = c->narrow_calls + 1;
   if (c->done || !c->narrow) return;  // same value in every CTA
   const int nc = (int)cl.num_blocks(), rank = (int)cl.block_rank();
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -1296,12 +1296,14 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
   cudaGraphNode_t cond_node;
   ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &w->init_node[k], 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  // Loop body: expand -> inspect -> if (narrow) { small-frontier cluster }.
+  // Loop body: expand -> inspect -> small-frontier cluster. The cluster kernel
+  // runs every iteration and leaves at once unless the inspector chose the
+  // small-frontier mode (its first read; the same value in every CTA): an
+  // always-launched kernel that exits costs less than an IF node that is not
+  // taken (measured on B200: about 1.1 against 2.4 us per loop iteration).
   LevelArgs la = w->args;
   la.cond = handle;
   la.use_cond = 1;
-  if (w->narrow_nc > 0)
-    ENT_CUDA(cudaGraphConditionalHandleCreate(&la.cond_narrow, body, 0, cudaGraphCondAssignDefault));
   void* largs[1] = {&la};
   cudaKernelNodeParams bp = {};
   bp.func = (void*)k_expand<DT>;
@@ -1316,18 +1318,12 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
   bp.sharedMemBytes = 0;
   ENT_CUDA(cudaGraphAddKernelNode(&n_inspect, body, &n_expand, 1, &bp));
   if (w->narrow_nc > 0) {
-    cudaGraphNodeParams ip = {};
-    ip.type = cudaGraphNodeTypeConditional;
-    ip.conditional.handle = la.cond_narrow;
-    ip.conditional.type = cudaGraphCondTypeIf;
-    ip.conditional.size = 1;
-    cudaGraphNode_t n_if, n_narrow;
-    ENT_CUDA(cudaGraphAddNode(&n_if, body, &n_inspect, 1, &ip));
+    cudaGraphNode_t n_narrow;
     bp.func = (void*)k_narrow<DT>;
     bp.gridDim = dim3(w->narrow_nc);
     bp.blockDim = dim3(NT);
     bp.sharedMemBytes = (unsigned)w->smem_narrow;
-    ENT_CUDA(cudaGraphAddKernelNode(&n_narrow, ip.conditional.phGraph_out[0], nullptr, 0, &bp));
+    ENT_CUDA(cudaGraphAddKernelNode(&n_narrow, body, &n_inspect, 1, &bp));
     cudaLaunchAttributeValue cv = {};
     cv.clusterDim.x = (unsigned)w->narrow_nc;
     cv.clusterDim.y = 1;
@@ -1493,7 +1489,7 @@ static void fill_stats(const BfsCtl& h, float ms, ent_stats* stats) {
   stats->status = h.err;
   stats->device_ms = ms;
   stats->narrow_levels = h.narrow_levels;
-  stats->launches = 2 + 2 * h.iters + h.narrow_runs;
+  stats->launches = 2 + 2 * h.iters + h.narrow_calls;
 }
 
 // One launch of the workspace's instantiated traversal graph on stream s.

@@ -92,6 +92,30 @@ def test_bottom_up_to_top_down_from_the_list(eb, orc, alpha, beta, loop):
                 assert st.td_levels + st.bu_levels == st.levels
 
 
+@pytest.mark.parametrize("hub", [0, 4096])
+@pytest.mark.parametrize("policy", ["beamer", "reference", "bu"])
+def test_bottom_up_levels_in_a_row(eb, orc, policy, hub):
+    """Runs of bottom-up levels (the bottom-up-only policy makes every level
+    one), with and without the hub table, through both loop drivers: depths
+    against the oracle, parents, the same statistics. Launch counts: the
+    CUDA-graph loop launches expand, inspector and the small-frontier kernel
+    (which leaves at once unless chosen) every iteration; the host-driven loop
+    launches the small-frontier kernel only where it runs."""
+    for csr in (eb.Csr.rmat(15, 16, seed=0x7159), eb.Csr.er(40000, 12.0, seed=0x715A)):
+        with _graph(eb, csr, policy=policy, hub_slots=hub) as gg, \
+                _graph(eb, csr, policy=policy, hub_slots=hub, loop="host") as gh:
+            for src in eb.pick_sources(csr.beg_pos, 23, 5):
+                sg = _check(eb, orc, csr, gg, src)
+                sh = _check(eb, orc, csr, gh, src)
+                assert (sg.levels, sg.td_levels, sg.bu_levels, sg.narrow_levels) == \
+                       (sh.levels, sh.td_levels, sh.bu_levels, sh.narrow_levels)
+                it, rem = divmod(sg.launches - 2, 3)
+                runs = sh.launches - 2 - 2 * it
+                assert rem == 0 and 0 <= runs <= it, (sg.launches, sh.launches)
+                if policy == "bu":
+                    assert sg.bu_levels == sg.levels >= 3
+
+
 def test_rmat_s16_64_sources_bit_exact(eb, orc):
     """R-MAT scale 16, edge factor 16, 64 seeded non-isolated sources."""
     host = eb.Csr.rmat(16, 16, seed=0x5EED0016)
