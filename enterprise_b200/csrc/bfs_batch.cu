@@ -38,6 +38,7 @@ namespace ent {
 
 constexpr int BB = 256;        // threads per CTA
 constexpr int KMAX = 16;       // log slots (levels per flush window)
+constexpr int LOOP_UNROLL = 2; // level-loop bodies per while-node iteration of the CUDA-graph loop
 constexpr int WMAX = 32;       // words per vertex per launch (2048 sources)
 
 struct BatchCtl {
@@ -64,6 +65,7 @@ struct BatchCtl {
   int32_t joined;     // sources that joined this run
   int32_t if_runs;    // level-loop iterations whose flush did work (window flush or joined sources)
   int32_t n_seed;     // entries of the seed list (0: one seed per source, src[s] for source s)
+  int32_t iters;      // commit launches (level-loop bodies run, those after the end included)
 };
 
 struct BatchArgs {
@@ -754,7 +756,10 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
   __shared__ int s_last;
   BatchCtl* c = a.ctl;
   if (c->done) {  // never leave the while node spinning on a finished traversal
-    if (a.use_cond && blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      c->iters = c->iters + 1;
+      if (a.use_cond) cudaGraphSetConditional(a.cond, 0u);
+    }
     return;
   }
   const int cur = c->cur, nxt = cur ^ 1;
@@ -841,6 +846,7 @@ __global__ void __launch_bounds__(BB) k_b_commit(BatchArgs a) {
   if (dir == 0) vc->td_levels = vc->td_levels + 1; else vc->bu_levels = vc->bu_levels + 1;
   const int L = vc->level + 1;
   vc->level = L;
+  vc->iters = vc->iters + 1;
   if (a.box) join_sources(a, vc, L, nxt, n_next, m_next);
   // level L's active set is spent: it collects level L+2's from here
   for (int w = 0; w < a.W; ++w) a.act[cur][w] = 0;
@@ -1355,10 +1361,12 @@ int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream
   ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &prev, 1, &cp));
   prev = cond_node;
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  // Loop body: expand -> commit -> flush. The flush runs every level and leaves
-  // at once unless the window is full or sources joined (flush_now, clear_done):
-  // an always-launched kernel that exits costs less than an IF node that is not
-  // taken (measured on B200: about 1.1 against 2.4 us per loop iteration).
+  // Loop body: LOOP_UNROLL copies of expand -> commit -> flush in a chain (a
+  // while-node iteration costs about 5 us more than the kernel nodes in it on
+  // B200; every kernel treats a finished run as a no-op). The flush runs every
+  // level and leaves at once unless the window is full or sources joined
+  // (flush_now, clear_done): an always-launched kernel that exits costs less
+  // than an IF node that is not taken (about 1.1 against 2.4 us).
   BatchArgs la = w->args;
   la.cond = handle;
   la.use_cond = 1;
@@ -1366,22 +1374,26 @@ int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream
     int zero = 0;
     void* kl[1] = {&la};
     void* kf[2] = {&la, &zero};
-    cudaKernelNodeParams kp = {};
-    kp.blockDim = dim3(BB);
-    kp.func = expand_kernel(w->W);
-    kp.gridDim = dim3(w->grid);
-    kp.sharedMemBytes = (unsigned)w->smem;
-    kp.kernelParams = kl;
-    cudaGraphNode_t n_expand, n_commit, n_flush;
-    ENT_CUDA(cudaGraphAddKernelNode(&n_expand, body, nullptr, 0, &kp));
-    kp.func = (void*)k_b_commit;
-    kp.sharedMemBytes = 0;
-    ENT_CUDA(cudaGraphAddKernelNode(&n_commit, body, &n_expand, 1, &kp));
-    kp.func = (void*)k_b_flush;
-    kp.gridDim = dim3(w->grid_flush);
-    kp.sharedMemBytes = (unsigned)w->smem_flush;
-    kp.kernelParams = kf;
-    ENT_CUDA(cudaGraphAddKernelNode(&n_flush, body, &n_commit, 1, &kp));
+    cudaGraphNode_t chain = nullptr;
+    for (int u = 0; u < LOOP_UNROLL; ++u) {
+      cudaKernelNodeParams kp = {};
+      kp.blockDim = dim3(BB);
+      kp.func = expand_kernel(w->W);
+      kp.gridDim = dim3(w->grid);
+      kp.sharedMemBytes = (unsigned)w->smem;
+      kp.kernelParams = kl;
+      cudaGraphNode_t n_expand, n_commit, n_flush;
+      ENT_CUDA(cudaGraphAddKernelNode(&n_expand, body, chain ? &chain : nullptr, chain ? 1 : 0, &kp));
+      kp.func = (void*)k_b_commit;
+      kp.sharedMemBytes = 0;
+      ENT_CUDA(cudaGraphAddKernelNode(&n_commit, body, &n_expand, 1, &kp));
+      kp.func = (void*)k_b_flush;
+      kp.gridDim = dim3(w->grid_flush);
+      kp.sharedMemBytes = (unsigned)w->smem_flush;
+      kp.kernelParams = kf;
+      ENT_CUDA(cudaGraphAddKernelNode(&n_flush, body, &n_commit, 1, &kp));
+      chain = n_flush;
+    }
   }
   (void)cap_stream;
   {
@@ -1526,8 +1538,9 @@ static int ensure_batch(ent_graph* g, int n_src) {
 }
 
 // Kernels one finished graph-driven run launched: seed, final flush, and
-// expand, commit and flush per level (the flush leaves at once on most levels).
-static int64_t run_launches(const BatchCtl& h) { return 2 + 3 * (int64_t)h.level; }
+// expand, commit and flush per loop body run (the flush leaves at once on
+// most levels; bodies after the end only cost their launches).
+static int64_t run_launches(const BatchCtl& h) { return 2 + 3 * (int64_t)h.iters; }
 
 // Uploads sources, mask and the output pointer (the kernels read them from
 // device memory, so one instantiated graph serves every batch).

@@ -72,6 +72,7 @@ constexpr int NQCAP = 4096;      // small-frontier entries per CTA and buffer
 constexpr uint32_t NF_HEAVY = 1, NF_SPILL = 2;
 constexpr int LCAP = 128;        // vertices a CTA of a listing bottom-up level keeps (then the bitmap is used)
 constexpr int BU_ILP = 2;        // bottom-up light path: neighbours checked per step (2 beat 4 and 8)
+constexpr int LOOP_UNROLL = 2;   // level-loop bodies per while-node iteration of the CUDA-graph loop
 
 // Device-resident loop state. Written only by the reset kernel's and the
 // inspector's last CTA (plus atomics on the acc_* counters and n_raw); read
@@ -1296,39 +1297,49 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
   cudaGraphNode_t cond_node;
   ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &w->init_node[k], 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  // Loop body: expand -> inspect -> small-frontier cluster. The cluster kernel
-  // runs every iteration and leaves at once unless the inspector chose the
-  // small-frontier mode (its first read; the same value in every CTA): an
-  // always-launched kernel that exits costs less than an IF node that is not
-  // taken (measured on B200: about 1.1 against 2.4 us per loop iteration).
+  // Loop body: LOOP_UNROLL copies of expand -> inspect -> small-frontier
+  // cluster, in a chain. Measured on B200 with trivial kernels: a kernel node
+  // in a chain costs about 1.7 us, a while-node iteration about 5 us more, so
+  // each copy after the first saves that iteration. Every level kernel treats
+  // a finished traversal as a no-op (the inspector still counts its launch),
+  // so copies after the one that finished only cost their launches.
+  // The cluster kernel runs in every copy and leaves at once unless the
+  // inspector chose the small-frontier mode (its first read; the same value
+  // in every CTA): such a kernel costs less than an IF node that is not
+  // taken (about 1.1 against 2.4 us per iteration).
   LevelArgs la = w->args;
   la.cond = handle;
   la.use_cond = 1;
   void* largs[1] = {&la};
-  cudaKernelNodeParams bp = {};
-  bp.func = (void*)k_expand<DT>;
-  bp.gridDim = dim3(w->grid_expand);
-  bp.blockDim = dim3(BT);
-  bp.sharedMemBytes = (unsigned)w->smem_expand;
-  bp.kernelParams = largs;
-  cudaGraphNode_t n_expand, n_inspect;
-  ENT_CUDA(cudaGraphAddKernelNode(&n_expand, body, nullptr, 0, &bp));
-  bp.func = (void*)k_inspect;
-  bp.gridDim = dim3(w->grid_inspect);
-  bp.sharedMemBytes = 0;
-  ENT_CUDA(cudaGraphAddKernelNode(&n_inspect, body, &n_expand, 1, &bp));
-  if (w->narrow_nc > 0) {
-    cudaGraphNode_t n_narrow;
-    bp.func = (void*)k_narrow<DT>;
-    bp.gridDim = dim3(w->narrow_nc);
-    bp.blockDim = dim3(NT);
-    bp.sharedMemBytes = (unsigned)w->smem_narrow;
-    ENT_CUDA(cudaGraphAddKernelNode(&n_narrow, body, &n_inspect, 1, &bp));
-    cudaLaunchAttributeValue cv = {};
-    cv.clusterDim.x = (unsigned)w->narrow_nc;
-    cv.clusterDim.y = 1;
-    cv.clusterDim.z = 1;
-    ENT_CUDA(cudaGraphKernelNodeSetAttribute(n_narrow, cudaLaunchAttributeClusterDimension, &cv));
+  cudaGraphNode_t prev = nullptr;
+  for (int u = 0; u < LOOP_UNROLL; ++u) {
+    cudaKernelNodeParams bp = {};
+    bp.func = (void*)k_expand<DT>;
+    bp.gridDim = dim3(w->grid_expand);
+    bp.blockDim = dim3(BT);
+    bp.sharedMemBytes = (unsigned)w->smem_expand;
+    bp.kernelParams = largs;
+    cudaGraphNode_t n_expand, n_inspect;
+    ENT_CUDA(cudaGraphAddKernelNode(&n_expand, body, prev ? &prev : nullptr, prev ? 1 : 0, &bp));
+    bp.func = (void*)k_inspect;
+    bp.gridDim = dim3(w->grid_inspect);
+    bp.sharedMemBytes = 0;
+    ENT_CUDA(cudaGraphAddKernelNode(&n_inspect, body, &n_expand, 1, &bp));
+    prev = n_inspect;
+    if (w->narrow_nc > 0) {
+      cudaGraphNode_t n_narrow;
+      bp.func = (void*)k_narrow<DT>;
+      bp.gridDim = dim3(w->narrow_nc);
+      bp.blockDim = dim3(NT);
+      bp.sharedMemBytes = (unsigned)w->smem_narrow;
+      ENT_CUDA(cudaGraphAddKernelNode(&n_narrow, body, &n_inspect, 1, &bp));
+      cudaLaunchAttributeValue cv = {};
+      cv.clusterDim.x = (unsigned)w->narrow_nc;
+      cv.clusterDim.y = 1;
+      cv.clusterDim.z = 1;
+      ENT_CUDA(cudaGraphKernelNodeSetAttribute(n_narrow, cudaLaunchAttributeClusterDimension, &cv));
+      prev = n_narrow;
+    }
   }
   ENT_CUDA(cudaGraphInstantiate(&w->exec[k], graph, 0));
   return ENT_OK;
