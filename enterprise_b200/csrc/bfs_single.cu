@@ -185,69 +185,62 @@ __device__ __forceinline__ uint32_t block_max(uint32_t x, uint32_t* s_red) {
 }
 
 // --------------------------------------------------------------- reset ----
-__device__ void fill_neg1(int32_t* p, int64_t n, int64_t tid, int64_t nth) {
+// Fills p[0, n) with -1, except p[sp] = sv. The thread that stores the
+// element or 16-byte vector holding sp stores sv in it, so nothing has to be
+// ordered after the fill to set the source's own entry.
+__device__ void fill_neg1(int32_t* p, int64_t n, int64_t tid, int64_t nth, int64_t sp, int32_t sv) {
   uintptr_t addr = (uintptr_t)p;
   int64_t head = (int64_t)(((16 - (addr & 15)) & 15) >> 2);
   if ((addr & 3) != 0) head = n;  // not even 4-byte aligned: scalar path
   if (head > n) head = n;
-  for (int64_t i = tid; i < head; i += nth) p[i] = -1;
+  for (int64_t i = tid; i < head; i += nth) p[i] = i == sp ? sv : -1;
   int64_t nvec = (n - head) >> 2;
   int4* pv = reinterpret_cast<int4*>(p + head);
-  for (int64_t i = tid; i < nvec; i += nth) pv[i] = make_int4(-1, -1, -1, -1);
-  for (int64_t i = head + nvec * 4 + tid; i < n; i += nth) p[i] = -1;
+  const int64_t vs = sp >= head ? (sp - head) >> 2 : -1;
+  const int ks = (int)((sp - head) & 3);
+  for (int64_t i = tid; i < nvec; i += nth) {
+    const bool at = i == vs;
+    pv[i] = make_int4(at && ks == 0 ? sv : -1, at && ks == 1 ? sv : -1, at && ks == 2 ? sv : -1,
+                      at && ks == 3 ? sv : -1);
+  }
+  for (int64_t i = head + nvec * 4 + tid; i < n; i += nth) p[i] = i == sp ? sv : -1;
 }
 
 // Byte depths, the reference's depth_t (unsigned char, comm.h:69): depth d
-// (0..254) as d, unreached as 255 (INFTY, comm.h:131).
-__device__ void fill_ff(uint8_t* p, int64_t n, int64_t tid, int64_t nth) {
+// (0..254) as d, unreached as 255 (INFTY, comm.h:131). Fills p[0, n) with
+// 0xFF except p[sp] = sv, as fill_neg1 does.
+__device__ void fill_ff(uint8_t* p, int64_t n, int64_t tid, int64_t nth, int64_t sp, uint8_t sv) {
   const uintptr_t addr = (uintptr_t)p;
   int64_t head = (int64_t)((16 - (addr & 15)) & 15);
   if (head > n) head = n;
-  for (int64_t i = tid; i < head; i += nth) p[i] = 0xFF;
+  for (int64_t i = tid; i < head; i += nth) p[i] = i == sp ? sv : (uint8_t)0xFF;
   const int64_t nvec = (n - head) >> 4;
   uint4* pv = reinterpret_cast<uint4*>(p + head);
-  for (int64_t i = tid; i < nvec; i += nth) pv[i] = make_uint4(~0u, ~0u, ~0u, ~0u);
-  for (int64_t i = head + nvec * 16 + tid; i < n; i += nth) p[i] = 0xFF;
+  const int64_t vs = sp >= head ? (sp - head) >> 4 : -1;
+  const int bs = (int)((sp - head) & 15), ws = bs >> 2, sh = 8 * (bs & 3);
+  const uint32_t patched = ~(0xFFu << sh) | ((uint32_t)sv << sh);
+  for (int64_t i = tid; i < nvec; i += nth) {
+    const bool at = i == vs;
+    pv[i] = make_uint4(at && ws == 0 ? patched : ~0u, at && ws == 1 ? patched : ~0u, at && ws == 2 ? patched : ~0u,
+                       at && ws == 3 ? patched : ~0u);
+  }
+  for (int64_t i = head + nvec * 16 + tid; i < n; i += nth) p[i] = i == sp ? sv : (uint8_t)0xFF;
 }
-__device__ __forceinline__ void fill_unreached(int32_t* p, int64_t n, int64_t tid, int64_t nth) {
-  fill_neg1(p, n, tid, nth);
+__device__ __forceinline__ void fill_unreached(int32_t* p, int64_t n, int64_t tid, int64_t nth, int64_t src) {
+  fill_neg1(p, n, tid, nth, src, 0);
 }
-__device__ __forceinline__ void fill_unreached(uint8_t* p, int64_t n, int64_t tid, int64_t nth) {
-  fill_ff(p, n, tid, nth);
+__device__ __forceinline__ void fill_unreached(uint8_t* p, int64_t n, int64_t tid, int64_t nth, int64_t src) {
+  fill_ff(p, n, tid, nth, src, 0);
 }
 
-// The level kernels are instantiated for int32 depths and for the reference's
-// byte depths (DT = uint8_t: written directly, no conversion pass).
+// Loop state for one traversal from src (its frontier: src alone, classified
+// by degree). Written by one thread of k_reset while the others fill; no fill
+// touches the control block or the queues.
 template <class DT>
-__global__ void __launch_bounds__(BT) k_reset(LevelArgs a, int32_t src, DT* depth, int32_t* parent) {
-  const int64_t tid = blockIdx.x * (int64_t)BT + threadIdx.x, nth = (int64_t)gridDim.x * BT;
-  fill_unreached(depth, a.V, tid, nth);
-  if (parent) fill_neg1(parent, a.V, tid, nth);
-  const int64_t W = (a.V + 31) >> 5;
-  for (int64_t i = tid; i < W; i += nth) {
-    a.vis[i] = 0;
-    a.fb[0][i] = 0;
-    a.fb[1][i] = 0;
-  }
-  for (int64_t i = tid; i < a.hub_slots; i += nth) {
-    a.hub[0][i] = 0;
-    a.hub[1][i] = 0;
-  }
-}
-
-// Initialises the loop state for one traversal (one thread; runs after
-// k_reset, so it needs no completion counter and also resets the counters
-// the level kernels use).
-template <class DT>
-__global__ void k_init(LevelArgs a, int32_t src, DT* depth, int32_t* parent) {
-  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+__device__ void init_state(const LevelArgs& a, int32_t src, DT* depth, int32_t* parent) {
   BfsCtl* c = a.ctl;
   const int d = a.deg[src];
   const int cl = cls_of(d, a);
-  depth[src] = 0;
-  if (parent) parent[src] = src;
-  a.vis[src >> 5] = 1u << (src & 31);
-  a.fb[0][src >> 5] = 1u << (src & 31);
   a.q[0][cl][0] = src;
   c->src = src;
   c->depth = reinterpret_cast<int32_t*>(depth);  // the level kernels of this DT cast it back
@@ -286,7 +279,31 @@ __global__ void k_init(LevelArgs a, int32_t src, DT* depth, int32_t* parent) {
   for (int k = 0; k < KS; ++k) c->tot[k] = 0;
   c->tile_ticket = 0;
   c->finished = 0;
-  __threadfence();
+}
+
+// The first kernel of a traversal: depths unreached but depth[src] = 0,
+// parents -1 but parent[src] = src, the visited and frontier-0 bitmaps holding
+// src alone, hub tables clear, and the loop state (one thread). The level
+// kernels are instantiated for int32 depths and for the reference's byte
+// depths (DT = uint8_t: written directly, no conversion pass).
+template <class DT>
+__global__ void __launch_bounds__(BT) k_reset(LevelArgs a, int32_t src, DT* depth, int32_t* parent) {
+  const int64_t tid = blockIdx.x * (int64_t)BT + threadIdx.x, nth = (int64_t)gridDim.x * BT;
+  if (tid == 0) init_state(a, src, depth, parent);
+  fill_unreached(depth, a.V, tid, nth, src);
+  if (parent) fill_neg1(parent, a.V, tid, nth, src, src);
+  const int64_t W = (a.V + 31) >> 5, sw = src >> 5;
+  const uint32_t sb = 1u << (src & 31);
+  for (int64_t i = tid; i < W; i += nth) {
+    const uint32_t x = i == sw ? sb : 0u;
+    a.vis[i] = x;
+    a.fb[0][i] = x;
+    a.fb[1][i] = 0;
+  }
+  for (int64_t i = tid; i < a.hub_slots; i += nth) {
+    a.hub[0][i] = 0;
+    a.hub[1][i] = 0;
+  }
 }
 
 // ------------------------------------------------------------ top-down ----
@@ -1224,7 +1241,6 @@ struct BfsWorkspace {
   cudaGraph_t graph[2] = {nullptr, nullptr};
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
   cudaGraphNode_t reset_node[2] = {nullptr, nullptr};
-  cudaGraphNode_t init_node[2] = {nullptr, nullptr};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // ent_bfs_many: a second depth buffer, a copy stream and pinned per-source
   // copies of the control block (created on first use)
@@ -1283,10 +1299,6 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
   kp.sharedMemBytes = 0;
   kp.kernelParams = rargs;
   ENT_CUDA(cudaGraphAddKernelNode(&w->reset_node[k], graph, nullptr, 0, &kp));
-  kp.func = (void*)k_init<DT>;
-  kp.gridDim = dim3(1);
-  kp.blockDim = dim3(32);
-  ENT_CUDA(cudaGraphAddKernelNode(&w->init_node[k], graph, &w->reset_node[k], 1, &kp));
   cudaGraphConditionalHandle handle;
   ENT_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
   cudaGraphNodeParams cp = {};
@@ -1295,7 +1307,7 @@ static int build_graph(ent_graph* g, BfsWorkspace* w) {
   cp.conditional.type = cudaGraphCondTypeWhile;
   cp.conditional.size = 1;
   cudaGraphNode_t cond_node;
-  ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &w->init_node[k], 1, &cp));
+  ENT_CUDA(cudaGraphAddNode(&cond_node, graph, &w->reset_node[k], 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   // Loop body: LOOP_UNROLL copies of expand -> inspect -> small-frontier
   // cluster, in a chain. Measured on B200 with trivial kernels: a kernel node
@@ -1500,7 +1512,7 @@ static void fill_stats(const BfsCtl& h, float ms, ent_stats* stats) {
   stats->status = h.err;
   stats->device_ms = ms;
   stats->narrow_levels = h.narrow_levels;
-  stats->launches = 2 + 2 * h.iters + h.narrow_calls;
+  stats->launches = 1 + 2 * h.iters + h.narrow_calls;
 }
 
 // One launch of the workspace's instantiated traversal graph on stream s.
@@ -1521,16 +1533,12 @@ static int launch_graph(ent_graph* g, BfsWorkspace* w, int32_t src, DT* depth, i
   kp.sharedMemBytes = 0;
   kp.kernelParams = rargs;
   ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec[k], w->reset_node[k], &kp));
-  kp.func = (void*)k_init<DT>;
-  kp.gridDim = dim3(1);
-  kp.blockDim = dim3(32);
-  ENT_CUDA(cudaGraphExecKernelNodeSetParams(w->exec[k], w->init_node[k], &kp));
   ENT_CUDA(cudaGraphLaunch(w->exec[k], s));
   return ENT_OK;
 }
 
 int launch_bfs_single(BfsWorkspace* w, int32_t src, int32_t* depth_dev, cudaStream_t s) {
-  g_kernel_launches += 2;  // reset + init; the level kernels are counted by bfs_single_stats
+  g_kernel_launches += 1;  // reset; the level kernels are counted by bfs_single_stats
   return launch_graph(nullptr, w, src, depth_dev, nullptr, s);  // int32 graph: built with the workspace
 }
 
@@ -1538,7 +1546,7 @@ int bfs_single_stats(BfsWorkspace* w, cudaStream_t s, ent_stats* stats) {
   ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));
   ENT_CUDA(cudaStreamSynchronize(s));
   fill_stats(*w->ctl_h, 0.f, stats);
-  g_kernel_launches += stats->launches - 2;
+  g_kernel_launches += stats->launches - 1;
   if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "device traversal reported error flags 0x%x", w->ctl_h->err);
   return ENT_OK;
 }
@@ -1559,8 +1567,7 @@ static int run_bfs_typed(ent_graph* g, int32_t src, DT* depth, int32_t* parent, 
     LevelArgs la = w->args;
     la.use_cond = 0;
     k_reset<DT><<<w->grid_reset, BT, 0, s>>>(la, src, depth, parent);
-    k_init<DT><<<1, 32, 0, s>>>(la, src, depth, parent);
-    g_kernel_launches += 2;
+    g_kernel_launches += 1;
     ENT_CUDA(cudaGetLastError());
     int32_t* flags_h = &w->ctl_h->done;  // done, narrow
     for (int64_t it = 0;; ++it) {
@@ -1588,7 +1595,7 @@ static int run_bfs_typed(ent_graph* g, int32_t src, DT* depth, int32_t* parent, 
     if (g->opts.loop == ENT_LOOP_GRAPH) g_kernel_launches += stats->launches;
     if (w->ctl_h->err) return fail(ENT_ERR_TIMEOUT, "device traversal reported error flags 0x%x", w->ctl_h->err);
   } else if (g->opts.loop == ENT_LOOP_GRAPH) {
-    g_kernel_launches += 2;  // reset + init; level kernels are counted when stats are read
+    g_kernel_launches += 1;  // reset; level kernels are counted when stats are read
   }
   return ENT_OK;
 }
@@ -1752,7 +1759,7 @@ int run_bfs_deep(ent_graph* g, const int32_t* src, int32_t n_src, void* depth_de
   }
   ENT_CUDA(cudaEventRecord(l->end, cs));
   if (!stats) {
-    g_kernel_launches += (bytes ? 3 : 2) * (int64_t)n_src;  // reset, init (+ pack); level kernels uncounted
+    g_kernel_launches += (bytes ? 2 : 1) * (int64_t)n_src;  // reset (+ pack); level kernels uncounted
     return ENT_OK;
   }
   ENT_CUDA(cudaEventSynchronize(l->end));
@@ -1806,8 +1813,7 @@ int ent_bfs_trace(ent_graph* g, int32_t src, ent_level_trace* out, int32_t max_l
   la.use_cond = 0;
   ENT_CUDA(cudaEventRecord(w->ev0, s));
   k_reset<int32_t><<<w->grid_reset, BT, 0, s>>>(la, src, w->depth, nullptr);
-  k_init<int32_t><<<1, 32, 0, s>>>(la, src, w->depth, nullptr);
-  g_kernel_launches += 2;
+  g_kernel_launches += 1;
   int n = 0;
   for (;;) {
     ENT_CUDA(cudaMemcpyAsync(w->ctl_h, w->ctl, sizeof(BfsCtl), cudaMemcpyDeviceToHost, s));
