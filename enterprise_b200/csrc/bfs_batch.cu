@@ -63,7 +63,7 @@ struct BatchCtl {
   int32_t out_bytes;  // depth rows are uint8 (the reference's depth type, 255 = unreached), not int32
   int32_t clear_done; // sources joined: the completion bits no longer hold (k_b_flush clears them)
   int32_t joined;     // sources that joined this run
-  int32_t if_runs;    // level-loop iterations whose flush did work (window flush or joined sources)
+  int32_t flush_runs;    // level-loop iterations whose flush did work (window flush or joined sources)
   int32_t n_seed;     // entries of the seed list (0: one seed per source, src[s] for source s)
   int32_t iters;      // commit launches (level-loop bodies run, those after the end included)
 };
@@ -1256,7 +1256,7 @@ __global__ void __launch_bounds__(BB, 3) k_b_flush(BatchArgs a, int final_flush)
     vc->flush_now = 0;
   }
   vc->clear_done = 0;
-  vc->if_runs = vc->if_runs + 1;
+  vc->flush_runs = vc->flush_runs + 1;
   vc->finished = 0;
   __threadfence();
 }

@@ -41,11 +41,13 @@
 //    each queue entry carries the vertex's row start and degree, read while
 //    its visit was being claimed, so a level costs one adjacency read, one
 //    status probe and one claim on its critical path.
-//  * The whole traversal is one CUDA graph: a reset kernel, then a while node
-//    whose body is [expand, inspect, if(narrow){narrow}]; the inspector sets
-//    both conditions. The look-back wait is the only spin: it is bounded, and
-//    a classification whose wait ran out ends the traversal with an error
-//    bit instead of handing on inconsistent queues.
+//  * The whole traversal is one CUDA graph: a reset kernel (which also writes
+//    the loop state), then a while node whose body is two copies of
+//    [expand, inspect, narrow]; the inspector sets the loop condition and the
+//    small-frontier flag, and the cluster kernel leaves at once unless that
+//    flag is set. The look-back wait is the only spin: it is bounded, and a
+//    classification whose wait ran out ends the traversal with an error bit
+//    instead of handing on inconsistent queues.
 #include <algorithm>
 #include <type_traits>
 #include <vector>
