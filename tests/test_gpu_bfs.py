@@ -378,3 +378,12 @@ def test_edgeless_graphs(eb, orc, V):
         g.bfs_many(srcs, outs)
         for s, o in zip(srcs, outs):
             np.testing.assert_array_equal(o, np.where(np.arange(V) == s, 0, 255).astype(np.uint8))
+        # a multi-graph plan whose union starts and ends with this edgeless graph
+        other = eb.Csr.rmat(8, 4, seed=0xED6E + V)
+        parts = [(csr, srcs), (other, [0, 5, 9]), (csr, [V - 1])]
+        with eb.Graph.from_csr(other) as go, eb.MultiPlan([g, go, g], [s for _, s in parts]) as plan:
+            plan.run()
+            for k, (c, ss) in enumerate(parts):
+                d = plan.depths(k)
+                for i, s in enumerate(ss):
+                    np.testing.assert_array_equal(d[i], orc.bfs(c.beg_pos, c.csr, s)[0], err_msg=f"part {k} row {i}")
