@@ -566,7 +566,19 @@ def run_batched(args, rank=0, no_multi=False):
     if args.no_multi or no_multi:
         torch.cuda.empty_cache()
         return out
-    # 48 graphs of uneven sizes, 64 sources each, one launch
+    out["multi_graph_48"] = run_multi(args)
+    return out
+
+
+def run_multi(args):
+    """48 R-MAT graphs of uneven sizes (scales 12-20, edge factors 8-32), 64
+    seeded sources each, as one multi-graph plan: one CUDA-graph launch, one
+    batched traversal over the disjoint union of the graphs. The first and
+    last row of every graph are compared with the oracle. With --batch-loop
+    host the plan also runs once through its host-driven trace (the same
+    kernels launched per level, which profilers can see) and reports it."""
+    import torch
+    import enterprise_b200 as eb
     rng = np.random.default_rng(0x48)
     graphs, sources, hosts, total_v = [], [], [], 0
     for k in range(48):
@@ -587,16 +599,23 @@ def run_batched(args, rank=0, no_multi=False):
         dd = torch.empty((len(sk), gk.vert_count), dtype=torch.int32, device="cuda")
         edges += sum(x.traversed_edges for x in gk.bfs_batch_device(sk, dd.data_ptr()))
         del dd
+    trace = None
+    if args.batch_loop == "host":
+        rows = plan.trace(0)
+        trace = [{"level": r["level"], "direction": r["direction"],
+                  "ms": round(r["expand_ms"] + r["inspect_ms"], 4)} for r in rows]
     # the first and the last row of every graph against the CPU oracle
     bad = []
     for k in range(48):
         dk = plan.depths(k)
         bad += [dict(m, graph=k) for m in
                 oracle_rows(hosts[k], [int(sources[k][0]), int(sources[k][63])], lambda j: dk[0 if j == 0 else 63])]
-    out["multi_graph_48"] = {"ms": round(ms, 3), "graphs": 48, "sources_per_graph": 64, "vertices_total": total_v,
-                             "gteps": round(edges / ms / 1e6, 2), "oracle_checked": 96, "oracle_mismatches": bad,
-                             "launches": "one CUDA graph launch: one batched traversal over the disjoint union of "
-                                         "the graphs (one width class, shared source slots)"}
+    out = {"ms": round(ms, 3), "graphs": 48, "sources_per_graph": 64, "vertices_total": total_v,
+           "gteps": round(edges / ms / 1e6, 2), "oracle_checked": 96, "oracle_mismatches": bad,
+           "launches": "one CUDA graph launch: one batched traversal over the disjoint union of "
+                       "the graphs (one width class, shared source slots)"}
+    if trace is not None:
+        out["host_driven_trace"] = trace
     plan.close()
     for gk in graphs:
         gk.close()
@@ -997,7 +1016,7 @@ def main():
     ap.add_argument("--deep-graphs", default="grid,er", help="graphs of the high-diameter/uniform leg")
     ap.add_argument("--deep-sources", type=int, default=32)
     ap.add_argument("--ingest-scale", type=int, default=24)
-    ap.add_argument("--only", choices=["batch", "serve", "deep", "ingest", "burst"], default=None,
+    ap.add_argument("--only", choices=["batch", "multi", "serve", "deep", "ingest", "burst"], default=None,
                     help="run only one of the extra measurements and print it")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -1015,8 +1034,8 @@ def main():
         dist = tdist
     try:
         if args.only:
-            line = {"batch": run_batched, "serve": run_serving, "deep": run_deep, "ingest": run_ingest,
-                    "burst": run_burst
+            line = {"batch": run_batched, "multi": run_multi, "serve": run_serving, "deep": run_deep,
+                    "ingest": run_ingest, "burst": run_burst
                     }[args.only](args)
         elif args.impl == "reference":
             line = run_reference(args, rank, world)

@@ -39,6 +39,7 @@ namespace ent {
 constexpr int BB = 256;        // threads per CTA
 constexpr int KMAX = 16;       // log slots (levels per flush window)
 constexpr int LOOP_UNROLL = 2; // level-loop bodies per while-node iteration of the CUDA-graph loop
+constexpr int SEED_THREADS = 1024;  // the one seeding CTA: a multi-graph plan seeds thousands of entries
 constexpr int WMAX = 32;       // words per vertex per launch (2048 sources)
 
 struct BatchCtl {
@@ -155,8 +156,10 @@ __device__ __forceinline__ void publish_act(const BatchArgs& a, const unsigned l
 }
 
 // ------------------------------------------------------------ seeding -----
-// Runs after X, donebits and both jfb bitmaps are zeroed (memset nodes). One CTA.
-__global__ void k_b_seed(BatchArgs a) {
+// Runs after X, donebits and both jfb bitmaps are zeroed (memset nodes). One CTA
+// of SEED_THREADS threads: each seed is a short chain of dependent atomics, and
+// a multi-graph plan's seed list holds thousands (48 graphs x 64 sources).
+__global__ void __launch_bounds__(SEED_THREADS) k_b_seed(BatchArgs a) {
   BatchCtl* c = a.ctl;
   unsigned long long* s0 = slot_ptr(a, 0);
   __shared__ int s_n, s_h;
@@ -165,20 +168,45 @@ __global__ void k_b_seed(BatchArgs a) {
   __syncthreads();
   // A seed list gives a source several start vertices: a traversal over the
   // disjoint union of many graphs seeds source s in every graph at once.
+  // The shared counters take one atomic per warp (ballot, then the leader),
+  // not one per seed: thousands of same-address atomics would serialise. The
+  // loop runs whole blocks at a time so that every lane takes part.
   const int n_seed = c->n_seed > 0 ? c->n_seed : c->n_src;
-  for (int i = threadIdx.x; i < n_seed; i += blockDim.x) {
-    const int v = a.src[i];
-    const int s = a.seed_slot ? a.seed_slot[i] : i;
-    const unsigned long long bit = 1ull << (s & 63);
-    atomicOr(&a.X[(size_t)v * a.W + (s >> 6)], bit);
-    atomicOr(&s0[(size_t)v * a.W + (s >> 6)], bit);
-    const uint32_t tb = 1u << (v & 31);
-    if (!(atomicOr(&a.jfb[0][v >> 5], tb) & tb)) {
-      a.jf[0][atomicAdd(&s_n, 1)] = v;
-      const int d = a.deg[v];
-      atomicAdd(&s_m, (unsigned long long)d);
-      if (d >= a.heavy_deg) a.heavy[0][atomicAdd(&s_h, 1)] = v;
+  const int lane = threadIdx.x & 31;
+  for (int i0 = 0; i0 < n_seed; i0 += blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    bool fresh = false;
+    int v = 0, d = 0;
+    if (i < n_seed) {
+      v = a.src[i];
+      const int s = a.seed_slot ? a.seed_slot[i] : i;
+      const unsigned long long bit = 1ull << (s & 63);
+      atomicOr(&a.X[(size_t)v * a.W + (s >> 6)], bit);
+      atomicOr(&s0[(size_t)v * a.W + (s >> 6)], bit);
+      const uint32_t tb = 1u << (v & 31);
+      fresh = !(atomicOr(&a.jfb[0][v >> 5], tb) & tb);
+      if (fresh) d = a.deg[v];
     }
+    const unsigned mf = __ballot_sync(FULL, fresh);
+    if (!mf) continue;
+    const int leader = __ffs(mf) - 1;
+    int at = 0;
+    if (lane == leader) at = atomicAdd(&s_n, __popc(mf));
+    at = __shfl_sync(FULL, at, leader);
+    if (fresh) a.jf[0][at + __popc(mf & lanemask_lt())] = v;
+    const bool hv = fresh && d >= a.heavy_deg;
+    const unsigned mh = __ballot_sync(FULL, hv);
+    if (mh) {
+      const int lh = __ffs(mh) - 1;
+      int ah = 0;
+      if (lane == lh) ah = atomicAdd(&s_h, __popc(mh));
+      ah = __shfl_sync(FULL, ah, lh);
+      if (hv) a.heavy[0][ah + __popc(mh & lanemask_lt())] = v;
+    }
+    // degrees are below 2^31: split in 16-bit halves, each sums over 32 lanes without overflow
+    const unsigned dlo = __reduce_add_sync(FULL, (unsigned)d & 0xFFFFu);
+    const unsigned dhi = __reduce_add_sync(FULL, (unsigned)d >> 16);
+    if (lane == leader) atomicAdd(&s_m, ((unsigned long long)dhi << 16) + dlo);
   }
   for (int w = threadIdx.x; w < a.W; w += blockDim.x) {
     a.act[0][w] = a.mask[w];
@@ -1344,7 +1372,7 @@ int append_branch(ent_graph* g, BatchWorkspace* w, cudaGraph_t graph, cudaStream
     cudaKernelNodeParams kp = {};
     kp.func = (void*)k_b_seed;
     kp.gridDim = dim3(1);
-    kp.blockDim = dim3(BB);
+    kp.blockDim = dim3(SEED_THREADS);
     kp.kernelParams = kargs;
     cudaGraphNode_t n;
     ENT_CUDA(cudaGraphAddKernelNode(&n, graph, &prev, 1, &kp));
@@ -1653,7 +1681,7 @@ static int host_batch_loop(BatchWorkspace* w, int64_t E, BatchArgs a, cudaStream
   cudaEvent_t e[4];
   for (int i = 0; i < 4; ++i) ENT_CUDA(cudaEventCreate(&e[i]));
   ENT_CUDA(cudaEventRecord(e[3], s));
-  k_b_seed<<<1, BB, 0, s>>>(a);
+  k_b_seed<<<1, SEED_THREADS, 0, s>>>(a);
   int n = 0;
   int64_t iters = 0;  // level-loop iterations: expand, commit and flush launches each
   for (;;) {
